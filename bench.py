@@ -1,0 +1,304 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 SVD (libpacosvd.so) on the plain FP32 single-matrix
+workload: M = N = 4096, entries iid N(0,1) from a seed (config 2a of the
+reference's benchmark plan), synthetic data.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload cfg2a|cfg2b|cfg1|cfg3]
+
+A step is one full SVD (stage 1 bidiagonalization + U/Vt formation, stage 2
+divide and conquer + final products) of a matrix already resident in HBM.
+Metric: SVDs/s (whole job).  One process per GPU; the SVD does not shard, so
+N > 1 runs independent replicas (weak scaling) and takes the max time over
+ranks.  Between timed steps a 512 MiB buffer is written to flush L2.
+
+`--impl reference` times the reference algorithm on the host CPU: the
+reference itself is Ascend C for a Huawei NPU and cannot be built here, so
+this is the FP64 C restatement in oracle/ (single-threaded), on a bounded
+sample matrix scaled to the workload by the O(n^3) operation count.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "paco-svd_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+WORKLOADS = {
+    "cfg2a": dict(M=4096, N=4096, gen="normal"),
+    "cfg2b": dict(M=4096, N=4096, gen="graded"),
+    "cfg1": dict(M=64, N=32, gen="uniform"),
+    "cfg3": dict(M=8192, N=4096, gen="clustered"),
+}
+CPU_SAMPLE_N = 768  # oracle sample size (about 5 s of single-thread work)
+
+
+def make_matrix(wl, seed=1234):
+    M, N, gen = wl["M"], wl["N"], wl["gen"]
+    rng = np.random.default_rng(seed)
+    if gen == "uniform":
+        return rng.uniform(-1, 1, (M, N)).astype(np.float32)
+    if gen == "normal":
+        return rng.standard_normal((M, N), dtype=np.float32)
+
+    def haar(n, m):
+        Q, R = np.linalg.qr(rng.standard_normal((n, m)))
+        return Q * np.sign(np.diag(R))[None, :]
+
+    if gen == "graded":
+        sig = 10.0 ** (-6 * np.arange(N) / (N - 1))
+    else:  # 512 clusters of 8, centres log-uniform in [1e-4, 1], spacing 1e-7
+        centres = 10.0 ** rng.uniform(-4, 0, N // 8)
+        sig = np.sort((centres[:, None] * (1 + 1e-7 * np.arange(8))[None, :]).ravel())[::-1]
+    return ((haar(M, N) * sig[None, :]) @ haar(N, N).T).astype(np.float32)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1])); smax = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def traffic_ratio():
+    """DRAM bytes per algorithmic byte of the row pass, from the committed ncu
+    summary (profiles/bd_row_pass.txt, line 'dram_per_alg_byte: X')."""
+    path = os.path.join(ROOT, "profiles", "bd_row_pass.txt")
+    try:
+        for ln in open(path):
+            if ln.startswith("dram_per_alg_byte:"):
+                return float(ln.split(":")[1])
+    except Exception:
+        pass
+    return None
+
+
+def cpu_baseline(wl, steps=1):
+    """Oracle port (FP64 C restatement, 1 thread) on a CPU_SAMPLE_N^2 sample,
+    scaled to the workload's SVDs/s by the n^3 work ratio."""
+    import oracle
+    n = min(CPU_SAMPLE_N, wl["N"])
+    A = make_matrix(dict(M=n * wl["M"] // wl["N"], N=n, gen=wl["gen"]), seed=99)
+    times = []
+    for _ in range(max(1, steps)):
+        t = time.perf_counter()
+        oracle.svd(A)
+        times.append(time.perf_counter() - t)
+    t = statistics.median(times)
+    scale = (wl["M"] * wl["N"] ** 2) / (A.shape[0] * A.shape[1] ** 2)
+    return {"value": 1.0 / (t * scale), "unit": "SVDs/s", "cores": 1, "kind": "port",
+            "sample": f"oracle.svd on a {A.shape[0]}x{A.shape[1]} {wl['gen']} matrix, median of {len(times)} "
+                      f"({t:.2f} s), scaled by the M*N^2 work ratio {scale:.1f}"}
+
+
+def run_reference(args, wl, rank):
+    if rank != 0:
+        return
+    for _ in range(args.warmup if args.warmup < 1 else 1):
+        pass
+    cb = cpu_baseline(wl, steps=args.steps)
+    line = {"metric": "SVDs/sec", "value": cb["value"], "unit": "SVDs/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 / cb["value"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: {wl['M']}x{wl['N']} FP32 {wl['gen']}, plain single-matrix SVD"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "SVDs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cfg2a", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, wl, rank)
+        return
+
+    import torch
+    import pacosvd as P
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    M, N = wl["M"], wl["N"]
+    A_host = make_matrix(wl, seed=1234 + rank)
+    A0 = torch.from_numpy(A_host).cuda()
+    W = P.Workspace(M, N)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        W.A.copy_(A0)
+        W.run()
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    rc, info = P.sync_status(W.ws)
+    if rc:
+        raise SystemExit(f"device status {rc} ({info}) during warm-up")
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    lib = P.lib()
+    lib.paco_launch_count.restype = ctypes.c_ulonglong
+    lib.paco_profile_read.argtypes = [ctypes.POINTER(ctypes.c_double)]
+    launches0 = lib.paco_launch_count()
+    lib.paco_profile_enable(1)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.fill_(k & 0xff)  # L2 flush outside the timed window
+        ev[k][0].record(stream)
+        step()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    prof = (ctypes.c_double * 3)()
+    lib.paco_profile_read(prof)
+    launches = lib.paco_launch_count() - launches0
+    lib.paco_profile_enable(0)
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    rc, info = P.sync_status(W.ws)
+    if rc:
+        raise SystemExit(f"device status {rc} ({info}) in the timed region")
+
+    # correctness of the last step, against LAPACK where affordable
+    s = W.sigma.float().cpu().numpy().astype(np.float64)
+
+    # end to end through the host-buffer C ABI (H2D of A, D2H of U, Vt, sigma)
+    ctx = P.HostContext(M, N)
+    pin = lambda shape: torch.empty(shape, dtype=torch.float32).pin_memory()
+    Ah, Uh, Vh, sh = pin((M, N)), pin((M, M)), pin((N, N)), pin((N,))
+    Ah.copy_(torch.from_numpy(A_host))
+    e2e_ms = []
+    ctx.svd(Ah, Uh, Vh, sh)
+    for _ in range(max(1, min(args.steps, 3))):
+        t = time.perf_counter()
+        ctx.svd(Ah, Uh, Vh, sh)
+        e2e_ms.append((time.perf_counter() - t) * 1000)
+    ctx.close()
+    e2e_t = statistics.median(e2e_ms)
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    peaks, peak_kind = measured_peaks()
+    rp_ms, rp_launches, rp_bytes = prof[0], prof[1], prof[2]
+    achieved = (rp_bytes / 1e9) / (rp_ms / 1e3) if rp_ms > 0 else None
+    ratio = traffic_ratio()
+    roof = {"kernel": "bd_row_pass (stage-1 fused GEMV row pass)", "bound": "hbm",
+            "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": (achieved / peaks["hbm_gbs"]) if achieved else None,
+            "traffic": (ratio * rp_bytes / rp_launches) if (ratio and rp_launches) else None,
+            "alg_bytes_per_launch": rp_bytes / max(rp_launches, 1),
+            "avg_launch_us": 1000.0 * rp_ms / max(rp_launches, 1),
+            "launches": int(rp_launches), "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)"}
+    value = world * args.steps / (total_ms / 1000.0)
+    line = {"metric": "SVDs/sec", "value": value, "unit": "SVDs/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: {M}x{N} FP32 {wl['gen']}, plain single-matrix SVD "
+                                   f"(bidiagonalization + U/Vt formation + divide and conquer)",
+                       "M": M, "N": N, "l2": "512 MiB buffer written between timed steps",
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+            "sigma_max": float(s[0]), "sigma_min": float(s[-1]),
+            "roofline": roof, "clocks": clk,
+            "e2e": {"value": 1000.0 / e2e_t * world, "unit": "SVDs/s",
+                    "h2d_bytes_per_step": 4 * M * N, "d2h_bytes_per_step": 4 * (M * M + N * N + N)},
+            "gpu_launches": int(launches)}
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(wl)
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

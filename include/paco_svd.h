@@ -1,0 +1,117 @@
+/*
+ * paco_svd.h -- C ABI of the B200 (sm_100a) SVD library libpacosvd.so.
+ *
+ * Drop-in for the operator surface of DEAVEN-MITCH/paco-svd: the two device
+ * kernels launched by main.cpp (upper_bidiagonalization, svd_DC), the host
+ * tiling helpers (getTilingSize, GenerateTiling) and the buffer contract of
+ * main.cpp:33-123.  Plain pointers and sizes only; `stream` is a
+ * cudaStream_t passed as void* (NULL = legacy default stream).
+ *
+ * All matrices are FP32, row-major, M >= N.  Every entry point returns a
+ * PACO_* status; device-side failures (non-convergence, bounded-wait
+ * timeouts, a tiling blob for another N) are recorded in the workspace and
+ * reported by paco_sync_status().
+ */
+#ifndef PACO_SVD_H
+#define PACO_SVD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum paco_status {
+    PACO_OK = 0,
+    PACO_ERR_INVALID_ARG = 1,     /* M < N, N <= 0, NULL pointer, short buffer  */
+    PACO_ERR_UNSUPPORTED = 2,     /* shape outside the kernels' limits         */
+    PACO_ERR_CUDA = 3,            /* a CUDA runtime call failed                 */
+    PACO_ERR_DEVICE = 4,          /* a kernel recorded an error                 */
+    PACO_ERR_NONCONVERGENCE = 5,  /* a secular root hit its iteration limit     */
+    PACO_ERR_TIMEOUT = 6,         /* a bounded device-side wait gave up         */
+    PACO_ERR_BAD_TILING = 7,      /* tiling blob does not describe this N       */
+    PACO_ERR_NONFINITE = 8        /* NaN/Inf in the input matrix                */
+};
+
+/* Largest N accepted by the stage-1 kernels (row tiles live in shared memory). */
+#define PACO_MAX_N 8192
+
+/* Size in bytes of the tiling blob for an N-column bidiagonal.
+ * Replaces svd_tiling.cpp:67 getTilingSize(int N, int svdBlockNum). */
+int getTilingSize(int N, int svdBlockNum);
+
+/* Writes the leaf partition of svd_tiling.cpp:83-130 (3-column leaves,
+ * remainder cases for N%3) into TilingHost (getTilingSize bytes).
+ * Replaces svd_tiling.cpp:83 GenerateTiling(int N, int blockDim, uint8_t*). */
+void GenerateTiling(int N, int blockDim, uint8_t *TilingHost);
+
+/* Buffer sizes in bytes of main.cpp:33-43, in this order:
+ * [0] U M*M, [1] A M*N, [2] Vt N*N, [3] d N, [4] e N-1, [5] tauq N,
+ * [6] taup N-1, [7] qt 2*N*N, [8] wt 2*N*N, [9] tiling, [10] idx 16*N*u32,
+ * [11] workspace (this library's, replaces the 40*32 B soft-sync area). */
+void paco_buffer_sizes(int M, int N, size_t out[12]);
+
+/* Workspace bytes needed by upper_bidiagonalization and svd_DC. */
+size_t paco_workspace_size(int M, int N);
+
+/* Stage 1: Golub-Kahan Householder upper bidiagonalization of a (M x N).
+ * a is overwritten with the Householder vectors (d on the diagonal, e on the
+ * superdiagonal); d[N], e[N-1], tauq[N], taup[N-1] are written; u (M x M)
+ * and vt (N x N) are formed explicitly (no pre-zeroing needed), so that
+ * A = U * B * Vt.  Reflector convention of upper_bidiagonalization.cpp:182-218
+ * (d_i, e_i >= 0 unless the reflected part is exactly zero).
+ * Replaces upper_bidiagonalization.cpp:967
+ *   upper_bidiagonalization(M, N, a, u, vt, d, e, tauq, taup, workspace). */
+int upper_bidiagonalization(int M, int N, float *a, float *u, float *vt, float *d,
+                            float *e, float *tauq, float *taup, void *workspace,
+                            void *stream);
+
+/* Stage 2: bidiagonal divide and conquer on (d, e).  On return d holds the
+ * singular values in descending order, u[:, :N] <- u[:, :N] * Q and
+ * vt <- W^T * vt.  a (M x N) is used as scratch (destroyed); qt, wt (2*N*N
+ * floats each) and idx (16*N uint32) are scratch; tiling is the device copy
+ * of the GenerateTiling blob.
+ * Replaces svd.cpp:2105 svd_DC(M, N, a, u, vt, d, e, qt, wt, idx, workspace, tiling). */
+int svd_DC(int M, int N, float *a, float *u, float *vt, float *d, float *e, float *qt,
+           float *wt, uint32_t *idx, void *workspace, const uint8_t *tiling, void *stream);
+
+/* Synchronizes `stream` and returns the first device-side error recorded in
+ * `workspace` since the last call (then clears it).  *info receives detail. */
+int paco_sync_status(void *workspace, void *stream, int *info);
+
+/* Device-buffer one-shot SVD (both stages, the flow of main.cpp:56-174 on
+ * device memory): A (M x N, destroyed), U (M x M), Vt (N x N), sigma (N,
+ * descending).  ws must hold paco_svd_workspace_size(M, N) bytes; all the
+ * intermediate buffers of main.cpp live in it.  Asynchronous on `stream`. */
+size_t paco_svd_workspace_size(int M, int N);
+int paco_svd(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws,
+             size_t ws_bytes, void *stream);
+
+/* Host-buffer SVD through a reusable context (device buffers and pinned
+ * staging allocated once): copies A to the device, runs both stages, copies
+ * U, Vt, sigma back, synchronizes.  The path svd_main takes (main.cpp:64-174). */
+typedef struct paco_ctx paco_ctx;
+int paco_ctx_create(int M, int N, paco_ctx **out);
+int paco_ctx_svd_host(paco_ctx *ctx, const float *A, float *U, float *Vt, float *sigma);
+void paco_ctx_destroy(paco_ctx *ctx);
+
+/* Library version string. */
+const char *paco_version(void);
+
+/* Kernel timing (no counterpart in the reference, which is profiled with
+ * msprof, myprof.sh:1-8): while enabled, every launch of the stage-1 row-pass
+ * kernel is bracketed by CUDA events on its stream.  paco_profile_read
+ * synchronizes on them and returns totals since the last enable:
+ * out[0] = milliseconds in row passes, out[1] = launches, out[2] = bytes the
+ * launches had to read (the live row segments).  Host-thread-local use only. */
+void paco_profile_enable(int on);
+void paco_profile_read(double out[3]);
+
+/* Number of kernel launches this library has issued in the process so far. */
+unsigned long long paco_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PACO_SVD_H */

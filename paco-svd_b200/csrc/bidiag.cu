@@ -1,0 +1,751 @@
+// Stage 1: one-sided Golub-Kahan Householder upper bidiagonalization of a
+// row-major M x N FP32 matrix (M >= N), blocked in panels of NB columns,
+// followed by the explicit formation of U (M x M) and Vt (N x N).
+//
+// Reference: upper_bidiagonalization.cpp (DEAVEN-MITCH/paco-svd).  The
+// reflector convention is the reference's (:182-218): sigma = |x[1:]|^2,
+// mu = +sqrt(x0^2 + sigma), v0 = x0 - mu (x0 <= 0) else -sigma/(x0 + mu),
+// tau = 2 v0^2/(sigma + v0^2), v = x/v0 with v[0] = 1 implicit, d or e = mu;
+// sigma == 0 (or a length-1 vector) gives tau = 0 and keeps x.  The
+// reference applies each reflector to the whole trailing matrix at once
+// (:426-563, two read+write sweeps per column step); here the updates are
+// deferred within a panel (A <- A - V Y^T - X U^T, dlabrd-style blocking), so
+// each column step only reads the trailing matrix:
+//
+//   row pass (RP, row-parallel)  one TMA-staged read of every trailing row
+//       finishes X(:, i-1) = taup*(A u - corrections)   [previous row reflector]
+//       updates column i and accumulates A^T x          [this column reflector]
+//       -- the two GEMVs of a step share that single read.
+//   column pass (CP, column-parallel)
+//       reduces the A^T x partials into Y(:, i), updates row i, and
+//       accumulates the row reflector's norm and panel dot products.
+//
+// Cross-block reductions (norms, panel dots) are finished by the last block
+// to arrive (ticket counter), summing the per-block partials in block order,
+// so results are bitwise reproducible.  After each panel one GEMM applies
+// the rank-2*NB update to the trailing matrix.
+#include <vector>
+
+#include "bidiag.cuh"
+#include "gemm.cuh"
+#include "tma.cuh"
+
+using namespace bd;
+
+// ------------------------------------------------------------ small kernels
+
+__global__ void bd_copy_in(const float *__restrict__ a, float *__restrict__ W, int M, int N, long ldw,
+                           DevStatus *st)
+{
+    long total = (long)M * ldw;
+    bool bad = false;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        long r = t / ldw, c = t % ldw;
+        float v = 0.f;
+        if (c < N) {
+            v = a[r * N + c];
+            if (!isfinite(v)) { // reported, and replaced so every later step stays finite
+                bad = true;
+                v = 0.f;
+            }
+        }
+        W[t] = v;
+    }
+    if (bad) dev_fail(st, PACO_ERR_NONFINITE, 0);
+}
+
+// a <- Householder vectors with d on the diagonal and e on the superdiagonal
+__global__ void bd_copy_out(float *__restrict__ a, const float *__restrict__ W, int M, int N, long ldw,
+                            const float *d, const float *e)
+{
+    long total = (long)M * N;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        long r = t / N, c = t % N;
+        float v = W[r * ldw + c];
+        if (r == c) v = d[r];
+        else if (c == r + 1) v = e[r];
+        a[t] = v;
+    }
+}
+
+__global__ void bd_set_identity(float *Q, long n, long ld)
+{
+    long total = n * n;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        long r = t / n, c = t % n;
+        Q[r * ld + c] = (r == c) ? 1.f : 0.f;
+    }
+}
+
+__global__ void bd_transpose(const float *__restrict__ src, float *__restrict__ dst, int n)
+{
+    __shared__ float tile[32][33];
+    int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+        int r = by + y, c = bx + threadIdx.x;
+        if (r < n && c < n) tile[y][threadIdx.x] = src[(long)r * n + c];
+    }
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+        int r = bx + y, c = by + threadIdx.x;
+        if (r < n && c < n) dst[(long)r * n + c] = tile[threadIdx.x][y];
+    }
+}
+
+// scales the stored entries of the last column reflector (rows >= N)
+__global__ void bd_scale_last_col(float *W, long ldw, int M, int N, const float *inv_v0c)
+{
+    float s = inv_v0c[N - 1];
+    for (int r = N + blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x)
+        W[(long)r * ldw + N - 1] *= s;
+}
+
+// reflector of upper_bidiagonalization.cpp:182-218 from x0 and sigma = |x[1:]|^2
+__device__ __forceinline__ void make_reflector(float x0, float sigma, int len, float *beta, float *tau,
+                                               float *v0)
+{
+    if (len <= 1 || sigma == 0.f) {
+        *beta = x0; *tau = 0.f; *v0 = 1.f;
+        return;
+    }
+    float mu = sqrtf(x0 * x0 + sigma);
+    float v = (x0 <= 0.f) ? x0 - mu : -sigma / (x0 + mu);
+    *v0 = v;
+    *tau = 2.f * v * v / (sigma + v * v);
+    *beta = mu;
+}
+
+// ------------------------------------------------------------- row pass
+
+// mode bits
+#define RP_DO_X 1      // finish X(:, i-1-p0) for the row reflector of row i-1
+#define RP_DO_COL 2    // column step i: update column i, accumulate A^T x
+#define RP_PANEL_END 4 // materialize the implicit 1 of row i-1 at column i
+
+template <int CPT>
+__global__ void __launch_bounds__(RP_THREADS, 1) bd_row_pass(BdArgs a, int i, int p0, int mode, int R)
+{
+    extern __shared__ __align__(128) float tiles[];
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ float red[RP_THREADS / 32][RMAX];
+    __shared__ float xs[RMAX];
+    __shared__ float s_t3[NB + 1], s_t4[NB], s_ycol[NB], s_wcol[NB];
+    __shared__ float s_part[RMAX][PR];
+    __shared__ float s_red[PR];
+    __shared__ int s_flag;
+    __shared__ float s_v0;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int M = a.M, N = a.N;
+    const long ldw = a.ldw;
+    const bool doX = (mode & RP_DO_X) != 0, doCol = (mode & RP_DO_COL) != 0;
+    const int ii = i - p0;  // panel columns before column i
+    const int iip = ii - 1; // local index of the previous row reflector
+    const int L = (int)(ldw - p0);
+    const int G = gridDim.x;
+    const int nrows = M - i;
+    const int rpb = (nrows + G - 1) / G;
+    const int r0 = i + blockIdx.x * rpb;
+    const int r1 = min(M, r0 + rpb);
+    DevStatus *st = a.st;
+
+    // row reflector i-1 (columns i..N-1, implicit 1 at column i)
+    const float invr = doX ? a.inv_v0r[i - 1] : 0.f;
+    const float taup_prev = doX ? a.taup[i - 1] : 0.f;
+    const float invc = (ii >= 1) ? a.inv_v0c[i - 1] : 1.f;
+
+    float4 u4[CPT], acc4[CPT];
+#pragma unroll
+    for (int k = 0; k < CPT; k++) {
+        int c = p0 + 4 * (tid + k * RP_THREADS);
+        float uv[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            int j = c + e;
+            float v = 0.f;
+            if (doX) {
+                if (j == i) v = 1.f;
+                else if (j > i && j < N) v = a.rowbuf[j] * invr;
+            }
+            uv[e] = v;
+        }
+        u4[k] = make_float4(uv[0], uv[1], uv[2], uv[3]);
+        acc4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if (tid <= NB) s_t3[tid] = (doX && tid <= iip) ? a.sc->t3[tid] : 0.f;
+    if (tid < NB) {
+        s_t4[tid] = (doX && tid < iip) ? a.sc->t4[tid] : 0.f;
+        s_ycol[tid] = (doCol && tid < ii) ? a.Yt[(long)tid * ldw + i] : 0.f;
+        s_wcol[tid] = (doCol && tid < ii) ? ((tid == ii - 1) ? 1.f : a.W[(long)(p0 + tid) * ldw + i]) : 0.f;
+    }
+    for (int t = tid; t < RMAX * PR; t += RP_THREADS) (&s_part[0][0])[t] = 0.f;
+
+    // block 0 stores the scaled row reflector i-1 into row i-1 of W
+    if (doX && blockIdx.x == 0) {
+        for (int j = i + 1 + tid; j < N; j += RP_THREADS) a.W[(long)(i - 1) * ldw + j] = a.rowbuf[j] * invr;
+        if ((mode & RP_PANEL_END) && tid == 0) a.W[(long)(i - 1) * ldw + i] = 1.f;
+    }
+
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+
+    const int nbatch = (r1 > r0) ? (r1 - r0 + R - 1) / R : 0;
+    auto issue = [&](int b, int stage) {
+        int rb = r0 + b * R;
+        int nr = min(R, r1 - rb);
+        mbar_expect_tx(&bars[stage], (uint32_t)nr * L * 4u);
+        for (int rr = 0; rr < nr; rr++)
+            tma_load_1d(tiles + ((long)stage * R + rr) * L, a.W + (long)(rb + rr) * ldw + p0, (uint32_t)L * 4u,
+                        &bars[stage]);
+    };
+    if (tid == 0) {
+        if (nbatch > 0) issue(0, 0);
+        if (nbatch > 1) issue(1, 1);
+    }
+    uint32_t phase0 = 0, phase1 = 0;
+    float w_ss = 0.f, w_g1 = 0.f, w_g2 = 0.f;
+    bool failed = false;
+
+    for (int b = 0; b < nbatch; b++) {
+        const int stage = b & 1;
+        const int rb = r0 + b * R;
+        const int nr = min(R, r1 - rb);
+        bool ok = mbar_wait_bounded(&bars[stage], stage ? phase1 : phase0, st, 100 + i);
+        if (stage) phase1 ^= 1; else phase0 ^= 1;
+        if (__syncthreads_or(!ok)) { failed = true; break; }
+        const float *T = tiles + (long)stage * R * L;
+
+        // (1) A u partial dot products, one per staged row
+        if (doX) {
+            float pd[RMAX];
+#pragma unroll
+            for (int rr = 0; rr < RMAX; rr++) pd[rr] = 0.f;
+#pragma unroll
+            for (int rr = 0; rr < RMAX; rr++) {
+                if (rr < nr) {
+#pragma unroll
+                    for (int k = 0; k < CPT; k++) {
+                        int c4 = tid + k * RP_THREADS;
+                        if (4 * c4 < L) {
+                            float4 v = *reinterpret_cast<const float4 *>(T + (long)rr * L + 4 * c4);
+                            pd[rr] += v.x * u4[k].x + v.y * u4[k].y + v.z * u4[k].z + v.w * u4[k].w;
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int rr = 0; rr < RMAX; rr++) {
+                if (rr < nr) {
+                    float v = warp_sum(pd[rr]);
+                    if (lane == 0) red[warp][rr] = v;
+                }
+            }
+            __syncthreads();
+        }
+        // (2) per-row panel work: warp rr handles staged row rr
+        if (warp < nr) {
+            const int rr = warp, r = rb + rr;
+            const float *trow = T + (long)rr * L;
+            float aq = (lane < ii) ? trow[lane] : 0.f;
+            if (lane == ii - 1) {
+                aq *= invc;
+                a.W[(long)r * ldw + (i - 1)] = aq;
+            }
+            float xq = (doX && lane < iip) ? a.X[(long)r * NB + lane] : 0.f;
+            float Xn = 0.f;
+            if (doX) {
+                float dot = 0.f;
+#pragma unroll
+                for (int w2 = 0; w2 < RP_THREADS / 32; w2++) dot += red[w2][rr];
+                float s = ((lane <= iip) ? aq * s_t3[lane] : 0.f) + ((lane < iip) ? xq * s_t4[lane] : 0.f);
+                float corr = warp_sum(s);
+                Xn = taup_prev * (dot - corr);
+                if (lane == 0) a.X[(long)r * NB + iip] = Xn;
+            }
+            if (doCol) {
+                float xrq = (lane < ii - 1) ? xq : ((lane == ii - 1) ? Xn : 0.f);
+                float s = (lane < ii) ? (aq * s_ycol[lane] + xrq * s_wcol[lane]) : 0.f;
+                float xr = trow[ii] - warp_sum(s);
+                if (lane == 0) {
+                    a.W[(long)r * ldw + i] = xr;
+                    xs[rr] = xr;
+                    if (r == i) a.sc->x0col = xr;
+                }
+                if (r > i) {
+                    if (lane == 0) w_ss += xr * xr;
+                    if (lane < ii) {
+                        w_g1 += aq * xr;
+                        w_g2 += xrq * xr;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // (3) A^T x accumulation over the staged rows below the pivot
+        if (doCol) {
+#pragma unroll
+            for (int rr = 0; rr < RMAX; rr++) {
+                if (rr < nr && rb + rr > i) {
+                    float xr = xs[rr];
+#pragma unroll
+                    for (int k = 0; k < CPT; k++) {
+                        int c4 = tid + k * RP_THREADS;
+                        if (4 * c4 < L) {
+                            float4 v = *reinterpret_cast<const float4 *>(T + (long)rr * L + 4 * c4);
+                            acc4[k].x += v.x * xr; acc4[k].y += v.y * xr;
+                            acc4[k].z += v.z * xr; acc4[k].w += v.w * xr;
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && b + 2 < nbatch) {
+            proxy_async_fence();
+            issue(b + 2, stage);
+        }
+    }
+    if (failed || !doCol) return;
+
+    // block partials: A^T x (all tile columns), |x|^2, panel dots
+#pragma unroll
+    for (int k = 0; k < CPT; k++) {
+        int c4 = tid + k * RP_THREADS;
+        if (4 * c4 < L) *reinterpret_cast<float4 *>(a.ypart + (long)blockIdx.x * ldw + p0 + 4 * c4) = acc4[k];
+    }
+    if (warp < RMAX) {
+        if (lane == 0) s_part[warp][0] = w_ss;
+        s_part[warp][1 + lane] = w_g1;
+        s_part[warp][1 + NB + lane] = w_g2;
+    }
+    __syncthreads();
+    for (int t = tid; t < PR; t += RP_THREADS) {
+        float v = 0.f;
+        for (int w = 0; w < RMAX; w++) v += s_part[w][t];
+        a.tpart[(long)blockIdx.x * PR + t] = v;
+    }
+    if (!last_block_ticket(&st->counters[0], G, &s_flag)) return;
+
+    // last block: finish the column reflector and t1 = V^T v, t2 = X^T v
+    {
+        const int nval = 1 + 2 * NB;
+        const int slices = RP_THREADS / nval; // 7
+        __shared__ float s_sl[RP_THREADS];
+        int t = tid % nval, sl = tid / nval;
+        float v = 0.f;
+        if (sl < slices)
+            for (int bb = sl; bb < G; bb += slices) v += __ldcg(&a.tpart[(long)bb * PR + t]);
+        s_sl[tid] = v;
+        __syncthreads();
+        if (tid < nval) {
+            float s = 0.f;
+            for (int q = 0; q < slices; q++) s += s_sl[q * nval + tid];
+            s_red[tid] = s;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            float x0 = __ldcg(&a.sc->x0col);
+            float beta, tau, v0;
+            make_reflector(x0, s_red[0], M - i, &beta, &tau, &v0);
+            a.d[i] = beta;
+            a.tauq[i] = tau;
+            a.inv_v0c[i] = 1.f / v0;
+            s_v0 = v0;
+        }
+        __syncthreads();
+        if (tid < ii) {
+            float inv = 1.f / s_v0;
+            a.sc->t1[tid] = __ldcg(&a.W[(long)i * ldw + p0 + tid]) + s_red[1 + tid] * inv;
+            a.sc->t2[tid] = __ldcg(&a.X[(long)i * NB + tid]) + s_red[1 + NB + tid] * inv;
+        }
+    }
+}
+
+// ----------------------------------------------------------- column pass
+
+__global__ void __launch_bounds__(CP_THREADS) bd_col_pass(BdArgs a, int i, int p0, int Gr)
+{
+    __shared__ float red[CP_THREADS / 32][32];
+    __shared__ float sA[CP_THREADS / 32][32], sB[CP_THREADS / 32][32];
+    __shared__ float s_t1[NB], s_t2[NB], s_ai[NB], s_xi[NB];
+    __shared__ float s_part[PR];
+    __shared__ float s_red[PR];
+    __shared__ float s_sl[CP_THREADS];
+    __shared__ int s_flag;
+    __shared__ float s_v0;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int N = a.N;
+    const long ldw = a.ldw;
+    const int ii = i - p0;
+    const int j = i + 1 + blockIdx.x * 32 + lane;
+    const bool valid = j < N;
+    DevStatus *st = a.st;
+
+    // (1) sum the row-pass partials of A^T x for this column
+    float ys = 0.f;
+    if (valid)
+        for (int bb = warp; bb < Gr; bb += CP_THREADS / 32) ys += __ldcg(&a.ypart[(long)bb * ldw + j]);
+    red[warp][lane] = ys;
+    for (int t = tid; t < PR; t += CP_THREADS) s_part[t] = 0.f;
+    if (tid < NB) {
+        bool q = tid < ii;
+        s_t1[tid] = q ? a.sc->t1[tid] : 0.f;
+        s_t2[tid] = q ? a.sc->t2[tid] : 0.f;
+        s_ai[tid] = q ? a.W[(long)i * ldw + p0 + tid] : 0.f;
+        s_xi[tid] = q ? a.X[(long)i * NB + tid] : 0.f;
+    }
+    __syncthreads();
+
+    // (2) warp w owns panel indices q in [4w, 4w+4)
+    float Yq[4], Wq[4];
+    float pa = 0.f, pb = 0.f;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        int q = 4 * warp + e;
+        bool use = valid && q < ii;
+        Yq[e] = use ? a.Yt[(long)q * ldw + j] : 0.f;
+        Wq[e] = use ? a.W[(long)(p0 + q) * ldw + j] : 0.f;
+        if (q < NB) {
+            pa += Yq[e] * s_t1[q] + Wq[e] * s_t2[q];
+            pb += Yq[e] * s_ai[q] + Wq[e] * s_xi[q];
+        }
+    }
+    sA[warp][lane] = pa;
+    sB[warp][lane] = pb;
+    __syncthreads();
+
+    // (3) Y(j, ii) and the updated row entry a_j (every warp, same values)
+    float y = 0.f, sa = 0.f, sb = 0.f;
+#pragma unroll
+    for (int w = 0; w < CP_THREADS / 32; w++) { y += red[w][lane]; sa += sA[w][lane]; sb += sB[w][lane]; }
+    float Ynew = 0.f, aj = 0.f;
+    if (valid) {
+        float wij = a.W[(long)i * ldw + j];
+        float yj = wij + y * a.inv_v0c[i];
+        Ynew = a.tauq[i] * (yj - sa);
+        aj = wij - Ynew - sb;
+        if (warp == 0) {
+            a.Yt[(long)ii * ldw + j] = Ynew;
+            a.rowbuf[j] = aj;
+            if (j == i + 1) a.sc->x0row = aj;
+        }
+    }
+    // (4) partials of the row reflector: |a|^2, Y^T a, U a (entries j >= i+2)
+    float m = (valid && j >= i + 2) ? aj : 0.f;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        int q = 4 * warp + e;
+        if (q < ii) {
+            float g3 = warp_sum(Yq[e] * m);
+            float g4 = warp_sum(Wq[e] * m);
+            if (lane == 0) { s_part[1 + q] = g3; s_part[NB + 2 + q] = g4; }
+        }
+    }
+    if (warp == 0) {
+        float ss = warp_sum(m * m);
+        float g3 = warp_sum(Ynew * m);
+        if (lane == 0) { s_part[0] = ss; s_part[1 + ii] = g3; }
+    }
+    __syncthreads();
+    for (int t = tid; t < PR; t += CP_THREADS) a.cpart[(long)blockIdx.x * PR + t] = s_part[t];
+    if (!last_block_ticket(&st->counters[1], gridDim.x, &s_flag)) return;
+
+    // last block: row reflector of row i and t3 = Y^T u, t4 = U u
+    {
+        const int nval = 2 * NB + 2;
+        const int slices = CP_THREADS / nval; // 3
+        int t = tid % nval, sl = tid / nval;
+        float v = 0.f;
+        if (sl < slices)
+            for (int bb = sl; bb < (int)gridDim.x; bb += slices) v += __ldcg(&a.cpart[(long)bb * PR + t]);
+        s_sl[tid] = v;
+        __syncthreads();
+        if (tid < nval) {
+            float s = 0.f;
+            for (int q = 0; q < slices; q++) s += s_sl[q * nval + tid];
+            s_red[tid] = s;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            float x0 = __ldcg(&a.sc->x0row);
+            float beta, tau, v0;
+            make_reflector(x0, s_red[0], N - i - 1, &beta, &tau, &v0);
+            a.e[i] = beta;
+            a.taup[i] = tau;
+            a.inv_v0r[i] = 1.f / v0;
+            s_v0 = v0;
+        }
+        __syncthreads();
+        float inv = 1.f / s_v0;
+        if (tid <= ii) a.sc->t3[tid] = __ldcg(&a.Yt[(long)tid * ldw + i + 1]) + s_red[1 + tid] * inv;
+        if (tid < ii) a.sc->t4[tid] = __ldcg(&a.W[(long)(p0 + tid) * ldw + i + 1]) + s_red[NB + 2 + tid] * inv;
+    }
+}
+
+// ---------------------------------------------- compact-WY formation of U, V
+
+// Vp (Lp x NB, ld NB): explicit reflector panel with unit diagonal.
+//   column reflectors (U): Vp[r][q] = W[p0+r][p0+q]        (r > q)
+//   row reflectors    (V): Vp[r][q] = W[p0+q][p0+1+r]      (r > q)
+__global__ void bd_panel_vectors(const float *W, long ldw, int p0, int nbp, int Lp, int rowref, float *Vp)
+{
+    long total = (long)Lp * NB;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        int r = (int)(t / NB), q = (int)(t % NB);
+        float v = 0.f;
+        if (q < nbp) {
+            if (r == q) v = 1.f;
+            else if (r > q) v = rowref ? W[(long)(p0 + q) * ldw + p0 + 1 + r] : W[(long)(p0 + r) * ldw + p0 + q];
+        }
+        Vp[t] = v;
+    }
+}
+
+// T (NB x NB, upper triangular) of the forward block reflector
+// H_0 ... H_{nbp-1} = I - Vp T Vp^T, from the Gram matrix Vp^T Vp.
+__global__ void __launch_bounds__(256) bd_gram_t(const float *Vp, int Lp, int nbp, const float *tau, float *T,
+                                                 float *gpart, int *counter)
+{
+    __shared__ float rows[64][NB + 1];
+    __shared__ int s_flag;
+    __shared__ float G[NB][NB + 1];
+    __shared__ float Ts[NB][NB + 1];
+    __shared__ float w[NB];
+    const int tid = threadIdx.x;
+    // each thread owns 4 Gram entries (a, q) with a = tid/8*... : 1024 entries / 256
+    float g[4] = {0.f, 0.f, 0.f, 0.f};
+    const int chunk = (Lp + gridDim.x - 1) / gridDim.x;
+    const int rbeg = blockIdx.x * chunk, rend = min(Lp, rbeg + chunk);
+    for (int r0 = rbeg; r0 < rend; r0 += 64) {
+        int nr = min(64, rend - r0);
+        for (int t = tid; t < 64 * NB; t += 256) {
+            int rr = t / NB, q = t % NB;
+            rows[rr][q] = (rr < nr) ? Vp[(long)(r0 + rr) * NB + q] : 0.f;
+        }
+        __syncthreads();
+        for (int e = 0; e < 4; e++) {
+            int idx = tid + 256 * e, ga = idx / NB, gq = idx % NB;
+            float s = 0.f;
+            for (int rr = 0; rr < nr; rr++) s += rows[rr][ga] * rows[rr][gq];
+            g[e] += s;
+        }
+        __syncthreads();
+    }
+    for (int e = 0; e < 4; e++) gpart[(long)blockIdx.x * NB * NB + tid + 256 * e] = g[e];
+    if (!last_block_ticket(counter, gridDim.x, &s_flag)) return;
+    for (int e = 0; e < 4; e++) {
+        int idx = tid + 256 * e;
+        float s = 0.f;
+        for (int bb = 0; bb < (int)gridDim.x; bb++) s += __ldcg(&gpart[(long)bb * NB * NB + idx]);
+        G[idx / NB][idx % NB] = s;
+    }
+    for (int t = tid; t < NB * (NB + 1); t += 256) (&Ts[0][0])[t] = 0.f;
+    __syncthreads();
+    if (tid < 32) {
+        const int l = tid;
+        for (int q = 0; q < nbp; q++) {
+            float tq = tau[q];
+            // T[0:q, q] = -tau_q * T[0:q, 0:q] * G[0:q, q]
+            if (l < q) w[l] = G[l][q];
+            __syncwarp();
+            float s = 0.f;
+            if (l < q)
+                for (int b = l; b < q; b++) s += Ts[l][b] * w[b];
+            __syncwarp();
+            if (l < q) Ts[l][q] = -tq * s;
+            if (l == q) Ts[q][q] = tq;
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    for (int t = tid; t < NB * NB; t += 256) T[t] = Ts[t / NB][t % NB];
+}
+
+// Q_sub <- (I - Vp T Vp^T) Q_sub for Q_sub = Q[off:off+Lp, off:off+Lp] (ld ldq)
+static cudaError_t apply_block_reflector(const BdWs &w, float *Q, long ldq, long off, int Lp, int nbp,
+                                         const float *tau, cudaStream_t s)
+{
+    const int gblocks = std::max(1, std::min(RB_CAP, ceil_div(Lp, 256)));
+    paco_count_launch(), bd_gram_t<<<gblocks, 256, 0, s>>>(w.Vp, Lp, nbp, tau, w.T, w.gpart, &w.st->counters[2]);
+    float *Qs = Q + off * ldq + off;
+    // G1 = Vp^T Q_sub  (NB x Lp), split along the long k = Lp dimension
+    int splits = std::max(1, std::min(SPLITS, ceil_div(Lp, 512)));
+    cudaError_t err = gemm_run(nbp, Lp, Lp, 1.f, gop(w.Vp, 1, NB), gop(Qs, ldq, 1), 0.f, w.G1, Lp, splits,
+                               w.gscr, s);
+    if (err) return err;
+    // G2 = T G1
+    err = gemm_run(nbp, Lp, nbp, 1.f, gop(w.T, NB, 1), gop(w.G1, Lp, 1), 0.f, w.G2, Lp, 1, nullptr, s);
+    if (err) return err;
+    // Q_sub -= Vp G2
+    return gemm_run(Lp, Lp, nbp, -1.f, gop(w.Vp, NB, 1), gop(w.G2, Lp, 1), 1.f, Qs, ldq, 1, nullptr, s);
+}
+
+// ------------------------------------------------------------ host driver
+
+size_t bd_workspace_bytes(int M, int N)
+{
+    BdWs w;
+    return bd_carve(nullptr, M, N, &w);
+}
+
+static int pick_R(int L)
+{
+    long budget = 192 * 1024;
+    int R = (int)(budget / (2L * L * 4));
+    return std::max(1, std::min(RMAX, R));
+}
+
+template <int CPT>
+static void launch_rp(const BdArgs &a, int i, int p0, int mode, int G, int R, int L, cudaStream_t s)
+{
+    size_t smem = (size_t)2 * R * L * 4;
+    paco_count_launch(), bd_row_pass<CPT><<<G, RP_THREADS, smem, s>>>(a, i, p0, mode, R);
+}
+
+static void rp_launch(const BdArgs &a, int i, int p0, int mode, int G, cudaStream_t s);
+
+// ---------------------------------------------------------- kernel timing
+// Optional CUDA-event timing of every row-pass launch (the stage's dominant
+// kernel), recorded on the launching stream; read by paco_profile_read().
+namespace {
+struct RpProfile {
+    bool on = false;
+    std::vector<cudaEvent_t> ev;
+    std::vector<double> bytes;
+    size_t used = 0;
+} g_prof;
+}  // namespace
+
+void bd_profile_enable(int on)
+{
+    g_prof.on = on != 0;
+    g_prof.used = 0;
+    g_prof.bytes.clear();
+}
+
+// totals since the last enable: [0] ms in row passes, [1] launches, [2] bytes
+void bd_profile_read(double out[3])
+{
+    double ms = 0;
+    for (size_t t = 0; t + 1 < g_prof.used; t += 2) {
+        float x = 0.f;
+        cudaEventSynchronize(g_prof.ev[t + 1]);
+        cudaEventElapsedTime(&x, g_prof.ev[t], g_prof.ev[t + 1]);
+        ms += x;
+    }
+    double b = 0;
+    for (double v : g_prof.bytes) b += v;
+    out[0] = ms;
+    out[1] = (double)(g_prof.used / 2);
+    out[2] = b;
+}
+
+static cudaEvent_t prof_event()
+{
+    if (g_prof.used == g_prof.ev.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        g_prof.ev.push_back(e);
+    }
+    return g_prof.ev[g_prof.used++];
+}
+
+static void rp(const BdArgs &a, int i, int p0, int mode, int G, cudaStream_t s)
+{
+    const bool prof = g_prof.on;
+    if (prof) {
+        cudaEventRecord(prof_event(), s);
+        // bytes the pass must read: the live segment [p0, N) of every active row
+        g_prof.bytes.push_back(4.0 * (double)(a.M - i) * (double)(a.N - p0));
+    }
+    rp_launch(a, i, p0, mode, G, s);
+    if (prof) cudaEventRecord(prof_event(), s);
+}
+
+static void rp_launch(const BdArgs &a, int i, int p0, int mode, int G, cudaStream_t s)
+{
+    int L = (int)(a.ldw - p0);
+    int R = pick_R(L);
+    int chunks = ceil_div(L, 4 * RP_THREADS);
+    if (chunks <= 1) launch_rp<1>(a, i, p0, mode, G, R, L, s);
+    else if (chunks == 2) launch_rp<2>(a, i, p0, mode, G, R, L, s);
+    else launch_rp<4>(a, i, p0, mode, G, R, L, s);
+}
+
+static bool rp_attrs_set = false;
+static void set_rp_attrs()
+{
+    if (rp_attrs_set) return;
+    int maxs = 200 * 1024;
+    cudaFuncSetAttribute(bd_row_pass<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
+    cudaFuncSetAttribute(bd_row_pass<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
+    cudaFuncSetAttribute(bd_row_pass<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
+    rp_attrs_set = true;
+}
+
+int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, float *d, float *e, float *tauq,
+           float *taup, void *workspace, cudaStream_t s, int num_sms)
+{
+    BdWs w;
+    bd_carve(workspace, M, N, &w);
+    set_rp_attrs();
+    BdArgs a;
+    a.M = M; a.N = N; a.ldw = w.ldw; a.st = w.st;
+    a.W = w.W; a.Yt = w.Yt; a.X = w.X; a.ypart = w.ypart; a.tpart = w.tpart; a.cpart = w.cpart;
+    a.rowbuf = w.rowbuf; a.inv_v0c = w.inv_v0c; a.inv_v0r = w.inv_v0r; a.sc = w.sc;
+    a.d = d; a.e = e; a.tauq = tauq; a.taup = taup;
+
+    const int gmax = std::max(1, std::min(RB_CAP, num_sms));
+    auto grid_rows = [&](int rows) { return std::max(1, std::min(gmax, ceil_div(rows, RMIN_PER_BLOCK))); };
+    cudaMemsetAsync(w.st->counters, 0, sizeof(w.st->counters), s);
+    cudaMemsetAsync(w.Yt, 0, sizeof(float) * NB * w.ldw, s);
+    cudaMemsetAsync(w.X, 0, sizeof(float) * (size_t)M * NB, s);
+    paco_count_launch(), bd_copy_in<<<std::min(4096, ceil_div((long)M * w.ldw, 256)), 256, 0, s>>>(a_in, w.W, M, N, w.ldw, w.st);
+
+    for (int p0 = 0; p0 < N; p0 += NB) {
+        const int p1 = std::min(N, p0 + NB), nbp = p1 - p0;
+        for (int i = p0; i < p1; i++) {
+            int G = grid_rows(M - i);
+            int mode = RP_DO_COL | ((i > p0) ? RP_DO_X : 0);
+            rp(a, i, p0, mode, G, s);
+            if (i < N - 1) paco_count_launch(), bd_col_pass<<<ceil_div(N - i - 1, 32), CP_THREADS, 0, s>>>(a, i, p0, G);
+        }
+        if (p1 < N) {
+            rp(a, p1, p0, RP_DO_X | RP_PANEL_END, grid_rows(M - p1), s);
+            // A[p1:, p1:] -= [V | X] [Y^T ; U]
+            GemmOp A = gop(w.W + (long)p1 * w.ldw + p0, w.ldw, 1);
+            A.p2 = w.X + (long)p1 * NB; A.rs2 = NB; A.cs2 = 1; A.ksplit = nbp;
+            GemmOp B = gop(w.Yt + p1, w.ldw, 1);
+            B.p2 = w.W + (long)p0 * w.ldw + p1; B.rs2 = w.ldw; B.cs2 = 1; B.ksplit = nbp;
+            gemm_run(M - p1, N - p1, 2 * nbp, -1.f, A, B, 1.f, w.W + (long)p1 * w.ldw + p1, w.ldw, 1, nullptr, s);
+        } else if (M > N) {
+            paco_count_launch(), bd_scale_last_col<<<std::min(1024, ceil_div(M - N, 256)), 256, 0, s>>>(w.W, w.ldw, M, N, w.inv_v0c);
+        }
+    }
+
+    // U = H_0 ... H_{N-1} (backward accumulation of the column reflectors)
+    paco_count_launch(), bd_set_identity<<<std::min(8192, ceil_div((long)M * M, 256)), 256, 0, s>>>(u, M, M);
+    for (int p0 = ((N - 1) / NB) * NB; p0 >= 0; p0 -= NB) {
+        int nbp = std::min(N, p0 + NB) - p0, Lp = M - p0;
+        paco_count_launch(), bd_panel_vectors<<<std::min(4096, ceil_div((long)Lp * NB, 256)), 256, 0, s>>>(w.W, w.ldw, p0, nbp, Lp, 0,
+                                                                                       w.Vp);
+        apply_block_reflector(w, u, M, p0, Lp, nbp, tauq + p0, s);
+    }
+    // V = G_0 ... G_{N-2} (row reflectors), then Vt = V^T
+    paco_count_launch(), bd_set_identity<<<std::min(8192, ceil_div((long)N * N, 256)), 256, 0, s>>>(w.Vtmp, N, N);
+    for (int p0 = ((N - 1) / NB) * NB; p0 >= 0; p0 -= NB) {
+        int nbp = std::min(N - 1, p0 + NB) - p0, Lp = N - p0 - 1;
+        if (nbp <= 0 || Lp <= 0) continue;
+        paco_count_launch(), bd_panel_vectors<<<std::min(4096, ceil_div((long)Lp * NB, 256)), 256, 0, s>>>(w.W, w.ldw, p0, nbp, Lp, 1,
+                                                                                       w.Vp);
+        apply_block_reflector(w, w.Vtmp, N, p0 + 1, Lp, nbp, taup + p0, s);
+    }
+    paco_count_launch(), bd_transpose<<<dim3(ceil_div(N, 32), ceil_div(N, 32)), dim3(32, 8), 0, s>>>(w.Vtmp, vt, N);
+    paco_count_launch(), bd_copy_out<<<std::min(4096, ceil_div((long)M * N, 256)), 256, 0, s>>>(a_out, w.W, M, N, w.ldw, d, e);
+    return cudaGetLastError() == cudaSuccess ? PACO_OK : PACO_ERR_CUDA;
+}

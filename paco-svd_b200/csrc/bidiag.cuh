@@ -1,0 +1,96 @@
+// Stage-1 (bidiagonalization) constants, kernel arguments and workspace layout.
+#pragma once
+
+#include "common.cuh"
+
+namespace bd {
+constexpr int NB = 32;             // panel width (reflectors per block update)
+constexpr int RP_THREADS = 512;    // row-pass CTA size
+constexpr int CP_THREADS = 256;    // column-pass CTA size (32 columns x 8 warps)
+constexpr int RMAX = 8;            // max rows staged per TMA batch
+constexpr int RB_CAP = 256;        // max row-pass CTAs (partial records)
+constexpr int CB_CAP = 512;        // max column-pass CTAs (N/32)
+constexpr int PR = 2 * NB + 8;     // floats per partial record
+constexpr int RMIN_PER_BLOCK = 16; // fewest rows a row-pass CTA is given
+constexpr int SPLITS = 8;          // split-K factor cap for the skinny V^T Q products
+}  // namespace bd
+
+struct StepScal {
+    float t1[bd::NB];     // V_panel^T v        (column step)
+    float t2[bd::NB];     // X_panel^T v
+    float t3[bd::NB + 1]; // Y_panel^T u        (row step)
+    float t4[bd::NB];     // U_panel u
+    float x0col, x0row;   // pivots of the current reflectors
+    float pad[5];
+};
+
+struct BdArgs {
+    int M, N;
+    long ldw;
+    DevStatus *st;
+    float *W, *Yt, *X, *ypart, *tpart, *cpart, *rowbuf, *inv_v0c, *inv_v0r;
+    StepScal *sc;
+    float *d, *e, *tauq, *taup;
+};
+
+struct BdWs {
+    DevStatus *st;
+    long ldw;
+    float *W;      // M x ldw   working copy of A (row stride padded to 32 floats)
+    float *Yt;     // NB x ldw  Y^T of the current panel
+    float *X;      // M x NB    X of the current panel
+    float *ypart;  // RB_CAP x ldw  per-CTA partial A^T x
+    float *tpart;  // RB_CAP x PR
+    float *cpart;  // CB_CAP x PR
+    float *rowbuf; // ldw       updated pivot row
+    float *inv_v0c, *inv_v0r; // N each: 1/v0 of every reflector
+    StepScal *sc;
+    float *Vp;     // max(M,N) x NB  explicit reflector panel
+    float *T;      // NB x NB
+    float *gpart;  // RB_CAP x NB*NB
+    float *G1, *G2;// NB x max(M,N)
+    float *gscr;   // SPLITS x NB x max(M,N)
+    float *Vtmp;   // N x N  (V before the transpose into vt)
+};
+
+// Lays the stage-1 buffers out in `base` (may be null to only measure);
+// returns the bytes used.  The DevStatus block comes first.
+static inline size_t bd_carve(void *base, int M, int N, BdWs *w)
+{
+    using namespace bd;
+    size_t off = 0;
+    auto take = [&](size_t bytes) -> char * {
+        off = (off + 255) & ~(size_t)255;
+        char *p = base ? (char *)base + off : nullptr;
+        off += bytes;
+        return p;
+    };
+    const long ldw = round_up(N, 32);
+    const long mx = std::max(M, N);
+    w->ldw = ldw;
+    w->st = (DevStatus *)take(sizeof(DevStatus));
+    w->W = (float *)take(sizeof(float) * (size_t)M * ldw);
+    w->Yt = (float *)take(sizeof(float) * (size_t)NB * ldw);
+    w->X = (float *)take(sizeof(float) * (size_t)M * NB);
+    w->ypart = (float *)take(sizeof(float) * (size_t)RB_CAP * ldw);
+    w->tpart = (float *)take(sizeof(float) * (size_t)RB_CAP * PR);
+    w->cpart = (float *)take(sizeof(float) * (size_t)CB_CAP * PR);
+    w->rowbuf = (float *)take(sizeof(float) * ldw);
+    w->inv_v0c = (float *)take(sizeof(float) * N);
+    w->inv_v0r = (float *)take(sizeof(float) * N);
+    w->sc = (StepScal *)take(sizeof(StepScal));
+    w->Vp = (float *)take(sizeof(float) * (size_t)mx * NB);
+    w->T = (float *)take(sizeof(float) * NB * NB);
+    w->gpart = (float *)take(sizeof(float) * (size_t)RB_CAP * NB * NB);
+    w->G1 = (float *)take(sizeof(float) * (size_t)NB * mx);
+    w->G2 = (float *)take(sizeof(float) * (size_t)NB * mx);
+    w->gscr = (float *)take(sizeof(float) * (size_t)SPLITS * NB * mx);
+    w->Vtmp = (float *)take(sizeof(float) * (size_t)N * N);
+    return (off + 255) & ~(size_t)255;
+}
+
+size_t bd_workspace_bytes(int M, int N);
+void bd_profile_enable(int on);
+void bd_profile_read(double out[3]);
+int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, float *d, float *e, float *tauq,
+           float *taup, void *workspace, cudaStream_t s, int num_sms);

@@ -1,0 +1,227 @@
+// C ABI of libpacosvd.so (declared in include/paco_svd.h).
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "bdc.cuh"
+#include "bidiag.cuh"
+
+namespace {
+
+int device_sms()
+{
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms > 0 ? sms : 148;
+}
+
+bool shape_ok(int M, int N) { return N >= 1 && M >= N && N <= PACO_MAX_N && (long)M * M < (1L << 40); }
+
+
+struct SvdLayout {
+    size_t ws, e, tauq, taup, qt, wt, idx, total;
+};
+
+SvdLayout svd_layout(int M, int N)
+{
+    SvdLayout L;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        off = (off + 255) & ~(size_t)255;
+        size_t p = off;
+        off += bytes;
+        return p;
+    };
+    const size_t nn = (size_t)N * N;
+    L.ws = take(std::max(bd_workspace_bytes(M, N), bdc_workspace_bytes(M, N)));
+    L.e = take(sizeof(float) * N);
+    L.tauq = take(sizeof(float) * N);
+    L.taup = take(sizeof(float) * N);
+    L.qt = take(sizeof(float) * 2 * nn);
+    L.wt = take(sizeof(float) * 2 * nn);
+    L.idx = take(sizeof(uint32_t) * 16 * (size_t)N);
+    L.total = (off + 255) & ~(size_t)255;
+    return L;
+}
+
+} // namespace
+
+static unsigned long long g_launches = 0;
+void paco_count_launch() { g_launches++; }
+
+extern "C" {
+
+unsigned long long paco_launch_count(void) { return g_launches; }
+
+const char *paco_version(void) { return "paco-svd-b200 1.0 (sm_100a)"; }
+
+void paco_profile_enable(int on) { bd_profile_enable(on); }
+
+void paco_profile_read(double out[3])
+{
+    if (out) bd_profile_read(out);
+}
+
+int getTilingSize(int N, int svdBlockNum)
+{
+    (void)svdBlockNum;
+    if (N <= 0) return (int)sizeof(TilingHeader);
+    return (int)sizeof(TilingHeader) + 8 * leaf_partition(N, nullptr, nullptr);
+}
+
+void GenerateTiling(int N, int blockDim, uint8_t *TilingHost)
+{
+    (void)blockDim;
+    if (!TilingHost || N <= 0) return;
+    TilingHeader h;
+    memset(&h, 0, sizeof(h));
+    h.magic = PACO_TILING_MAGIC;
+    h.N = (uint32_t)N;
+    h.nleaf = (uint32_t)leaf_partition(N, nullptr, nullptr);
+    h.offset = sizeof(TilingHeader);
+    h.version = 1;
+    memcpy(TilingHost, &h, sizeof(h));
+    int *s = (int *)malloc(sizeof(int) * h.nleaf), *e = (int *)malloc(sizeof(int) * h.nleaf);
+    leaf_partition(N, s, e);
+    uint32_t *lv = (uint32_t *)(TilingHost + sizeof(TilingHeader));
+    for (uint32_t t = 0; t < h.nleaf; t++) { lv[2 * t] = (uint32_t)s[t]; lv[2 * t + 1] = (uint32_t)e[t]; }
+    free(s);
+    free(e);
+}
+
+size_t paco_workspace_size(int M, int N)
+{
+    if (!shape_ok(M, N)) return 0;
+    return std::max(bd_workspace_bytes(M, N), bdc_workspace_bytes(M, N));
+}
+
+void paco_buffer_sizes(int M, int N, size_t out[12])
+{
+    if (!out) return;
+    size_t m = M > 0 ? M : 0, n = N > 0 ? N : 0;
+    out[0] = m * m * 4; out[1] = m * n * 4; out[2] = n * n * 4; out[3] = n * 4;
+    out[4] = n > 0 ? (n - 1) * 4 : 0; out[5] = n * 4; out[6] = n > 0 ? (n - 1) * 4 : 0;
+    out[7] = 2 * n * n * 4; out[8] = 2 * n * n * 4; out[9] = (size_t)getTilingSize(N, 1);
+    out[10] = 16 * n * 4; out[11] = paco_workspace_size(M, N);
+}
+
+int upper_bidiagonalization(int M, int N, float *a, float *u, float *vt, float *d, float *e, float *tauq,
+                            float *taup, void *workspace, void *stream)
+{
+    if (!shape_ok(M, N)) return (N >= 1 && M >= N) ? PACO_ERR_UNSUPPORTED : PACO_ERR_INVALID_ARG;
+    if (!a || !u || !vt || !d || !tauq || !workspace || (N > 1 && (!e || !taup))) return PACO_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    // a new factorization starts: clear the device status block
+    if (cudaMemsetAsync(workspace, 0, sizeof(DevStatus), s) != cudaSuccess) return PACO_ERR_CUDA;
+    return bd_run(M, N, a, a, u, vt, d, e, tauq, taup, workspace, s, device_sms());
+}
+
+int svd_DC(int M, int N, float *a, float *u, float *vt, float *d, float *e, float *qt, float *wt, uint32_t *idx,
+           void *workspace, const uint8_t *tiling, void *stream)
+{
+    if (!shape_ok(M, N)) return (N >= 1 && M >= N) ? PACO_ERR_UNSUPPORTED : PACO_ERR_INVALID_ARG;
+    if (!a || !u || !vt || !d || !qt || !wt || !idx || !workspace || (N > 1 && !e)) return PACO_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaMemsetAsync((char *)workspace + offsetof(DevStatus, counters), 0, sizeof(((DevStatus *)0)->counters),
+                        s) != cudaSuccess)
+        return PACO_ERR_CUDA;
+    return bdc_run(M, N, a, u, vt, d, e, qt, wt, idx, workspace, tiling, s);
+}
+
+int paco_sync_status(void *workspace, void *stream, int *info)
+{
+    if (!workspace) return PACO_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) {
+        if (info) *info = (int)err;
+        return PACO_ERR_CUDA;
+    }
+    DevStatus st;
+    if (cudaMemcpy(&st, workspace, sizeof(int) * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return PACO_ERR_CUDA;
+    int zero[4] = {0, 0, 0, 0};
+    cudaMemcpy(workspace, zero, sizeof(zero), cudaMemcpyHostToDevice);
+    if (info) *info = st.code ? st.info : st.secular_nonconv;
+    if (st.code) return st.code;
+    if (st.secular_nonconv) return PACO_ERR_NONCONVERGENCE;
+    return PACO_OK;
+}
+
+size_t paco_svd_workspace_size(int M, int N)
+{
+    if (!shape_ok(M, N)) return 0;
+    return svd_layout(M, N).total;
+}
+
+int paco_svd(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws, size_t ws_bytes, void *stream)
+{
+    if (!shape_ok(M, N)) return (N >= 1 && M >= N) ? PACO_ERR_UNSUPPORTED : PACO_ERR_INVALID_ARG;
+    if (!A || !U || !Vt || !sigma || !ws) return PACO_ERR_INVALID_ARG;
+    SvdLayout L = svd_layout(M, N);
+    if (ws_bytes < L.total) return PACO_ERR_INVALID_ARG;
+    char *b = (char *)ws;
+    float *e = (float *)(b + L.e), *tq = (float *)(b + L.tauq), *tp = (float *)(b + L.taup);
+    int rc = upper_bidiagonalization(M, N, A, U, Vt, sigma, e, tq, tp, b + L.ws, stream);
+    if (rc) return rc;
+    return svd_DC(M, N, A, U, Vt, sigma, e, (float *)(b + L.qt), (float *)(b + L.wt), (uint32_t *)(b + L.idx),
+                  b + L.ws, nullptr, stream);
+}
+
+struct paco_ctx {
+    int M, N;
+    float *A, *U, *Vt, *sigma;
+    void *ws;
+    size_t ws_bytes;
+    cudaStream_t stream;
+};
+
+int paco_ctx_create(int M, int N, paco_ctx **out)
+{
+    if (!out) return PACO_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (!shape_ok(M, N)) return (N >= 1 && M >= N) ? PACO_ERR_UNSUPPORTED : PACO_ERR_INVALID_ARG;
+    paco_ctx *c = (paco_ctx *)calloc(1, sizeof(paco_ctx));
+    c->M = M; c->N = N;
+    c->ws_bytes = paco_svd_workspace_size(M, N);
+    cudaError_t err = cudaSuccess;
+    err = err ? err : cudaMalloc(&c->A, sizeof(float) * (size_t)M * N);
+    err = err ? err : cudaMalloc(&c->U, sizeof(float) * (size_t)M * M);
+    err = err ? err : cudaMalloc(&c->Vt, sizeof(float) * (size_t)N * N);
+    err = err ? err : cudaMalloc(&c->sigma, sizeof(float) * N);
+    err = err ? err : cudaMalloc(&c->ws, c->ws_bytes);
+    err = err ? err : cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (err != cudaSuccess) {
+        paco_ctx_destroy(c);
+        return PACO_ERR_CUDA;
+    }
+    *out = c;
+    return PACO_OK;
+}
+
+int paco_ctx_svd_host(paco_ctx *c, const float *A, float *U, float *Vt, float *sigma)
+{
+    if (!c || !A) return PACO_ERR_INVALID_ARG;
+    const int M = c->M, N = c->N;
+    cudaStream_t s = c->stream;
+    if (cudaMemcpyAsync(c->A, A, sizeof(float) * (size_t)M * N, cudaMemcpyHostToDevice, s)) return PACO_ERR_CUDA;
+    int rc = paco_svd(M, N, c->A, c->U, c->Vt, c->sigma, c->ws, c->ws_bytes, s);
+    if (rc) return rc;
+    if (U && cudaMemcpyAsync(U, c->U, sizeof(float) * (size_t)M * M, cudaMemcpyDeviceToHost, s)) return PACO_ERR_CUDA;
+    if (Vt && cudaMemcpyAsync(Vt, c->Vt, sizeof(float) * (size_t)N * N, cudaMemcpyDeviceToHost, s))
+        return PACO_ERR_CUDA;
+    if (sigma && cudaMemcpyAsync(sigma, c->sigma, sizeof(float) * N, cudaMemcpyDeviceToHost, s)) return PACO_ERR_CUDA;
+    SvdLayout L = svd_layout(M, N);
+    int info = 0;
+    return paco_sync_status((char *)c->ws + L.ws, s, &info);
+}
+
+void paco_ctx_destroy(paco_ctx *c)
+{
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    cudaFree(c->A); cudaFree(c->U); cudaFree(c->Vt); cudaFree(c->sigma); cudaFree(c->ws);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    free(c);
+}
+
+} // extern "C"

@@ -1,0 +1,67 @@
+// Shared definitions for the sm_100a kernels of the paco-svd B200 library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "../../include/paco_svd.h"
+
+#define PACO_WARP 32
+
+// Device-side status block, the first bytes of every workspace.  Kernels never
+// trap: they record what went wrong here and return, so the context stays
+// usable and the host reads the cause after a synchronize.
+struct DevStatus {
+    int code;            // first fatal error code (PACO_ERR_*), 0 if none
+    int info;            // detail for `code` (kernel-specific)
+    int secular_nonconv; // secular roots that hit the iteration limit
+    int wait_timeouts;   // bounded waits that gave up
+    int counters[60];    // arrival tickets for last-block reductions
+};
+
+__device__ __forceinline__ void dev_fail(DevStatus *st, int code, int info)
+{
+    if (atomicCAS(&st->code, 0, code) == 0) st->info = info;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_max(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Last-block-done ticket: every block calls this once after writing its
+// partial results; exactly one block (the last to arrive) gets `true` and may
+// then read every other block's partials.  The counter is reset for reuse.
+__device__ __forceinline__ bool last_block_ticket(int *counter, int nblocks, int *s_flag)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        int t = atomicAdd(counter, 1);
+        *s_flag = (t == nblocks - 1);
+        if (*s_flag) atomicExch(counter, 0);
+    }
+    __syncthreads();
+    bool last = *s_flag != 0;
+    if (last) __threadfence();
+    return last;
+}
+
+// Host-side count of kernel launches issued by the library (paco_launch_count).
+void paco_count_launch();
+
+static inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
+static inline long round_up(long a, long b) { return (a + b - 1) / b * b; }

@@ -1,0 +1,103 @@
+"""CPU tests of the C ABI library: it loads, exports every entry point that
+include/paco_svd.h declares, and its host-side logic (tiling blob, buffer
+sizes, argument validation, the svd_main CLI's argument handling) behaves as
+the reference's host code does.  No kernel runs here."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as O
+import pacosvd as P
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "paco_svd.h")
+PKG = os.path.join(ROOT, "paco-svd_b200")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"^[A-Za-z_][\w\s\*]*?\b(\w+)\s*\(", src, flags=re.M)
+    return sorted(set(n for n in names if n not in ("if", "defined")))
+
+
+def test_header_declares_the_reference_entry_points():
+    names = declared_functions()
+    for ref in ("upper_bidiagonalization", "svd_DC", "getTilingSize", "GenerateTiling"):
+        assert ref in names
+
+
+@pytest.mark.parametrize("name", declared_functions())
+def test_library_exports_declared_symbol(name):
+    L = ctypes.CDLL(P.LIB_PATH)
+    assert hasattr(L, name), f"{name} declared in paco_svd.h but not exported"
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 6, 7, 8, 9, 31, 32, 33, 100, 4096])
+def test_tiling_blob_holds_the_reference_leaf_partition(N):
+    blob = P.generate_tiling(N)
+    assert len(blob) == P.tiling_size(N)
+    hdr = np.frombuffer(blob[:32], np.uint32)
+    assert hdr[0] == 0x4F434150 and hdr[1] == N and hdr[3] == 32
+    leaves = np.frombuffer(blob[32:], np.uint32).reshape(-1, 2)
+    assert hdr[2] == len(leaves)
+    assert [tuple(map(int, x)) for x in leaves] == O.leaf_partition(N)
+
+
+def test_buffer_sizes_follow_main_cpp():
+    M, N = 64, 32
+    b = P.buffer_sizes(M, N)
+    # main.cpp:33-43
+    assert b["U"] == M * M * 4 and b["A"] == M * N * 4 and b["Vt"] == N * N * 4
+    assert b["d"] == N * 4 and b["e"] == (N - 1) * 4 and b["tauq"] == N * 4 and b["taup"] == (N - 1) * 4
+    assert b["qt"] == 2 * N * N * 4 and b["wt"] == 2 * N * N * 4 and b["idx"] == 16 * N * 4
+    assert b["workspace"] > 0 and b["tiling"] == P.tiling_size(N)
+
+
+def test_workspace_size_rejects_bad_shapes():
+    assert P.workspace_size(4, 8) == 0          # M < N
+    assert P.workspace_size(10, 0) == 0         # N = 0
+    assert P.workspace_size(10000, P.PACO_MAX_N + 1) == 0
+    assert P.workspace_size(64, 32) > 0
+
+
+def test_entry_points_validate_before_touching_the_device():
+    L = P.lib()
+    nul = None
+    # M < N (main.cpp:25-29 rejects it)
+    assert L.upper_bidiagonalization(4, 8, *([nul] * 9)) == P.PACO_ERR_INVALID_ARG
+    assert L.svd_DC(4, 8, *([nul] * 11)) == P.PACO_ERR_INVALID_ARG
+    # N beyond the stage-1 limit
+    assert L.upper_bidiagonalization(9000, 9000, *([nul] * 9)) == P.PACO_ERR_UNSUPPORTED
+    # valid shape, missing buffers
+    assert L.upper_bidiagonalization(64, 32, *([nul] * 9)) == P.PACO_ERR_INVALID_ARG
+    assert L.svd_DC(64, 32, *([nul] * 11)) == P.PACO_ERR_INVALID_ARG
+    assert L.paco_svd(64, 32, *([nul] * 4), nul, 0, nul) == P.PACO_ERR_INVALID_ARG
+    h = ctypes.c_void_p()
+    assert L.paco_ctx_create(3, 5, ctypes.byref(h)) == P.PACO_ERR_INVALID_ARG
+
+
+def test_version_string():
+    assert b"sm_100a" in P.lib().paco_version()
+
+
+def test_svd_main_rejects_wide_matrix(tmp_path):
+    exe = os.path.join(PKG, "svd_main")
+    (tmp_path / "args.txt").write_text("3 5")
+    r = subprocess.run([exe, "--args", str(tmp_path / "args.txt"), "--input", str(tmp_path / "A.bin"),
+                        "--output", str(tmp_path / "out")], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1
+    assert "M must be greater than N" in r.stderr
+
+
+def test_svd_main_reports_short_input(tmp_path):
+    exe = os.path.join(PKG, "svd_main")
+    (tmp_path / "args.txt").write_text("8 4")
+    np.zeros(5, np.float32).tofile(tmp_path / "A.bin")
+    r = subprocess.run([exe, "--args", str(tmp_path / "args.txt"), "--input", str(tmp_path / "A.bin"),
+                        "--output", str(tmp_path / "out")], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "expected" in r.stderr
