@@ -108,7 +108,8 @@ const char *paco_version(void);
 void paco_profile_enable(int on);
 void paco_profile_read(double out[3]);
 
-/* Number of kernel launches this library has issued in the process so far. */
+/* Number of kernels this library has launched in the process so far (a
+ * replay of a recorded CUDA graph counts the kernels the graph holds). */
 unsigned long long paco_launch_count(void);
 
 #ifdef __cplusplus

@@ -697,15 +697,20 @@ size_t bdc_workspace_bytes(int M, int N)
 
 static bool bdc_attrs_set = false;
 
+void bdc_init_attrs()
+{
+    if (!bdc_attrs_set) {
+        cudaFuncSetAttribute(bdc_prepare, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        bdc_attrs_set = true;
+    }
+}
+
 int bdc_run(int M, int N, float *a, float *u, float *vt, float *d, float *e, float *qt, float *wt, uint32_t *idx,
             void *workspace, const uint8_t *tiling, cudaStream_t s)
 {
     BdcWs w;
     bdc_carve(workspace, M, N, &w);
-    if (!bdc_attrs_set) {
-        cudaFuncSetAttribute(bdc_prepare, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        bdc_attrs_set = true;
-    }
+    bdc_init_attrs();
     std::vector<HostLevel> lv;
     const int nleaf = host_schedule(N, lv);
     LevelArgs A;

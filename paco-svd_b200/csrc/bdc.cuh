@@ -87,5 +87,6 @@ __host__ __device__ inline int leaf_partition(int N, int *starts, int *ends)
 }
 
 size_t bdc_workspace_bytes(int M, int N);
+void bdc_init_attrs();
 int bdc_run(int M, int N, float *a, float *u, float *vt, float *d, float *e, float *qt, float *wt, uint32_t *idx,
             void *workspace, const uint8_t *tiling, cudaStream_t s);

@@ -611,60 +611,126 @@ static void rp_launch(const BdArgs &a, int i, int p0, int mode, int G, cudaStrea
 
 // ---------------------------------------------------------- kernel timing
 // Optional CUDA-event timing of every row-pass launch (the stage's dominant
-// kernel), recorded on the launching stream; read by paco_profile_read().
+// kernel), recorded on the launching stream.  The events of one stage-1 run
+// form a "run"; a run issued directly is read once, a run captured into a CUDA
+// graph is re-recorded by every replay of that graph (read after each replay).
 namespace {
+struct ProfRun {
+    std::vector<cudaEvent_t> ev; // start/end pairs
+    std::vector<double> bytes;   // bytes each launch had to read
+};
 struct RpProfile {
     bool on = false;
-    std::vector<cudaEvent_t> ev;
-    std::vector<double> bytes;
-    size_t used = 0;
+    bool capturing = false;
+    std::vector<cudaEvent_t> free_ev;
+    ProfRun cur;
+    std::vector<ProfRun> graph_runs;          // owned by captured graphs
+    std::vector<std::pair<int, bool>> pending; // (run id, direct?) awaiting a read
+    std::vector<ProfRun> direct_runs;
+    double ms = 0, launches = 0, bytes = 0;
 } g_prof;
+
+cudaEvent_t prof_event()
+{
+    if (!g_prof.free_ev.empty()) {
+        cudaEvent_t e = g_prof.free_ev.back();
+        g_prof.free_ev.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+void prof_record(cudaEvent_t e, cudaStream_t s)
+{
+    if (g_prof.capturing) cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+    else cudaEventRecord(e, s);
+}
 }  // namespace
 
 void bd_profile_enable(int on)
 {
     g_prof.on = on != 0;
-    g_prof.used = 0;
-    g_prof.bytes.clear();
+    g_prof.ms = g_prof.launches = g_prof.bytes = 0;
+    for (auto &p : g_prof.pending)
+        if (p.second)
+            for (cudaEvent_t e : g_prof.direct_runs[p.first].ev) g_prof.free_ev.push_back(e);
+    g_prof.pending.clear();
+    g_prof.direct_runs.clear();
+}
+
+// opens a stage-1 run (called by bd_run)
+static void prof_begin(cudaStream_t s)
+{
+    g_prof.cur = ProfRun();
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &cs);
+    g_prof.capturing = (cs == cudaStreamCaptureStatusActive);
+}
+
+// closes the run: a captured run is kept for its graph, a direct run is queued
+static void prof_end()
+{
+    if (!g_prof.on) return;
+    if (g_prof.capturing) {
+        g_prof.graph_runs.push_back(std::move(g_prof.cur));
+    } else {
+        g_prof.direct_runs.push_back(std::move(g_prof.cur));
+        g_prof.pending.push_back({(int)g_prof.direct_runs.size() - 1, true});
+    }
+    g_prof.capturing = false;
+}
+
+// id of the run captured last (-1 if none), for the graph cache
+int bd_profile_last_graph_run() { return (int)g_prof.graph_runs.size() - 1; }
+
+// a replay of a graph holding run `id` was launched
+void bd_profile_replayed(int id)
+{
+    if (g_prof.on && id >= 0) g_prof.pending.push_back({id, false});
 }
 
 // totals since the last enable: [0] ms in row passes, [1] launches, [2] bytes
 void bd_profile_read(double out[3])
 {
-    double ms = 0;
-    for (size_t t = 0; t + 1 < g_prof.used; t += 2) {
-        float x = 0.f;
-        cudaEventSynchronize(g_prof.ev[t + 1]);
-        cudaEventElapsedTime(&x, g_prof.ev[t], g_prof.ev[t + 1]);
-        ms += x;
+    for (auto &p : g_prof.pending) {
+        ProfRun &r = p.second ? g_prof.direct_runs[p.first] : g_prof.graph_runs[p.first];
+        for (size_t t = 0; t + 1 < r.ev.size(); t += 2) {
+            float x = 0.f;
+            cudaEventSynchronize(r.ev[t + 1]);
+            cudaEventElapsedTime(&x, r.ev[t], r.ev[t + 1]);
+            g_prof.ms += x;
+        }
+        for (double v : r.bytes) g_prof.bytes += v;
+        g_prof.launches += (double)(r.ev.size() / 2);
+        if (p.second) {
+            for (cudaEvent_t e : r.ev) g_prof.free_ev.push_back(e);
+            r.ev.clear();
+        }
     }
-    double b = 0;
-    for (double v : g_prof.bytes) b += v;
-    out[0] = ms;
-    out[1] = (double)(g_prof.used / 2);
-    out[2] = b;
-}
-
-static cudaEvent_t prof_event()
-{
-    if (g_prof.used == g_prof.ev.size()) {
-        cudaEvent_t e;
-        cudaEventCreate(&e);
-        g_prof.ev.push_back(e);
-    }
-    return g_prof.ev[g_prof.used++];
+    g_prof.pending.clear();
+    out[0] = g_prof.ms;
+    out[1] = g_prof.launches;
+    out[2] = g_prof.bytes;
 }
 
 static void rp(const BdArgs &a, int i, int p0, int mode, int G, cudaStream_t s)
 {
     const bool prof = g_prof.on;
     if (prof) {
-        cudaEventRecord(prof_event(), s);
+        cudaEvent_t e = prof_event();
+        prof_record(e, s);
+        g_prof.cur.ev.push_back(e);
         // bytes the pass must read: the live segment [p0, N) of every active row
-        g_prof.bytes.push_back(4.0 * (double)(a.M - i) * (double)(a.N - p0));
+        g_prof.cur.bytes.push_back(4.0 * (double)(a.M - i) * (double)(a.N - p0));
     }
     rp_launch(a, i, p0, mode, G, s);
-    if (prof) cudaEventRecord(prof_event(), s);
+    if (prof) {
+        cudaEvent_t e = prof_event();
+        prof_record(e, s);
+        g_prof.cur.ev.push_back(e);
+    }
 }
 
 static void rp_launch(const BdArgs &a, int i, int p0, int mode, int G, cudaStream_t s)
@@ -678,7 +744,7 @@ static void rp_launch(const BdArgs &a, int i, int p0, int mode, int G, cudaStrea
 }
 
 static bool rp_attrs_set = false;
-static void set_rp_attrs()
+void bd_init_attrs()
 {
     if (rp_attrs_set) return;
     int maxs = 200 * 1024;
@@ -693,7 +759,8 @@ int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, f
 {
     BdWs w;
     bd_carve(workspace, M, N, &w);
-    set_rp_attrs();
+    bd_init_attrs();
+    prof_begin(s);
     BdArgs a;
     a.M = M; a.N = N; a.ldw = w.ldw; a.st = w.st;
     a.W = w.W; a.Yt = w.Yt; a.X = w.X; a.ypart = w.ypart; a.tpart = w.tpart; a.cpart = w.cpart;
@@ -746,6 +813,7 @@ int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, f
         apply_block_reflector(w, w.Vtmp, N, p0 + 1, Lp, nbp, taup + p0, s);
     }
     paco_count_launch(), bd_transpose<<<dim3(ceil_div(N, 32), ceil_div(N, 32)), dim3(32, 8), 0, s>>>(w.Vtmp, vt, N);
+    prof_end();
     paco_count_launch(), bd_copy_out<<<std::min(4096, ceil_div((long)M * N, 256)), 256, 0, s>>>(a_out, w.W, M, N, w.ldw, d, e);
     return cudaGetLastError() == cudaSuccess ? PACO_OK : PACO_ERR_CUDA;
 }

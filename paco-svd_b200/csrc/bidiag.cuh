@@ -92,5 +92,8 @@ static inline size_t bd_carve(void *base, int M, int N, BdWs *w)
 size_t bd_workspace_bytes(int M, int N);
 void bd_profile_enable(int on);
 void bd_profile_read(double out[3]);
+int bd_profile_last_graph_run();
+void bd_profile_replayed(int id);
+void bd_init_attrs();
 int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, float *d, float *e, float *tauq,
            float *taup, void *workspace, cudaStream_t s, int num_sms);

@@ -2,6 +2,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 
 #include "bdc.cuh"
 #include "bidiag.cuh"
@@ -47,6 +48,7 @@ SvdLayout svd_layout(int M, int N)
 } // namespace
 
 static unsigned long long g_launches = 0;
+static int g_prof_on = 0;
 void paco_count_launch() { g_launches++; }
 
 extern "C" {
@@ -55,7 +57,11 @@ unsigned long long paco_launch_count(void) { return g_launches; }
 
 const char *paco_version(void) { return "paco-svd-b200 1.0 (sm_100a)"; }
 
-void paco_profile_enable(int on) { bd_profile_enable(on); }
+void paco_profile_enable(int on)
+{
+    g_prof_on = on != 0;
+    bd_profile_enable(on);
+}
 
 void paco_profile_read(double out[3])
 {
@@ -153,6 +159,41 @@ size_t paco_svd_workspace_size(int M, int N)
     return svd_layout(M, N).total;
 }
 
+static int svd_direct(int M, int N, float *A, float *U, float *Vt, float *sigma, char *b, const SvdLayout &L,
+                      void *stream)
+{
+    float *e = (float *)(b + L.e), *tq = (float *)(b + L.tauq), *tp = (float *)(b + L.taup);
+    int rc = upper_bidiagonalization(M, N, A, U, Vt, sigma, e, tq, tp, b + L.ws, stream);
+    if (rc) return rc;
+    return svd_DC(M, N, A, U, Vt, sigma, e, (float *)(b + L.qt), (float *)(b + L.wt), (uint32_t *)(b + L.idx),
+                  b + L.ws, nullptr, stream);
+}
+
+// The one-shot path issues thousands of small launches per SVD; on a
+// capturable stream it is recorded once into a CUDA graph per (shape,
+// buffers, stream) and replayed with a single cudaGraphLaunch afterwards.
+// PACO_GRAPHS=0 in the environment turns this off.
+namespace {
+struct GraphEntry {
+    int M, N, prof;
+    void *A, *U, *Vt, *sigma, *ws;
+    cudaStream_t s;
+    cudaGraphExec_t exec;
+    int prof_run;
+    unsigned long long kernels; // kernel launches recorded into the graph
+};
+std::vector<GraphEntry> g_graphs;
+bool graphs_enabled()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *v = getenv("PACO_GRAPHS");
+        on = !(v && v[0] == '0');
+    }
+    return on != 0;
+}
+}  // namespace
+
 int paco_svd(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws, size_t ws_bytes, void *stream)
 {
     if (!shape_ok(M, N)) return (N >= 1 && M >= N) ? PACO_ERR_UNSUPPORTED : PACO_ERR_INVALID_ARG;
@@ -160,11 +201,56 @@ int paco_svd(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws
     SvdLayout L = svd_layout(M, N);
     if (ws_bytes < L.total) return PACO_ERR_INVALID_ARG;
     char *b = (char *)ws;
-    float *e = (float *)(b + L.e), *tq = (float *)(b + L.tauq), *tp = (float *)(b + L.taup);
-    int rc = upper_bidiagonalization(M, N, A, U, Vt, sigma, e, tq, tp, b + L.ws, stream);
-    if (rc) return rc;
-    return svd_DC(M, N, A, U, Vt, sigma, e, (float *)(b + L.qt), (float *)(b + L.wt), (uint32_t *)(b + L.idx),
-                  b + L.ws, nullptr, stream);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (!graphs_enabled() || s == nullptr || s == cudaStreamLegacy || s == cudaStreamPerThread ||
+        cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+        return svd_direct(M, N, A, U, Vt, sigma, b, L, stream);
+    for (GraphEntry &g : g_graphs) {
+        if (g.M == M && g.N == N && g.A == A && g.U == U && g.Vt == Vt && g.sigma == sigma && g.ws == ws &&
+            g.s == s && g.prof == g_prof_on) {
+            if (cudaGraphLaunch(g.exec, s) != cudaSuccess) return PACO_ERR_CUDA;
+            bd_profile_replayed(g.prof_run);
+            g_launches += g.kernels;
+            return PACO_OK;
+        }
+    }
+    bd_init_attrs();
+    bdc_init_attrs();
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return svd_direct(M, N, A, U, Vt, sigma, b, L, stream);
+    }
+    const unsigned long long k0 = g_launches;
+    int rc = svd_direct(M, N, A, U, Vt, sigma, b, L, stream);
+    const unsigned long long kernels = g_launches - k0;
+    g_launches = k0; // recorded, not yet run
+    cudaGraph_t graph = nullptr;
+    cudaError_t err = cudaStreamEndCapture(s, &graph);
+    if (rc || err != cudaSuccess || !graph) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return rc ? rc : svd_direct(M, N, A, U, Vt, sigma, b, L, stream);
+    }
+    GraphEntry g;
+    g.M = M; g.N = N; g.prof = g_prof_on; g.A = A; g.U = U; g.Vt = Vt; g.sigma = sigma; g.ws = ws; g.s = s;
+    g.prof_run = g_prof_on ? bd_profile_last_graph_run() : -1;
+    g.kernels = kernels;
+    err = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (err != cudaSuccess) {
+        cudaGetLastError();
+        return svd_direct(M, N, A, U, Vt, sigma, b, L, stream);
+    }
+    if (g_graphs.size() >= 16) {
+        cudaGraphExecDestroy(g_graphs.front().exec);
+        g_graphs.erase(g_graphs.begin());
+    }
+    g_graphs.push_back(g);
+    if (cudaGraphLaunch(g.exec, s) != cudaSuccess) return PACO_ERR_CUDA;
+    bd_profile_replayed(g.prof_run);
+    g_launches += g.kernels;
+    return PACO_OK;
 }
 
 struct paco_ctx {
