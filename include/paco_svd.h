@@ -96,6 +96,20 @@ int paco_ctx_create(int M, int N, paco_ctx **out);
 int paco_ctx_svd_host(paco_ctx *ctx, const float *A, float *U, float *Vt, float *sigma);
 void paco_ctx_destroy(paco_ctx *ctx);
 
+/* Allocation-free SVD (no counterpart in the reference) for callers that
+ * cannot call cudaMalloc: code running where a framework's caching allocator
+ * owns all device memory, or real-time and embedded hosts that must not grow
+ * their memory after start-up.  Same inputs and outputs as paco_svd (A is
+ * destroyed), M <= 1024 and N <= 512 (larger shapes return
+ * PACO_ERR_UNSUPPORTED).  All scratch lives in a 12 MiB device array inside
+ * the library, which every GPU that loads the library holds until the process
+ * exits; no device memory is allocated per call.  The first call on a device
+ * looks up that array's address (make it before any stream capture).  Calls
+ * share the array: calls that overlap on the GPU, from any stream or thread,
+ * race and must be serialized by the caller.  The call synchronizes `stream`
+ * and returns the device status of the run. */
+int paco_svd_noalloc(int M, int N, float *A, float *U, float *Vt, float *sigma, void *stream);
+
 /* Library version string. */
 const char *paco_version(void);
 

@@ -2,6 +2,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "bdc.cuh"
@@ -251,6 +252,59 @@ int paco_svd(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws
     bd_profile_replayed(g.prof_run);
     g_launches += g.kernels;
     return PACO_OK;
+}
+
+// ------------------------------------------------ allocation-free entry point
+// Scratch of paco_svd_noalloc: a file-scope device array, so the entry point
+// needs no cudaMalloc.  It is part of the loaded module, so every GPU that
+// loads the library holds these bytes until the process exits.
+#define PACO_NOALLOC_MAX_M 1024
+#define PACO_NOALLOC_MAX_N 512
+#define PACO_NOALLOC_BYTES (12u << 20)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[PACO_NOALLOC_BYTES];
+
+namespace {
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[64]; // device address of the array, per device ordinal
+}  // namespace
+
+// Device address of g_noalloc_scratch on the current device.  In host code
+// the array's name only stands in for the symbol, so the address is looked up
+// once per device, with that device current, and cached.
+static int noalloc_scratch(void **out)
+{
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return PACO_ERR_CUDA;
+    if (dev < 0 || dev >= 64) return PACO_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+            cudaGetLastError();
+            return PACO_ERR_CUDA;
+        }
+        g_noalloc_addr[dev] = p;
+    }
+    *out = g_noalloc_addr[dev];
+    return PACO_OK;
+}
+
+int paco_svd_noalloc(int M, int N, float *A, float *U, float *Vt, float *sigma, void *stream)
+{
+    if (N < 1 || M < N) return PACO_ERR_INVALID_ARG;
+    if (M > PACO_NOALLOC_MAX_M || N > PACO_NOALLOC_MAX_N) return PACO_ERR_UNSUPPORTED;
+    if (!A || !U || !Vt || !sigma) return PACO_ERR_INVALID_ARG;
+    SvdLayout L = svd_layout(M, N);
+    if (L.total > PACO_NOALLOC_BYTES) return PACO_ERR_UNSUPPORTED;
+    void *scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    // the status block and counters at the start of the scratch are cleared by
+    // the stages themselves; everything else is written before it is read
+    rc = svd_direct(M, N, A, U, Vt, sigma, (char *)scratch, L, stream);
+    if (rc) return rc;
+    int info = 0;
+    return paco_sync_status((char *)scratch + L.ws, stream, &info);
 }
 
 struct paco_ctx {
