@@ -125,7 +125,7 @@ def measured_peaks():
 def traffic_ratio():
     """DRAM bytes per algorithmic byte of the row pass, from the committed ncu
     summary (profiles/bd_row_pass.txt, line 'dram_per_alg_byte: X')."""
-    path = os.path.join(ROOT, "profiles", "bd_row_pass.txt")
+    path = os.path.join(ROOT, "profiles", "bd_row_pass.txt")  # ncu, 8192x4096 row pass
     try:
         for ln in open(path):
             if ln.startswith("dram_per_alg_byte:"):
@@ -133,6 +133,21 @@ def traffic_ratio():
     except Exception:
         pass
     return None
+
+
+def max_over_ranks(total_ms, dist, device="cuda"):
+    """Slowest rank's timed-region length (replicas run concurrently)."""
+    if dist is None:
+        return float(total_ms)
+    import torch
+    t = torch.tensor([float(total_ms)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_value(world, steps, total_ms):
+    """SVDs/s of the whole job: every rank ran `steps` SVDs in at most total_ms."""
+    return world * steps / (total_ms / 1000.0)
 
 
 def cpu_baseline(wl, steps=1):
@@ -177,6 +192,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cfg2a", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end measurement")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
 
@@ -207,7 +223,7 @@ def main():
     lib = P.lib()
     lib.paco_launch_count.restype = ctypes.c_ulonglong
     lib.paco_profile_read.argtypes = [ctypes.POINTER(ctypes.c_double)]
-    prof = (ctypes.c_double * 3)()
+    prof = (ctypes.c_double * 4)()
 
     def step():
         W.A.copy_(A0)
@@ -246,11 +262,7 @@ def main():
     lib.paco_profile_enable(0)
     clk = clocks.stop()
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    total_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(step_ms), dist)
     rc, info = P.sync_status(W.ws, stream)
     if rc:
         raise SystemExit(f"device status {rc} ({info}) in the timed region")
@@ -259,18 +271,20 @@ def main():
     s = W.sigma.float().cpu().numpy().astype(np.float64)
 
     # end to end through the host-buffer C ABI (H2D of A, D2H of U, Vt, sigma)
-    ctx = P.HostContext(M, N)
-    pin = lambda shape: torch.empty(shape, dtype=torch.float32).pin_memory()
-    Ah, Uh, Vh, sh = pin((M, N)), pin((M, M)), pin((N, N)), pin((N,))
-    Ah.copy_(torch.from_numpy(A_host))
-    e2e_ms = []
-    ctx.svd(Ah, Uh, Vh, sh)
-    for _ in range(max(1, min(args.steps, 3))):
-        t = time.perf_counter()
+    e2e_t = None
+    if not args.no_e2e:
+        ctx = P.HostContext(M, N)
+        pin = lambda shape: torch.empty(shape, dtype=torch.float32).pin_memory()
+        Ah, Uh, Vh, sh = pin((M, N)), pin((M, M)), pin((N, N)), pin((N,))
+        Ah.copy_(torch.from_numpy(A_host))
+        e2e_ms = []
         ctx.svd(Ah, Uh, Vh, sh)
-        e2e_ms.append((time.perf_counter() - t) * 1000)
-    ctx.close()
-    e2e_t = statistics.median(e2e_ms)
+        for _ in range(max(1, min(args.steps, 3))):
+            t = time.perf_counter()
+            ctx.svd(Ah, Uh, Vh, sh)
+            e2e_ms.append((time.perf_counter() - t) * 1000)
+        ctx.close()
+        e2e_t = statistics.median(e2e_ms)
 
     if rank != 0:
         if dist:
@@ -278,16 +292,21 @@ def main():
         return
     peaks, peak_kind = measured_peaks()
     rp_ms, rp_launches, rp_bytes = prof[0], prof[1], prof[2]
+    kname = ("bd_panel_pk (persistent stage-1 panel kernel: all column steps of a 32-column panel)"
+             if prof[3] == 1 else "bd_row_pass (stage-1 fused GEMV row pass)")
+    # the classic two-GEMV count of SURVEY 8(d): 8 * sum_i (M-i)(N-i) bytes per SVD
+    classic = 8.0 * sum((M - i) * (N - i) for i in range(N))
     achieved = (rp_bytes / 1e9) / (rp_ms / 1e3) if rp_ms > 0 else None
     ratio = traffic_ratio()
-    roof = {"kernel": "bd_row_pass (stage-1 fused GEMV row pass)", "bound": "hbm",
+    roof = {"kernel": kname, "bound": "hbm",
             "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": (achieved / peaks["hbm_gbs"]) if achieved else None,
             "traffic": (ratio * rp_bytes / rp_launches) if (ratio and rp_launches) else None,
             "alg_bytes_per_launch": rp_bytes / max(rp_launches, 1),
             "avg_launch_us": 1000.0 * rp_ms / max(rp_launches, 1),
-            "launches": int(rp_launches), "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)"}
-    value = world * args.steps / (total_ms / 1000.0)
+            "launches": int(rp_launches), "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+            "gemv_phase_equiv_gbs": (classic * args.steps / 1e9) / (rp_ms / 1e3) if rp_ms > 0 else None}
+    value = whole_job_value(world, args.steps, total_ms)
     line = {"metric": "SVDs/sec", "value": value, "unit": "SVDs/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -297,8 +316,9 @@ def main():
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
             "sigma_max": float(s[0]), "sigma_min": float(s[-1]),
             "roofline": roof, "clocks": clk,
-            "e2e": {"value": 1000.0 / e2e_t * world, "unit": "SVDs/s",
-                    "h2d_bytes_per_step": 4 * M * N, "d2h_bytes_per_step": 4 * (M * M + N * N + N)},
+            "e2e": ({"value": 1000.0 / e2e_t * world, "unit": "SVDs/s",
+                     "h2d_bytes_per_step": 4 * M * N, "d2h_bytes_per_step": 4 * (M * M + N * N + N)}
+                    if e2e_t else None),
             "gpu_launches": int(launches)}
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(wl)

@@ -114,13 +114,15 @@ int paco_svd_noalloc(int M, int N, float *A, float *U, float *Vt, float *sigma, 
 const char *paco_version(void);
 
 /* Kernel timing (no counterpart in the reference, which is profiled with
- * msprof, myprof.sh:1-8): while enabled, every launch of the stage-1 row-pass
- * kernel is bracketed by CUDA events on its stream.  paco_profile_read
- * synchronizes on them and returns totals since the last enable:
- * out[0] = milliseconds in row passes, out[1] = launches, out[2] = bytes the
- * launches had to read (the live row segments).  Host-thread-local use only. */
+ * msprof, myprof.sh:1-8): while enabled, every launch of the dominant
+ * stage-1 kernel (the persistent panel kernel, or the row pass where that
+ * one cannot launch) is bracketed by CUDA events on its stream.
+ * paco_profile_read synchronizes on them and returns totals since the last
+ * enable: out[0] = milliseconds, out[1] = launches, out[2] = bytes the
+ * launches had to read (live row segments), out[3] = 1 for the persistent
+ * panel kernel, 0 for the row pass.  Host-thread-local use only. */
 void paco_profile_enable(int on);
-void paco_profile_read(double out[3]);
+void paco_profile_read(double out[4]);
 
 /* Number of kernels this library has launched in the process so far (a
  * replay of a recorded CUDA graph counts the kernels the graph holds). */

@@ -24,6 +24,7 @@
 // to arrive (ticket counter), summing the per-block partials in block order,
 // so results are bitwise reproducible.  After each panel one GEMM applies
 // the rank-2*NB update to the trailing matrix.
+#include <cstdlib>
 #include <vector>
 
 #include "bidiag.cuh"
@@ -98,21 +99,6 @@ __global__ void bd_scale_last_col(float *W, long ldw, int M, int N, const float 
     float s = inv_v0c[N - 1];
     for (int r = N + blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x)
         W[(long)r * ldw + N - 1] *= s;
-}
-
-// reflector of upper_bidiagonalization.cpp:182-218 from x0 and sigma = |x[1:]|^2
-__device__ __forceinline__ void make_reflector(float x0, float sigma, int len, float *beta, float *tau,
-                                               float *v0)
-{
-    if (len <= 1 || sigma == 0.f) {
-        *beta = x0; *tau = 0.f; *v0 = 1.f;
-        return;
-    }
-    float mu = sqrtf(x0 * x0 + sigma);
-    float v = (x0 <= 0.f) ? x0 - mu : -sigma / (x0 + mu);
-    *v0 = v;
-    *tau = 2.f * v * v / (sigma + v * v);
-    *beta = mu;
 }
 
 // ------------------------------------------------------------- row pass
@@ -326,27 +312,13 @@ __global__ void __launch_bounds__(RP_THREADS, 1) bd_row_pass(BdArgs a, int i, in
     for (int t = tid; t < PR; t += RP_THREADS) {
         float v = 0.f;
         for (int w = 0; w < RMAX; w++) v += s_part[w][t];
-        a.tpart[(long)blockIdx.x * PR + t] = v;
+        a.tpart[(long)t * PCAP + blockIdx.x] = v;
     }
     if (!last_block_ticket(&st->counters[0], G, &s_flag)) return;
 
     // last block: finish the column reflector and t1 = V^T v, t2 = X^T v
     {
-        const int nval = 1 + 2 * NB;
-        const int slices = RP_THREADS / nval; // 7
-        __shared__ float s_sl[RP_THREADS];
-        int t = tid % nval, sl = tid / nval;
-        float v = 0.f;
-        if (sl < slices)
-            for (int bb = sl; bb < G; bb += slices) v += __ldcg(&a.tpart[(long)bb * PR + t]);
-        s_sl[tid] = v;
-        __syncthreads();
-        if (tid < nval) {
-            float s = 0.f;
-            for (int q = 0; q < slices; q++) s += s_sl[q * nval + tid];
-            s_red[tid] = s;
-        }
-        __syncthreads();
+        reduce_records(a.tpart, G, 1 + 2 * NB, s_red);
         if (tid == 0) {
             float x0 = __ldcg(&a.sc->x0col);
             float beta, tau, v0;
@@ -374,7 +346,6 @@ __global__ void __launch_bounds__(CP_THREADS) bd_col_pass(BdArgs a, int i, int p
     __shared__ float s_t1[NB], s_t2[NB], s_ai[NB], s_xi[NB];
     __shared__ float s_part[PR];
     __shared__ float s_red[PR];
-    __shared__ float s_sl[CP_THREADS];
     __shared__ int s_flag;
     __shared__ float s_v0;
 
@@ -387,9 +358,15 @@ __global__ void __launch_bounds__(CP_THREADS) bd_col_pass(BdArgs a, int i, int p
     DevStatus *st = a.st;
 
     // (1) sum the row-pass partials of A^T x for this column
+    float yv[RB_CAP / (CP_THREADS / 32)];
+#pragma unroll
+    for (int k = 0; k < RB_CAP / (CP_THREADS / 32); k++) {
+        int bb = warp + (CP_THREADS / 32) * k;
+        yv[k] = (valid && bb < Gr) ? __ldcg(&a.ypart[(long)bb * ldw + j]) : 0.f;
+    }
     float ys = 0.f;
-    if (valid)
-        for (int bb = warp; bb < Gr; bb += CP_THREADS / 32) ys += __ldcg(&a.ypart[(long)bb * ldw + j]);
+#pragma unroll
+    for (int k = 0; k < RB_CAP / (CP_THREADS / 32); k++) ys += yv[k];
     red[warp][lane] = ys;
     for (int t = tid; t < PR; t += CP_THREADS) s_part[t] = 0.f;
     if (tid < NB) {
@@ -452,25 +429,12 @@ __global__ void __launch_bounds__(CP_THREADS) bd_col_pass(BdArgs a, int i, int p
         if (lane == 0) { s_part[0] = ss; s_part[1 + ii] = g3; }
     }
     __syncthreads();
-    for (int t = tid; t < PR; t += CP_THREADS) a.cpart[(long)blockIdx.x * PR + t] = s_part[t];
+    for (int t = tid; t < PR; t += CP_THREADS) a.cpart[(long)t * PCAP + blockIdx.x] = s_part[t];
     if (!last_block_ticket(&st->counters[1], gridDim.x, &s_flag)) return;
 
     // last block: row reflector of row i and t3 = Y^T u, t4 = U u
     {
-        const int nval = 2 * NB + 2;
-        const int slices = CP_THREADS / nval; // 3
-        int t = tid % nval, sl = tid / nval;
-        float v = 0.f;
-        if (sl < slices)
-            for (int bb = sl; bb < (int)gridDim.x; bb += slices) v += __ldcg(&a.cpart[(long)bb * PR + t]);
-        s_sl[tid] = v;
-        __syncthreads();
-        if (tid < nval) {
-            float s = 0.f;
-            for (int q = 0; q < slices; q++) s += s_sl[q * nval + tid];
-            s_red[tid] = s;
-        }
-        __syncthreads();
+        reduce_records(a.cpart, gridDim.x, 2 * NB + 2, s_red);
         if (tid == 0) {
             float x0 = __ldcg(&a.sc->x0row);
             float beta, tau, v0;
@@ -628,6 +592,7 @@ struct RpProfile {
     std::vector<std::pair<int, bool>> pending; // (run id, direct?) awaiting a read
     std::vector<ProfRun> direct_runs;
     double ms = 0, launches = 0, bytes = 0;
+    int kind = 0; // dominant stage-1 kernel timed: 0 row pass, 1 persistent panel kernel
 } g_prof;
 
 cudaEvent_t prof_event()
@@ -691,8 +656,9 @@ void bd_profile_replayed(int id)
     if (g_prof.on && id >= 0) g_prof.pending.push_back({id, false});
 }
 
-// totals since the last enable: [0] ms in row passes, [1] launches, [2] bytes
-void bd_profile_read(double out[3])
+// totals since the last enable: [0] ms in the timed kernel, [1] launches,
+// [2] bytes, [3] which kernel (0 row pass, 1 persistent panel kernel)
+void bd_profile_read(double out[4])
 {
     for (auto &p : g_prof.pending) {
         ProfRun &r = p.second ? g_prof.direct_runs[p.first] : g_prof.graph_runs[p.first];
@@ -713,6 +679,21 @@ void bd_profile_read(double out[3])
     out[0] = g_prof.ms;
     out[1] = g_prof.launches;
     out[2] = g_prof.bytes;
+    out[3] = g_prof.kind;
+}
+
+// Bytes one persistent panel launch must read from memory: the live row
+// segments [p0, N) of rows [p0, M) once if they stay resident in shared memory,
+// else those of rows [i, M) at every step i of the panel (and the X pass).
+static double pk_alg_bytes(int M, int N, int p0, int p1, int G, long ldw)
+{
+    const long L = ldw - p0;
+    const long own = (M - p0 + G - 1) / G;
+    if (own * L * 4 <= 200L * 1024) return 4.0 * (double)(M - p0) * (double)(N - p0);
+    double b = 0;
+    const int last = (p1 < N) ? p1 : p1 - 1;
+    for (int i = p0; i <= last; i++) b += 4.0 * (double)(M - i) * (double)(N - p0);
+    return b;
 }
 
 static void rp(const BdArgs &a, int i, int p0, int mode, int G, cudaStream_t s)
@@ -770,20 +751,45 @@ int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, f
     const int gmax = std::max(1, std::min(RB_CAP, num_sms));
     auto grid_rows = [&](int rows) { return std::max(1, std::min(gmax, ceil_div(rows, RMIN_PER_BLOCK))); };
     cudaMemsetAsync(w.st->counters, 0, sizeof(w.st->counters), s);
+    cudaMemsetAsync(w.ctl, 0, sizeof(PkCtl), s);
+    bd_pk_init_attrs();
+    // the persistent panel kernel needs every CTA co-resident (one per SM)
+    static int use_pk_env = -1;
+    if (use_pk_env < 0) {
+        const char *v = getenv("PACO_PERSISTENT");
+        use_pk_env = !(v && v[0] == '0');
+    }
+    const bool use_pk = use_pk_env != 0;
     cudaMemsetAsync(w.Yt, 0, sizeof(float) * NB * w.ldw, s);
     cudaMemsetAsync(w.X, 0, sizeof(float) * (size_t)M * NB, s);
     paco_count_launch(), bd_copy_in<<<std::min(4096, ceil_div((long)M * w.ldw, 256)), 256, 0, s>>>(a_in, w.W, M, N, w.ldw, w.st);
 
     for (int p0 = 0; p0 < N; p0 += NB) {
         const int p1 = std::min(N, p0 + NB), nbp = p1 - p0;
-        for (int i = p0; i < p1; i++) {
-            int G = grid_rows(M - i);
-            int mode = RP_DO_COL | ((i > p0) ? RP_DO_X : 0);
-            rp(a, i, p0, mode, G, s);
-            if (i < N - 1) paco_count_launch(), bd_col_pass<<<ceil_div(N - i - 1, 32), CP_THREADS, 0, s>>>(a, i, p0, G);
+        const int Gp = std::max(1, std::min(gmax, ceil_div(M - p0, 16)));
+        bool pk = false;
+        if (use_pk) {
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            if (g_prof.on) prof_record(e0 = prof_event(), s);
+            pk = bd_panel_pk_launch(a, w.ctl, p0, p1, Gp, s);
+            if (g_prof.on) {
+                prof_record(e1 = prof_event(), s);
+                g_prof.cur.ev.push_back(e0);
+                g_prof.cur.ev.push_back(e1);
+                g_prof.cur.bytes.push_back(pk_alg_bytes(M, N, p0, p1, Gp, w.ldw));
+                g_prof.kind = 1;
+            }
+        }
+        if (!pk) {
+            for (int i = p0; i < p1; i++) {
+                int G = grid_rows(M - i);
+                int mode = RP_DO_COL | ((i > p0) ? RP_DO_X : 0);
+                rp(a, i, p0, mode, G, s);
+                if (i < N - 1) paco_count_launch(), bd_col_pass<<<ceil_div(N - i - 1, 32), CP_THREADS, 0, s>>>(a, i, p0, G);
+            }
         }
         if (p1 < N) {
-            rp(a, p1, p0, RP_DO_X | RP_PANEL_END, grid_rows(M - p1), s);
+            if (!pk) rp(a, p1, p0, RP_DO_X | RP_PANEL_END, grid_rows(M - p1), s);
             // A[p1:, p1:] -= [V | X] [Y^T ; U]
             GemmOp A = gop(w.W + (long)p1 * w.ldw + p0, w.ldw, 1);
             A.p2 = w.X + (long)p1 * NB; A.rs2 = NB; A.cs2 = 1; A.ksplit = nbp;

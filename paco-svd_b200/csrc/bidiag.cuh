@@ -13,6 +13,7 @@ constexpr int CB_CAP = 512;        // max column-pass CTAs (N/32)
 constexpr int PR = 2 * NB + 8;     // floats per partial record
 constexpr int RMIN_PER_BLOCK = 16; // fewest rows a row-pass CTA is given
 constexpr int SPLITS = 8;          // split-K factor cap for the skinny V^T Q products
+constexpr int PCAP = 512;          // CTA slots of a partial record (>= RB_CAP, CB_CAP)
 }  // namespace bd
 
 struct StepScal {
@@ -22,6 +23,14 @@ struct StepScal {
     float t4[bd::NB];     // U_panel u
     float x0col, x0row;   // pivots of the current reflectors
     float pad[5];
+};
+
+// Control words of the persistent panel kernel's grid barrier.
+struct PkCtl {
+    unsigned cnt;   // CTAs arrived at the current barrier
+    unsigned gen;   // barrier generation, bumped by the last CTA
+    unsigned abort; // set by a CTA whose bounded wait gave up
+    unsigned pad[29];
 };
 
 struct BdArgs {
@@ -40,11 +49,12 @@ struct BdWs {
     float *Yt;     // NB x ldw  Y^T of the current panel
     float *X;      // M x NB    X of the current panel
     float *ypart;  // RB_CAP x ldw  per-CTA partial A^T x
-    float *tpart;  // RB_CAP x PR
-    float *cpart;  // CB_CAP x PR
+    float *tpart;  // PR x PCAP, value-major: tpart[t * PCAP + cta]
+    float *cpart;  // PR x PCAP
     float *rowbuf; // ldw       updated pivot row
     float *inv_v0c, *inv_v0r; // N each: 1/v0 of every reflector
     StepScal *sc;
+    PkCtl *ctl;
     float *Vp;     // max(M,N) x NB  explicit reflector panel
     float *T;      // NB x NB
     float *gpart;  // RB_CAP x NB*NB
@@ -73,12 +83,13 @@ static inline size_t bd_carve(void *base, int M, int N, BdWs *w)
     w->Yt = (float *)take(sizeof(float) * (size_t)NB * ldw);
     w->X = (float *)take(sizeof(float) * (size_t)M * NB);
     w->ypart = (float *)take(sizeof(float) * (size_t)RB_CAP * ldw);
-    w->tpart = (float *)take(sizeof(float) * (size_t)RB_CAP * PR);
-    w->cpart = (float *)take(sizeof(float) * (size_t)CB_CAP * PR);
+    w->tpart = (float *)take(sizeof(float) * (size_t)PCAP * PR);
+    w->cpart = (float *)take(sizeof(float) * (size_t)PCAP * PR);
     w->rowbuf = (float *)take(sizeof(float) * ldw);
     w->inv_v0c = (float *)take(sizeof(float) * N);
     w->inv_v0r = (float *)take(sizeof(float) * N);
     w->sc = (StepScal *)take(sizeof(StepScal));
+    w->ctl = (PkCtl *)take(sizeof(PkCtl));
     w->Vp = (float *)take(sizeof(float) * (size_t)mx * NB);
     w->T = (float *)take(sizeof(float) * NB * NB);
     w->gpart = (float *)take(sizeof(float) * (size_t)RB_CAP * NB * NB);
@@ -89,9 +100,50 @@ static inline size_t bd_carve(void *base, int M, int N, BdWs *w)
     return (off + 255) & ~(size_t)255;
 }
 
+// reflector of upper_bidiagonalization.cpp:182-218 from x0 and sigma = |x[1:]|^2
+static __device__ __forceinline__ void make_reflector(float x0, float sigma, int len, float *beta, float *tau,
+                                                      float *v0)
+{
+    if (len <= 1 || sigma == 0.f) {
+        *beta = x0; *tau = 0.f; *v0 = 1.f;
+        return;
+    }
+    float mu = sqrtf(x0 * x0 + sigma);
+    float v = (x0 <= 0.f) ? x0 - mu : -sigma / (x0 + mu);
+    *v0 = v;
+    *tau = 2.f * v * v / (sigma + v * v);
+    *beta = mu;
+}
+
+// Sums the per-CTA partial records rec[t * PCAP + cta] (cta < ncta) into
+// out[t] for t < nval: one warp per value, all CTA slots loaded at once,
+// summed in a fixed order.  Called by every thread of the CTA.
+static __device__ __forceinline__ void reduce_records(const float *rec, int ncta, int nval, float *out)
+{
+    using namespace bd;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int t = warp; t < nval; t += nw) {
+        float v[PCAP / 32];
+#pragma unroll
+        for (int k = 0; k < PCAP / 32; k++) {
+            int c = lane + 32 * k;
+            v[k] = (c < ncta) ? __ldcg(&rec[(long)t * PCAP + c]) : 0.f;
+        }
+        float sum = 0.f;
+#pragma unroll
+        for (int k = 0; k < PCAP / 32; k++) sum += v[k];
+        sum = warp_sum(sum);
+        if (lane == 0) out[t] = sum;
+    }
+    __syncthreads();
+}
+
+bool bd_panel_pk_launch(const BdArgs &a, PkCtl *ctl, int p0, int p1, int G, cudaStream_t s);
+void bd_pk_init_attrs();
+
 size_t bd_workspace_bytes(int M, int N);
 void bd_profile_enable(int on);
-void bd_profile_read(double out[3]);
+void bd_profile_read(double out[4]);
 int bd_profile_last_graph_run();
 void bd_profile_replayed(int id);
 void bd_init_attrs();

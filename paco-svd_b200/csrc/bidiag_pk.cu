@@ -1,0 +1,469 @@
+// Persistent panel kernel of the stage-1 bidiagonalization.
+//
+// One cooperative launch (one CTA per SM) runs all NB column steps of a
+// panel [p0, p1).  Each step is the row pass (row-parallel: finish X for the
+// previous row reflector, update column i, accumulate A^T x) and the column
+// pass (column-parallel: Y(:, i), row i, row-reflector partials), separated
+// by grid barriers.  At each barrier the CTA that arrives last sums the
+// per-CTA partials in CTA order (bitwise reproducible), forms the reflector
+// and only then releases the others.  Barrier waits are bounded: a CTA that
+// waits for ~2 s of SM clock records PACO_ERR_TIMEOUT, raises the abort flag
+// and returns, and the others follow at their next barrier.
+//
+// Rows are owned cyclically (row r belongs to CTA (r - p0) % G).  When a
+// CTA's rows [p0, N) fit in shared memory they are staged once per panel and
+// kept resident for its NB steps, so the trailing matrix is read from HBM
+// once per panel instead of once per step; otherwise they are re-staged with
+// TMA bulk copies at every step (double-buffered).  Data that other CTAs wrote
+// earlier in the same launch is read with ld.global.cg (L2), never from L1.
+#include "bidiag.cuh"
+#include "tma.cuh"
+
+using namespace bd;
+
+namespace {
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid barrier, part 1: returns true in the CTA that arrived last.  That CTA
+// finishes the phase (its reduction) and then calls pk_release; every other
+// CTA calls pk_wait.
+__device__ bool pk_arrive(PkCtl *c, int G, int *s_flag, unsigned *s_gen)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned g = ld_acquire(&c->gen);
+        __threadfence();
+        unsigned t = atomicAdd(&c->cnt, 1u);
+        *s_gen = g;
+        *s_flag = (t == (unsigned)G - 1);
+    }
+    __syncthreads();
+    const bool last = *s_flag != 0;
+    if (last) __threadfence();
+    return last;
+}
+
+__device__ void pk_release(PkCtl *c)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        atomicExch(&c->cnt, 0u);
+        __threadfence();
+        atomicAdd(&c->gen, 1u);
+    }
+    __syncthreads();
+}
+
+// Bounded wait for the generation to move past g; false if the launch aborts.
+__device__ bool pk_wait(PkCtl *c, unsigned g, DevStatus *st, int where, int *s_ok)
+{
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        long long t0 = clock64();
+        while (ld_acquire(&c->gen) == g) {
+            if (ld_acquire(&c->abort)) { ok = 0; break; }
+            if (clock64() - t0 > 4000000000LL) {
+                atomicAdd(&st->wait_timeouts, 1);
+                dev_fail(st, PACO_ERR_TIMEOUT, where);
+                atomicExch(&c->abort, 1u);
+                ok = 0;
+                break;
+            }
+        }
+        *s_ok = ok;
+    }
+    __syncthreads();
+    __threadfence();
+    return *s_ok != 0;
+}
+
+}  // namespace
+
+template <int CPT>
+__global__ void __launch_bounds__(RP_THREADS, 1)
+    bd_panel_pk(BdArgs a, PkCtl *ctl, int p0, int p1, int resident, int R)
+{
+    extern __shared__ __align__(128) float tiles[];
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ float red[RP_THREADS / 32][RMAX];
+    __shared__ float xs[RMAX];
+    __shared__ float s_t3[NB + 1], s_t4[NB], s_ycol[NB], s_wcol[NB];
+    __shared__ float s_t1[NB], s_t2[NB], s_ai[NB], s_xi[NB];
+    __shared__ float s_part[RMAX][PR];
+    __shared__ float s_red[PR];
+    __shared__ float cy[RP_THREADS / 32][32], cA[RP_THREADS / 32][32], cB[RP_THREADS / 32][32];
+    __shared__ float s_cpart[PR];
+    __shared__ int s_flag, s_ok;
+    __shared__ unsigned s_gen;
+    __shared__ float s_v0;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int M = a.M, N = a.N, G = gridDim.x, b = blockIdx.x;
+    const long ldw = a.ldw;
+    const int L = (int)(ldw - p0);
+    DevStatus *st = a.st;
+    // rows owned by this CTA: p0 + b + k*G, k < nown
+    const int nown = (M - p0 - b + G - 1) / G > 0 ? (M - p0 - b + G - 1) / G : 0;
+    auto own_row = [&](int k) { return p0 + b + k * G; };
+
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    uint32_t phase0 = 0, phase1 = 0;
+    bool failed = false;
+
+    if (resident && nown > 0) {
+        if (tid == 0) {
+            mbar_expect_tx(&bars[0], (uint32_t)nown * L * 4u);
+            for (int k = 0; k < nown; k++)
+                tma_load_1d(tiles + (long)k * L, a.W + (long)own_row(k) * ldw + p0, (uint32_t)L * 4u, &bars[0]);
+        }
+        bool ok = mbar_wait_bounded(&bars[0], 0, st, 90);
+        phase0 = 1;
+        if (__syncthreads_or(!ok)) failed = true;
+    }
+
+    // the panel's steps, then (when a trailing matrix follows) the X-only pass
+    const int last_step = (p1 < N) ? p1 : p1 - 1;
+    for (int i = p0; i <= last_step && !failed; i++) {
+        const bool xonly = (i == p1);
+        const bool doX = (i > p0);
+        const bool doCol = !xonly;
+        const int ii = i - p0, iip = ii - 1;
+        const float invr = doX ? __ldcg(&a.inv_v0r[i - 1]) : 0.f;
+        const float taup_prev = doX ? __ldcg(&a.taup[i - 1]) : 0.f;
+        const float invc = (ii >= 1) ? __ldcg(&a.inv_v0c[i - 1]) : 1.f;
+
+        // ------------------------------------------------------ row pass
+        float4 u4[CPT], acc4[CPT];
+#pragma unroll
+        for (int k = 0; k < CPT; k++) {
+            int c = p0 + 4 * (tid + k * RP_THREADS);
+            float uv[4];
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                int j = c + e;
+                float v = 0.f;
+                if (doX) {
+                    if (j == i) v = 1.f;
+                    else if (j > i && j < N) v = __ldcg(&a.rowbuf[j]) * invr;
+                }
+                uv[e] = v;
+            }
+            u4[k] = make_float4(uv[0], uv[1], uv[2], uv[3]);
+            acc4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        if (tid <= NB) s_t3[tid] = (doX && tid <= iip) ? __ldcg(&a.sc->t3[tid]) : 0.f;
+        if (tid < NB) {
+            s_t4[tid] = (doX && tid < iip) ? __ldcg(&a.sc->t4[tid]) : 0.f;
+            s_ycol[tid] = (doCol && tid < ii) ? __ldcg(&a.Yt[(long)tid * ldw + i]) : 0.f;
+            s_wcol[tid] = (doCol && tid < ii) ? ((tid == ii - 1) ? 1.f : __ldcg(&a.W[(long)(p0 + tid) * ldw + i]))
+                                               : 0.f;
+        }
+        for (int t = tid; t < RMAX * PR; t += RP_THREADS) (&s_part[0][0])[t] = 0.f;
+        if (doX && b == 0) {
+            for (int j = i + 1 + tid; j < N; j += RP_THREADS)
+                a.W[(long)(i - 1) * ldw + j] = __ldcg(&a.rowbuf[j]) * invr;
+            if (xonly && tid == 0) a.W[(long)(i - 1) * ldw + i] = 1.f;
+        }
+        // owned rows that are active in this step (r >= i)
+        int kfirst = 0;
+        while (kfirst < nown && own_row(kfirst) < i) kfirst++;
+        const int nact = nown - kfirst;
+        const int nbatch = (nact + R - 1) / R;
+        __syncthreads();
+        if (!resident && tid == 0) {
+            proxy_async_fence();
+            asm volatile("fence.proxy.async.global;" ::: "memory");
+        }
+        auto issue = [&](int bb, int stage) {
+            int k0 = kfirst + bb * R, nr = min(R, nown - k0);
+            mbar_expect_tx(&bars[stage], (uint32_t)nr * L * 4u);
+            for (int rr = 0; rr < nr; rr++)
+                tma_load_1d(tiles + ((long)stage * R + rr) * L, a.W + (long)own_row(k0 + rr) * ldw + p0,
+                            (uint32_t)L * 4u, &bars[stage]);
+        };
+        if (!resident && tid == 0) {
+            if (nbatch > 0) issue(0, 0);
+            if (nbatch > 1) issue(1, 1);
+        }
+        float w_ss = 0.f, w_g1 = 0.f, w_g2 = 0.f;
+        for (int bb = 0; bb < nbatch; bb++) {
+            const int k0 = kfirst + bb * R, nr = min(R, nown - k0);
+            const float *T;
+            const int stage = bb & 1;
+            if (resident) {
+                T = tiles + (long)k0 * L;
+            } else {
+                bool ok = mbar_wait_bounded(&bars[stage], stage ? phase1 : phase0, st, 200 + i);
+                if (stage) phase1 ^= 1; else phase0 ^= 1;
+                if (__syncthreads_or(!ok)) { failed = true; break; }
+                T = tiles + (long)stage * R * L;
+            }
+            if (doX) {
+                float pd[RMAX];
+#pragma unroll
+                for (int rr = 0; rr < RMAX; rr++) pd[rr] = 0.f;
+#pragma unroll
+                for (int rr = 0; rr < RMAX; rr++) {
+                    if (rr < nr) {
+#pragma unroll
+                        for (int k = 0; k < CPT; k++) {
+                            int c4 = tid + k * RP_THREADS;
+                            if (4 * c4 < L) {
+                                float4 v = *reinterpret_cast<const float4 *>(T + (long)rr * L + 4 * c4);
+                                pd[rr] += v.x * u4[k].x + v.y * u4[k].y + v.z * u4[k].z + v.w * u4[k].w;
+                            }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int rr = 0; rr < RMAX; rr++) {
+                    if (rr < nr) {
+                        float v = warp_sum(pd[rr]);
+                        if (lane == 0) red[warp][rr] = v;
+                    }
+                }
+                __syncthreads();
+            }
+            if (warp < nr) {
+                const int rr = warp, r = own_row(k0 + rr);
+                float *trow = (float *)T + (long)rr * L;
+                float aq = (lane < ii) ? trow[lane] : 0.f;
+                if (lane == ii - 1) {
+                    aq *= invc;
+                    a.W[(long)r * ldw + (i - 1)] = aq;
+                    if (resident) trow[lane] = aq;
+                }
+                float xq = (doX && lane < iip) ? a.X[(long)r * NB + lane] : 0.f;
+                float Xn = 0.f;
+                if (doX) {
+                    float dot = 0.f;
+#pragma unroll
+                    for (int w2 = 0; w2 < RP_THREADS / 32; w2++) dot += red[w2][rr];
+                    float sx = ((lane <= iip) ? aq * s_t3[lane] : 0.f) + ((lane < iip) ? xq * s_t4[lane] : 0.f);
+                    Xn = taup_prev * (dot - warp_sum(sx));
+                    if (lane == 0) a.X[(long)r * NB + iip] = Xn;
+                }
+                if (doCol) {
+                    float xrq = (lane < ii - 1) ? xq : ((lane == ii - 1) ? Xn : 0.f);
+                    float sc = (lane < ii) ? (aq * s_ycol[lane] + xrq * s_wcol[lane]) : 0.f;
+                    float xr = trow[ii] - warp_sum(sc);
+                    __syncwarp();
+                    if (lane == 0) {
+                        a.W[(long)r * ldw + i] = xr;
+                        if (resident) trow[ii] = xr;
+                        xs[rr] = xr;
+                        if (r == i) a.sc->x0col = xr;
+                    }
+                    if (r > i) {
+                        if (lane == 0) w_ss += xr * xr;
+                        if (lane < ii) { w_g1 += aq * xr; w_g2 += xrq * xr; }
+                    }
+                }
+            }
+            __syncthreads();
+            if (doCol) {
+#pragma unroll
+                for (int rr = 0; rr < RMAX; rr++) {
+                    if (rr < nr && own_row(k0 + rr) > i) {
+                        float xr = xs[rr];
+#pragma unroll
+                        for (int k = 0; k < CPT; k++) {
+                            int c4 = tid + k * RP_THREADS;
+                            if (4 * c4 < L) {
+                                float4 v = *reinterpret_cast<const float4 *>(T + (long)rr * L + 4 * c4);
+                                acc4[k].x += v.x * xr; acc4[k].y += v.y * xr;
+                                acc4[k].z += v.z * xr; acc4[k].w += v.w * xr;
+                            }
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            if (!resident && tid == 0 && bb + 2 < nbatch) {
+                proxy_async_fence();
+                issue(bb + 2, stage);
+            }
+        }
+        if (__syncthreads_or(failed)) { failed = true; break; }
+        if (xonly) break; // the X-only pass ends the panel
+
+        // row-pass partials and barrier A
+#pragma unroll
+        for (int k = 0; k < CPT; k++) {
+            int c4 = tid + k * RP_THREADS;
+            if (4 * c4 < L) *reinterpret_cast<float4 *>(a.ypart + (long)b * ldw + p0 + 4 * c4) = acc4[k];
+        }
+        if (warp < RMAX) {
+            if (lane == 0) s_part[warp][0] = w_ss;
+            s_part[warp][1 + lane] = w_g1;
+            s_part[warp][1 + NB + lane] = w_g2;
+        }
+        __syncthreads();
+        for (int t = tid; t < PR; t += RP_THREADS) {
+            float v = 0.f;
+            for (int w = 0; w < RMAX; w++) v += s_part[w][t];
+            a.tpart[(long)t * PCAP + b] = v;
+        }
+        if (pk_arrive(ctl, G, &s_flag, &s_gen)) {
+            reduce_records(a.tpart, G, 1 + 2 * NB, s_red);
+            if (tid == 0) {
+                float beta, tau, v0;
+                make_reflector(__ldcg(&a.sc->x0col), s_red[0], M - i, &beta, &tau, &v0);
+                a.d[i] = beta; a.tauq[i] = tau; a.inv_v0c[i] = 1.f / v0;
+                s_v0 = v0;
+            }
+            __syncthreads();
+            if (tid < ii) {
+                float inv = 1.f / s_v0;
+                a.sc->t1[tid] = __ldcg(&a.W[(long)i * ldw + p0 + tid]) + s_red[1 + tid] * inv;
+                a.sc->t2[tid] = __ldcg(&a.X[(long)i * NB + tid]) + s_red[1 + NB + tid] * inv;
+            }
+            pk_release(ctl);
+        } else if (!pk_wait(ctl, s_gen, st, 300 + i, &s_ok)) {
+            failed = true;
+            break;
+        }
+        if (i >= N - 1) break; // no row reflector after the last column
+
+        // --------------------------------------------------- column pass
+        const float tq = __ldcg(&a.tauq[i]), invc_i = __ldcg(&a.inv_v0c[i]);
+        if (tid < NB) {
+            bool q = tid < ii;
+            s_t1[tid] = q ? __ldcg(&a.sc->t1[tid]) : 0.f;
+            s_t2[tid] = q ? __ldcg(&a.sc->t2[tid]) : 0.f;
+            s_ai[tid] = q ? __ldcg(&a.W[(long)i * ldw + p0 + tid]) : 0.f;
+            s_xi[tid] = q ? __ldcg(&a.X[(long)i * NB + tid]) : 0.f;
+        }
+        for (int t = tid; t < PR; t += RP_THREADS) s_cpart[t] = 0.f;
+        __syncthreads();
+        const int nchunk = (N - i - 1 + 31) / 32;
+        for (int ch = b; ch < nchunk; ch += G) {
+            const int j = i + 1 + ch * 32 + lane;
+            const bool valid = j < N;
+            float yv[RB_CAP / (RP_THREADS / 32)];
+#pragma unroll
+            for (int k = 0; k < RB_CAP / (RP_THREADS / 32); k++) {
+                int q = warp + (RP_THREADS / 32) * k;
+                yv[k] = (valid && q < G) ? __ldcg(&a.ypart[(long)q * ldw + j]) : 0.f;
+            }
+            float ys = 0.f;
+#pragma unroll
+            for (int k = 0; k < RB_CAP / (RP_THREADS / 32); k++) ys += yv[k];
+            cy[warp][lane] = ys;
+            // warp w owns panel indices q in [2w, 2w+2)
+            float Yq[2], Wq[2], pa = 0.f, pb = 0.f;
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                int q = 2 * warp + e;
+                bool use = valid && q < ii;
+                Yq[e] = use ? __ldcg(&a.Yt[(long)q * ldw + j]) : 0.f;
+                Wq[e] = use ? __ldcg(&a.W[(long)(p0 + q) * ldw + j]) : 0.f;
+                pa += Yq[e] * s_t1[q] + Wq[e] * s_t2[q];
+                pb += Yq[e] * s_ai[q] + Wq[e] * s_xi[q];
+            }
+            cA[warp][lane] = pa;
+            cB[warp][lane] = pb;
+            __syncthreads();
+            float y = 0.f, sa = 0.f, sb = 0.f;
+#pragma unroll
+            for (int w = 0; w < RP_THREADS / 32; w++) { y += cy[w][lane]; sa += cA[w][lane]; sb += cB[w][lane]; }
+            float Ynew = 0.f, aj = 0.f;
+            if (valid) {
+                float wij = __ldcg(&a.W[(long)i * ldw + j]);
+                Ynew = tq * (wij + y * invc_i - sa);
+                aj = wij - Ynew - sb;
+                if (warp == 0) {
+                    a.Yt[(long)ii * ldw + j] = Ynew;
+                    a.rowbuf[j] = aj;
+                    if (j == i + 1) a.sc->x0row = aj;
+                }
+            }
+            float m = (valid && j >= i + 2) ? aj : 0.f;
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                int q = 2 * warp + e;
+                if (q < ii) {
+                    float g3 = warp_sum(Yq[e] * m), g4 = warp_sum(Wq[e] * m);
+                    if (lane == 0) { s_cpart[1 + q] += g3; s_cpart[NB + 2 + q] += g4; }
+                }
+            }
+            if (warp == 0) {
+                float ss = warp_sum(m * m), g3 = warp_sum(Ynew * m);
+                if (lane == 0) { s_cpart[0] += ss; s_cpart[1 + ii] += g3; }
+            }
+            __syncthreads();
+        }
+        for (int t = tid; t < PR; t += RP_THREADS) a.cpart[(long)t * PCAP + b] = s_cpart[t];
+        if (pk_arrive(ctl, G, &s_flag, &s_gen)) {
+            reduce_records(a.cpart, G, 2 * NB + 2, s_red);
+            if (tid == 0) {
+                float beta, tau, v0;
+                make_reflector(__ldcg(&a.sc->x0row), s_red[0], N - i - 1, &beta, &tau, &v0);
+                a.e[i] = beta; a.taup[i] = tau; a.inv_v0r[i] = 1.f / v0;
+                s_v0 = v0;
+            }
+            __syncthreads();
+            float inv = 1.f / s_v0;
+            if (tid <= ii) a.sc->t3[tid] = __ldcg(&a.Yt[(long)tid * ldw + i + 1]) + s_red[1 + tid] * inv;
+            if (tid < ii) a.sc->t4[tid] = __ldcg(&a.W[(long)(p0 + tid) * ldw + i + 1]) + s_red[NB + 2 + tid] * inv;
+            pk_release(ctl);
+        } else if (!pk_wait(ctl, s_gen, st, 400 + i, &s_ok)) {
+            failed = true;
+            break;
+        }
+    }
+}
+
+// Host side: launches the persistent kernel for panel [p0, p1) cooperatively.
+// Returns false when a cooperative launch of G CTAs is not possible.
+bool bd_panel_pk_launch(const BdArgs &a, PkCtl *ctl, int p0, int p1, int G, cudaStream_t s)
+{
+    const int L = (int)(a.ldw - p0);
+    const int own = (a.M - p0 + G - 1) / G;
+    const long budget = 200 * 1024;
+    int resident = ((long)own * L * 4 <= budget) ? 1 : 0;
+    int R = std::max(1, std::min(RMAX, (int)(budget / (2L * L * 4))));
+    size_t smem = resident ? (size_t)own * L * 4 : (size_t)2 * R * L * 4;
+    if (resident) R = RMAX;
+    const int chunks = ceil_div(L, 4 * RP_THREADS);
+    void *fn;
+    if (chunks <= 1) fn = (void *)bd_panel_pk<1>;
+    else if (chunks == 2) fn = (void *)bd_panel_pk<2>;
+    else fn = (void *)bd_panel_pk<4>;
+    BdArgs aa = a;
+    void *args[] = {&aa, &ctl, &p0, &p1, &resident, &R};
+    paco_count_launch();
+    return cudaLaunchCooperativeKernel(fn, dim3(G), dim3(RP_THREADS), args, smem, s) == cudaSuccess;
+}
+
+void bd_pk_init_attrs()
+{
+    static bool done = false;
+    if (done) return;
+    int maxs = 200 * 1024 + 1024;
+    cudaFuncSetAttribute(bd_panel_pk<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
+    cudaFuncSetAttribute(bd_panel_pk<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
+    cudaFuncSetAttribute(bd_panel_pk<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
+    done = true;
+}
+
+// CTAs per SM the persistent kernel can keep resident (for the grid size)
+int bd_pk_max_blocks_per_sm(int L)
+{
+    size_t smem = (size_t)200 * 1024;
+    (void)L;
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, bd_panel_pk<4>, RP_THREADS, smem);
+    return nb;
+}

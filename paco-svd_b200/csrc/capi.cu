@@ -64,7 +64,7 @@ void paco_profile_enable(int on)
     bd_profile_enable(on);
 }
 
-void paco_profile_read(double out[3])
+void paco_profile_read(double out[4])
 {
     if (out) bd_profile_read(out);
 }

@@ -5,10 +5,12 @@ Tolerances (FP32 outputs, Frobenius norms):
   sigma:          max_i |s_i - s_ref_i| / s_ref_1            <= 1e-5
   residual:       ||A - U[:, :N] S Vt||_F / ||A||_F          <= 1e-5 * N
   orthogonality:  ||U^T U - I||_F, ||V^T V - I||_F           <= 1e-5 * N
-Stage 1 alone: d, e, tauq, taup against the oracle's FP64 values (same
-reflector convention, so the signs agree) within 1e-4 * ||A||_F (d, e) and
-1e-5 * N (tau in [0, 2]; late reflectors come from a trailing matrix whose
-FP32 rounding has grown with the step count)."""
+Stage 1 alone: d, e against the oracle's FP64 values (same reflector
+convention, so the signs agree) within 1e-4 * ||A||_F; every reflector is
+exactly orthogonal, tau * (1 + |v[1:]|^2) = 2 within 1e-4, for the vectors
+the GPU left in A; tau itself is compared with the oracle only loosely
+(1e-2): late reflectors come from small trailing matrices whose FP32
+rounding has grown with the step count, so their tau is ill-conditioned."""
 import numpy as np
 import pytest
 
@@ -68,10 +70,19 @@ def test_bidiag_matches_oracle(shape):
     nrm = np.linalg.norm(A.astype(np.float64))
     d = g["d"].cpu().numpy(); e = g["e"].cpu().numpy()
     assert np.max(np.abs(d - o["d"])) <= 1e-4 * nrm
+    tq = g["tauq"].cpu().numpy().astype(np.float64)
+    tp = g["taup"].cpu().numpy().astype(np.float64)
+    Ah = g["A"].cpu().numpy().astype(np.float64)
     if N > 1:
         assert np.max(np.abs(e - o["e"])) <= 1e-4 * nrm
-        assert np.max(np.abs(g["taup"].cpu().numpy() - o["taup"])) <= max(1e-4, tol_n(N))
-    assert np.max(np.abs(g["tauq"].cpu().numpy() - o["tauq"])) <= max(1e-4, tol_n(N))
+        assert np.max(np.abs(tp - o["taup"])) <= 1e-2
+    assert np.max(np.abs(tq - o["tauq"])) <= 1e-2
+    for i in range(N):  # column reflectors: v = [1, A[i+1:, i]]
+        if tq[i] != 0:
+            assert abs(tq[i] * (1 + np.sum(Ah[i + 1:, i] ** 2)) - 2) <= 1e-4
+    for i in range(N - 1):  # row reflectors: u = [1, A[i, i+2:]]
+        if tp[i] != 0:
+            assert abs(tp[i] * (1 + np.sum(Ah[i, i + 2:] ** 2)) - 2) <= 1e-4
     # U B Vt = A and orthogonality (verify_result.py:58-123,194-198)
     U = g["U"].cpu().numpy().astype(np.float64); Vt = g["Vt"].cpu().numpy().astype(np.float64)
     B = np.zeros((M, N)); B[np.arange(N), np.arange(N)] = d
@@ -80,8 +91,7 @@ def test_bidiag_matches_oracle(shape):
     assert np.linalg.norm(U @ B @ Vt - A) <= tol_n(N) * nrm
     assert O.orth_err(U) <= tol_n(N)
     assert O.orth_err(Vt.T) <= tol_n(N)
-    # the Householder vectors left in A rebuild U (first column) like the oracle's
-    Ah = g["A"].cpu().numpy()
+    # d on the diagonal of the returned A (upper_bidiagonalization.cpp:193-207)
     np.testing.assert_allclose(np.diag(Ah), d, rtol=0, atol=0)
 
 
