@@ -101,7 +101,7 @@ void paco_ctx_destroy(paco_ctx *ctx);
  * owns all device memory, or real-time and embedded hosts that must not grow
  * their memory after start-up.  Same inputs and outputs as paco_svd (A is
  * destroyed), M <= 1024 and N <= 512 (larger shapes return
- * PACO_ERR_UNSUPPORTED).  All scratch lives in a 12 MiB device array inside
+ * PACO_ERR_UNSUPPORTED).  All scratch lives in a 16 MiB device array inside
  * the library, which every GPU that loads the library holds until the process
  * exits; no device memory is allocated per call.  The first call on a device
  * looks up that array's address (make it before any stream capture).  Calls

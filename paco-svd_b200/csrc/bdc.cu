@@ -523,10 +523,14 @@ __global__ void __launch_bounds__(256) bdc_secular(LevelArgs A, int nm)
     if (lane == 0) A.d[s + i] = (float)(o + tau);
 }
 
-// Loewner (Gu-Eisenstat) z, one thread per pole, products in FP64 (svd.cpp:1422-1438)
-__global__ void bdc_lowner(LevelArgs A, int nm)
+// Loewner (Gu-Eisenstat) z, one warp per pole: each lane multiplies the
+// FP64 ratios of its share of j, then a butterfly product combines the lanes
+// (the same product in every lane, so the result is reproducible)
+// (svd.cpp:1422-1438)
+__global__ void __launch_bounds__(256) bdc_lowner(LevelArgs A, int nm)
 {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     const int N = A.N;
     if (g >= N) return;
     int lo = 0, hi = nm - 1, mg = -1;
@@ -542,16 +546,15 @@ __global__ void bdc_lowner(LevelArgs A, int nm)
     const float *ds = A.dsig + s;
     const float *D = A.diff + (long)s * N + s; // D[j*N + i] = d_i^2 - sigma_j^2
     const double dii = ds[i];
-    double p = D[(long)(k - 1) * N + i];
-    for (int j = 0; j < i; j++) {
-        double dj = ds[j];
+    double p = 1.0;
+    for (int j = lane; j < k - 1; j += 32) {
+        double dj = (j < i) ? (double)ds[j] : (double)ds[j + 1];
         p *= (double)D[(long)j * N + i] / ((dii - dj) * (dii + dj));
     }
-    for (int j = i; j < k - 1; j++) {
-        double dj = ds[j + 1];
-        p *= (double)D[(long)j * N + i] / ((dii - dj) * (dii + dj));
-    }
-    A.zhat[s + i] = (float)copysign(sqrt(fabs(p)), A.w.zsec[s + i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) p *= __shfl_xor_sync(0xffffffffu, p, o);
+    p *= (double)D[(long)(k - 1) * N + i];
+    if (lane == 0) A.zhat[s + i] = (float)copysign(sqrt(fabs(p)), A.w.zsec[s + i]);
 }
 
 // normalized singular vectors of the secular problem (svd.cpp:1440-1496)
@@ -734,7 +737,7 @@ int bdc_run(int M, int N, float *a, float *u, float *vt, float *d, float *e, flo
         dim3 g2(ceil_div(L.max_nc, 128), ceil_div(L.max_nc, GATHER_ROWS), L.nm);
         paco_count_launch(), bdc_gather<<<g2, 128, 0, s>>>(A);
         paco_count_launch(), bdc_secular<<<ceil_div((long)N * 32, 256), 256, 0, s>>>(A, L.nm);
-        paco_count_launch(), bdc_lowner<<<ceil_div(N, 128), 128, 0, s>>>(A, L.nm);
+        paco_count_launch(), bdc_lowner<<<ceil_div((long)N * 32, 256), 256, 0, s>>>(A, L.nm);
         paco_count_launch(), bdc_vectors<<<ceil_div((long)N * 32, 256), 256, 0, s>>>(A, L.nm);
         paco_count_launch(), bdc_copyback<<<g2, 128, 0, s>>>(A);
         int tiles_n = ceil_div(L.max_nc, 128);

@@ -453,14 +453,14 @@ __global__ void __launch_bounds__(CP_THREADS) bd_col_pass(BdArgs a, int i, int p
 
 // ---------------------------------------------- compact-WY formation of U, V
 
-// Vp (Lp x NB, ld NB): explicit reflector panel with unit diagonal.
+// Vp (Lp x NBF, ld NBF): explicit block of nbp reflectors with unit diagonal.
 //   column reflectors (U): Vp[r][q] = W[p0+r][p0+q]        (r > q)
 //   row reflectors    (V): Vp[r][q] = W[p0+q][p0+1+r]      (r > q)
 __global__ void bd_panel_vectors(const float *W, long ldw, int p0, int nbp, int Lp, int rowref, float *Vp)
 {
-    long total = (long)Lp * NB;
+    long total = (long)Lp * NBF;
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-        int r = (int)(t / NB), q = (int)(t % NB);
+        int r = (int)(t / NBF), q = (int)(t % NBF);
         float v = 0.f;
         if (q < nbp) {
             if (r == q) v = 1.f;
@@ -470,83 +470,52 @@ __global__ void bd_panel_vectors(const float *W, long ldw, int p0, int nbp, int 
     }
 }
 
-// T (NB x NB, upper triangular) of the forward block reflector
-// H_0 ... H_{nbp-1} = I - Vp T Vp^T, from the Gram matrix Vp^T Vp.
-__global__ void __launch_bounds__(256) bd_gram_t(const float *Vp, int Lp, int nbp, const float *tau, float *T,
-                                                 float *gpart, int *counter)
+// T (NBF x NBF, upper triangular) of the forward block reflector
+// H_0 ... H_{nbp-1} = I - Vp T Vp^T, from the Gram matrix G = Vp^T Vp:
+//   T[q][q] = tau_q,  T[0:q, q] = -tau_q T[0:q, 0:q] G[0:q, q]
+// (the recurrence of LAPACK's larft).  One CTA, columns in sequence.
+__global__ void __launch_bounds__(256) bd_build_t(const float *gram, int nbp, const float *tau, float *T)
 {
-    __shared__ float rows[64][NB + 1];
-    __shared__ int s_flag;
-    __shared__ float G[NB][NB + 1];
-    __shared__ float Ts[NB][NB + 1];
-    __shared__ float w[NB];
+    extern __shared__ float sm_t[];
+    float *Ts = sm_t;                    // NBF x (NBF + 1)
+    float *w = sm_t + NBF * (NBF + 1);   // NBF
     const int tid = threadIdx.x;
-    // each thread owns 4 Gram entries (a, q) with a = tid/8*... : 1024 entries / 256
-    float g[4] = {0.f, 0.f, 0.f, 0.f};
-    const int chunk = (Lp + gridDim.x - 1) / gridDim.x;
-    const int rbeg = blockIdx.x * chunk, rend = min(Lp, rbeg + chunk);
-    for (int r0 = rbeg; r0 < rend; r0 += 64) {
-        int nr = min(64, rend - r0);
-        for (int t = tid; t < 64 * NB; t += 256) {
-            int rr = t / NB, q = t % NB;
-            rows[rr][q] = (rr < nr) ? Vp[(long)(r0 + rr) * NB + q] : 0.f;
-        }
+    for (int t = tid; t < NBF * (NBF + 1); t += blockDim.x) Ts[t] = 0.f;
+    __syncthreads();
+    for (int q = 0; q < nbp; q++) {
+        const float tq = tau[q];
+        if (tid < q) w[tid] = gram[tid * NBF + q];
         __syncthreads();
-        for (int e = 0; e < 4; e++) {
-            int idx = tid + 256 * e, ga = idx / NB, gq = idx % NB;
-            float s = 0.f;
-            for (int rr = 0; rr < nr; rr++) s += rows[rr][ga] * rows[rr][gq];
-            g[e] += s;
+        if (tid < q) {
+            float acc = 0.f;
+            for (int b = tid; b < q; b++) acc += Ts[tid * (NBF + 1) + b] * w[b];
+            Ts[tid * (NBF + 1) + q] = -tq * acc;
         }
+        if (tid == 0) Ts[q * (NBF + 1) + q] = tq;
         __syncthreads();
     }
-    for (int e = 0; e < 4; e++) gpart[(long)blockIdx.x * NB * NB + tid + 256 * e] = g[e];
-    if (!last_block_ticket(counter, gridDim.x, &s_flag)) return;
-    for (int e = 0; e < 4; e++) {
-        int idx = tid + 256 * e;
-        float s = 0.f;
-        for (int bb = 0; bb < (int)gridDim.x; bb++) s += __ldcg(&gpart[(long)bb * NB * NB + idx]);
-        G[idx / NB][idx % NB] = s;
-    }
-    for (int t = tid; t < NB * (NB + 1); t += 256) (&Ts[0][0])[t] = 0.f;
-    __syncthreads();
-    if (tid < 32) {
-        const int l = tid;
-        for (int q = 0; q < nbp; q++) {
-            float tq = tau[q];
-            // T[0:q, q] = -tau_q * T[0:q, 0:q] * G[0:q, q]
-            if (l < q) w[l] = G[l][q];
-            __syncwarp();
-            float s = 0.f;
-            if (l < q)
-                for (int b = l; b < q; b++) s += Ts[l][b] * w[b];
-            __syncwarp();
-            if (l < q) Ts[l][q] = -tq * s;
-            if (l == q) Ts[q][q] = tq;
-            __syncwarp();
-        }
-    }
-    __syncthreads();
-    for (int t = tid; t < NB * NB; t += 256) T[t] = Ts[t / NB][t % NB];
+    for (int t = tid; t < NBF * NBF; t += blockDim.x) T[t] = Ts[(t / NBF) * (NBF + 1) + t % NBF];
 }
 
 // Q_sub <- (I - Vp T Vp^T) Q_sub for Q_sub = Q[off:off+Lp, off:off+Lp] (ld ldq)
 static cudaError_t apply_block_reflector(const BdWs &w, float *Q, long ldq, long off, int Lp, int nbp,
                                          const float *tau, cudaStream_t s)
 {
-    const int gblocks = std::max(1, std::min(RB_CAP, ceil_div(Lp, 256)));
-    paco_count_launch(), bd_gram_t<<<gblocks, 256, 0, s>>>(w.Vp, Lp, nbp, tau, w.T, w.gpart, &w.st->counters[2]);
-    float *Qs = Q + off * ldq + off;
-    // G1 = Vp^T Q_sub  (NB x Lp), split along the long k = Lp dimension
-    int splits = std::max(1, std::min(SPLITS, ceil_div(Lp, 512)));
-    cudaError_t err = gemm_run(nbp, Lp, Lp, 1.f, gop(w.Vp, 1, NB), gop(Qs, ldq, 1), 0.f, w.G1, Lp, splits,
+    const int splits = std::max(1, std::min(SPLITS, ceil_div(Lp, 512)));
+    // G = Vp^T Vp (split along the long k = Lp dimension), then T
+    cudaError_t err = gemm_run(nbp, nbp, Lp, 1.f, gop(w.Vp, 1, NBF), gop(w.Vp, NBF, 1), 0.f, w.gram, NBF, splits,
                                w.gscr, s);
     if (err) return err;
+    paco_count_launch(), bd_build_t<<<1, 256, (NBF * (NBF + 1) + NBF) * sizeof(float), s>>>(w.gram, nbp, tau, w.T);
+    float *Qs = Q + off * ldq + off;
+    // G1 = Vp^T Q_sub  (nbp x Lp)
+    err = gemm_run(nbp, Lp, Lp, 1.f, gop(w.Vp, 1, NBF), gop(Qs, ldq, 1), 0.f, w.G1, Lp, splits, w.gscr, s);
+    if (err) return err;
     // G2 = T G1
-    err = gemm_run(nbp, Lp, nbp, 1.f, gop(w.T, NB, 1), gop(w.G1, Lp, 1), 0.f, w.G2, Lp, 1, nullptr, s);
+    err = gemm_run(nbp, Lp, nbp, 1.f, gop(w.T, NBF, 1), gop(w.G1, Lp, 1), 0.f, w.G2, Lp, 1, nullptr, s);
     if (err) return err;
     // Q_sub -= Vp G2
-    return gemm_run(Lp, Lp, nbp, -1.f, gop(w.Vp, NB, 1), gop(w.G2, Lp, 1), 1.f, Qs, ldq, 1, nullptr, s);
+    return gemm_run(Lp, Lp, nbp, -1.f, gop(w.Vp, NBF, 1), gop(w.G2, Lp, 1), 1.f, Qs, ldq, 1, nullptr, s);
 }
 
 // ------------------------------------------------------------ host driver
@@ -732,6 +701,8 @@ void bd_init_attrs()
     cudaFuncSetAttribute(bd_row_pass<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
     cudaFuncSetAttribute(bd_row_pass<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
     cudaFuncSetAttribute(bd_row_pass<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
+    cudaFuncSetAttribute(bd_build_t, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)((NBF * (NBF + 1) + NBF) * sizeof(float)));
     rp_attrs_set = true;
 }
 
@@ -747,6 +718,14 @@ int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, f
     a.W = w.W; a.Yt = w.Yt; a.X = w.X; a.ypart = w.ypart; a.tpart = w.tpart; a.cpart = w.cpart;
     a.rowbuf = w.rowbuf; a.inv_v0c = w.inv_v0c; a.inv_v0r = w.inv_v0r; a.sc = w.sc;
     a.d = d; a.e = e; a.tauq = tauq; a.taup = taup;
+    // PACO_PK_TRACE=<p0>: phase timestamps of the panel starting at column p0
+    static int trace_env = -2;
+    if (trace_env == -2) {
+        const char *v = getenv("PACO_PK_TRACE");
+        trace_env = v ? atoi(v) : -1;
+    }
+    a.trace = (trace_env >= 0) ? w.trace : nullptr;
+    a.trace_p0 = trace_env;
 
     const int gmax = std::max(1, std::min(RB_CAP, num_sms));
     auto grid_rows = [&](int rows) { return std::max(1, std::min(gmax, ceil_div(rows, RMIN_PER_BLOCK))); };
@@ -801,21 +780,22 @@ int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, f
         }
     }
 
-    // U = H_0 ... H_{N-1} (backward accumulation of the column reflectors)
+    // U = H_0 ... H_{N-1} (backward accumulation of the column reflectors,
+    // NBF reflectors per block update)
     paco_count_launch(), bd_set_identity<<<std::min(8192, ceil_div((long)M * M, 256)), 256, 0, s>>>(u, M, M);
-    for (int p0 = ((N - 1) / NB) * NB; p0 >= 0; p0 -= NB) {
-        int nbp = std::min(N, p0 + NB) - p0, Lp = M - p0;
-        paco_count_launch(), bd_panel_vectors<<<std::min(4096, ceil_div((long)Lp * NB, 256)), 256, 0, s>>>(w.W, w.ldw, p0, nbp, Lp, 0,
-                                                                                       w.Vp);
+    for (int p0 = ((N - 1) / NBF) * NBF; p0 >= 0; p0 -= NBF) {
+        int nbp = std::min(N, p0 + NBF) - p0, Lp = M - p0;
+        paco_count_launch(), bd_panel_vectors<<<std::min(4096, ceil_div((long)Lp * NBF, 256)), 256, 0, s>>>(
+            w.W, w.ldw, p0, nbp, Lp, 0, w.Vp);
         apply_block_reflector(w, u, M, p0, Lp, nbp, tauq + p0, s);
     }
     // V = G_0 ... G_{N-2} (row reflectors), then Vt = V^T
     paco_count_launch(), bd_set_identity<<<std::min(8192, ceil_div((long)N * N, 256)), 256, 0, s>>>(w.Vtmp, N, N);
-    for (int p0 = ((N - 1) / NB) * NB; p0 >= 0; p0 -= NB) {
-        int nbp = std::min(N - 1, p0 + NB) - p0, Lp = N - p0 - 1;
+    for (int p0 = ((N - 1) / NBF) * NBF; p0 >= 0; p0 -= NBF) {
+        int nbp = std::min(N - 1, p0 + NBF) - p0, Lp = N - p0 - 1;
         if (nbp <= 0 || Lp <= 0) continue;
-        paco_count_launch(), bd_panel_vectors<<<std::min(4096, ceil_div((long)Lp * NB, 256)), 256, 0, s>>>(w.W, w.ldw, p0, nbp, Lp, 1,
-                                                                                       w.Vp);
+        paco_count_launch(), bd_panel_vectors<<<std::min(4096, ceil_div((long)Lp * NBF, 256)), 256, 0, s>>>(
+            w.W, w.ldw, p0, nbp, Lp, 1, w.Vp);
         apply_block_reflector(w, w.Vtmp, N, p0 + 1, Lp, nbp, taup + p0, s);
     }
     paco_count_launch(), bd_transpose<<<dim3(ceil_div(N, 32), ceil_div(N, 32)), dim3(32, 8), 0, s>>>(w.Vtmp, vt, N);

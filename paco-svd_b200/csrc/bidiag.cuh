@@ -14,6 +14,7 @@ constexpr int PR = 2 * NB + 8;     // floats per partial record
 constexpr int RMIN_PER_BLOCK = 16; // fewest rows a row-pass CTA is given
 constexpr int SPLITS = 8;          // split-K factor cap for the skinny V^T Q products
 constexpr int PCAP = 512;          // CTA slots of a partial record (>= RB_CAP, CB_CAP)
+constexpr int NBF = 128;           // reflectors per block update when U and V are formed
 }  // namespace bd
 
 struct StepScal {
@@ -40,6 +41,8 @@ struct BdArgs {
     float *W, *Yt, *X, *ypart, *tpart, *cpart, *rowbuf, *inv_v0c, *inv_v0r;
     StepScal *sc;
     float *d, *e, *tauq, *taup;
+    unsigned long long *trace; // phase timestamps of one traced panel (or null)
+    int trace_p0;
 };
 
 struct BdWs {
@@ -55,11 +58,12 @@ struct BdWs {
     float *inv_v0c, *inv_v0r; // N each: 1/v0 of every reflector
     StepScal *sc;
     PkCtl *ctl;
-    float *Vp;     // max(M,N) x NB  explicit reflector panel
-    float *T;      // NB x NB
-    float *gpart;  // RB_CAP x NB*NB
-    float *G1, *G2;// NB x max(M,N)
-    float *gscr;   // SPLITS x NB x max(M,N)
+    unsigned long long *trace; // NB+1 steps x 8 phases x 2 CTAs
+    float *Vp;     // max(M,N) x NBF explicit reflector block (formation of U, V)
+    float *T;      // NBF x NBF
+    float *gram;   // NBF x NBF  Vp^T Vp
+    float *G1, *G2;// NBF x max(M,N)
+    float *gscr;   // SPLITS x NBF x max(M,N)  split-K partial products
     float *Vtmp;   // N x N  (V before the transpose into vt)
 };
 
@@ -90,12 +94,13 @@ static inline size_t bd_carve(void *base, int M, int N, BdWs *w)
     w->inv_v0r = (float *)take(sizeof(float) * N);
     w->sc = (StepScal *)take(sizeof(StepScal));
     w->ctl = (PkCtl *)take(sizeof(PkCtl));
-    w->Vp = (float *)take(sizeof(float) * (size_t)mx * NB);
-    w->T = (float *)take(sizeof(float) * NB * NB);
-    w->gpart = (float *)take(sizeof(float) * (size_t)RB_CAP * NB * NB);
-    w->G1 = (float *)take(sizeof(float) * (size_t)NB * mx);
-    w->G2 = (float *)take(sizeof(float) * (size_t)NB * mx);
-    w->gscr = (float *)take(sizeof(float) * (size_t)SPLITS * NB * mx);
+    w->trace = (unsigned long long *)take(sizeof(unsigned long long) * (NB + 1) * 8 * 2);
+    w->Vp = (float *)take(sizeof(float) * (size_t)mx * NBF);
+    w->T = (float *)take(sizeof(float) * NBF * NBF);
+    w->gram = (float *)take(sizeof(float) * NBF * NBF);
+    w->G1 = (float *)take(sizeof(float) * (size_t)NBF * mx);
+    w->G2 = (float *)take(sizeof(float) * (size_t)NBF * mx);
+    w->gscr = (float *)take(sizeof(float) * (size_t)SPLITS * NBF * mx);
     w->Vtmp = (float *)take(sizeof(float) * (size_t)N * N);
     return (off + 255) & ~(size_t)255;
 }

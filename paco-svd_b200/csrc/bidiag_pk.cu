@@ -83,6 +83,43 @@ __device__ bool pk_wait(PkCtl *c, unsigned g, DevStatus *st, int where, int *s_o
     return *s_ok != 0;
 }
 
+// Sums the per-CTA partial records rec[t * PCAP + cta] (cta < G <= 160) into
+// out[t] for t < nval <= 80.  Every warp issues all of its loads before the
+// first add, so the whole reduction costs one L2 round trip; the sum order is
+// fixed (bitwise reproducible).  Called by every thread of the CTA.
+__device__ __forceinline__ void reduce_records_fast(const float *rec, int G, int nval, float *out)
+{
+    constexpr int NW = RP_THREADS / 32, VPW = 5, LPV = 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float x[VPW][LPV];
+#pragma unroll
+    for (int v = 0; v < VPW; v++) {
+        const int t = warp + NW * v;
+#pragma unroll
+        for (int k = 0; k < LPV; k++) {
+            const int c = lane + 32 * k;
+            x[v][k] = (t < nval && c < G) ? __ldcg(&rec[(long)t * PCAP + c]) : 0.f;
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < VPW; v++) {
+        const int t = warp + NW * v;
+        float sum = 0.f;
+#pragma unroll
+        for (int k = 0; k < LPV; k++) sum += x[v][k];
+        sum = warp_sum(sum);
+        if (lane == 0 && t < nval) out[t] = sum;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ unsigned long long gtimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
 }  // namespace
 
 template <int CPT>
@@ -134,7 +171,13 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
 
     // the panel's steps, then (when a trailing matrix follows) the X-only pass
     const int last_step = (p1 < N) ? p1 : p1 - 1;
+    // optional phase timestamps (block 0 and the last block, thread 0)
+    const bool tracing = a.trace && a.trace_p0 == p0 && tid == 0 && (b == 0 || b == G - 1);
+    auto stamp = [&](int i, int ph) {
+        if (tracing) a.trace[(((i - p0) * 8 + ph) * 2) + (b == 0 ? 0 : 1)] = gtimer();
+    };
     for (int i = p0; i <= last_step && !failed; i++) {
+        stamp(i, 0);
         const bool xonly = (i == p1);
         const bool doX = (i > p0);
         const bool doCol = !xonly;
@@ -181,6 +224,7 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
         const int nact = nown - kfirst;
         const int nbatch = (nact + R - 1) / R;
         __syncthreads();
+        stamp(i, 1);
         if (!resident && tid == 0) {
             proxy_async_fence();
             asm volatile("fence.proxy.async.global;" ::: "memory");
@@ -209,6 +253,9 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
                 if (__syncthreads_or(!ok)) { failed = true; break; }
                 T = tiles + (long)stage * R * L;
             }
+            // X entries of the staged rows, loaded before the dot products so
+            // their latency overlaps them
+            const float xq_pre = (warp < nr && doX && lane < iip) ? a.X[(long)own_row(k0 + warp) * NB + lane] : 0.f;
             if (doX) {
                 float pd[RMAX];
 #pragma unroll
@@ -244,7 +291,7 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
                     a.W[(long)r * ldw + (i - 1)] = aq;
                     if (resident) trow[lane] = aq;
                 }
-                float xq = (doX && lane < iip) ? a.X[(long)r * NB + lane] : 0.f;
+                const float xq = xq_pre;
                 float Xn = 0.f;
                 if (doX) {
                     float dot = 0.f;
@@ -296,6 +343,7 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
             }
         }
         if (__syncthreads_or(failed)) { failed = true; break; }
+        stamp(i, 2);
         if (xonly) break; // the X-only pass ends the panel
 
         // row-pass partials and barrier A
@@ -306,8 +354,10 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
         }
         if (warp < RMAX) {
             if (lane == 0) s_part[warp][0] = w_ss;
-            s_part[warp][1 + lane] = w_g1;
-            s_part[warp][1 + NB + lane] = w_g2;
+            if (lane < ii) {
+                s_part[warp][1 + lane] = w_g1;
+                s_part[warp][1 + ii + lane] = w_g2;
+            }
         }
         __syncthreads();
         for (int t = tid; t < PR; t += RP_THREADS) {
@@ -315,25 +365,49 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
             for (int w = 0; w < RMAX; w++) v += s_part[w][t];
             a.tpart[(long)t * PCAP + b] = v;
         }
+        // operands of this CTA's first column-pass chunk do not depend on the
+        // barrier: load them now so their latency hides behind it
+        const int nchunk = (i < N - 1) ? (N - i - 1 + 31) / 32 : 0;
+        float pY[2] = {0.f, 0.f}, pW[2] = {0.f, 0.f}, pwij = 0.f;
+        if (b < nchunk) {
+            const int j = i + 1 + b * 32 + lane;
+            if (j < N) {
+                pwij = __ldcg(&a.W[(long)i * ldw + j]);
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    int q = 2 * warp + e;
+                    if (q < ii) {
+                        pY[e] = __ldcg(&a.Yt[(long)q * ldw + j]);
+                        pW[e] = __ldcg(&a.W[(long)(p0 + q) * ldw + j]);
+                    }
+                }
+            }
+        }
+        stamp(i, 3);
         if (pk_arrive(ctl, G, &s_flag, &s_gen)) {
-            reduce_records(a.tpart, G, 1 + 2 * NB, s_red);
+            // every load of this phase is issued before the first use
+            const float wi = (tid < ii) ? __ldcg(&a.W[(long)i * ldw + p0 + tid]) : 0.f;
+            const float xi = (tid < ii) ? __ldcg(&a.X[(long)i * NB + tid]) : 0.f;
+            const float x0 = __ldcg(&a.sc->x0col);
+            reduce_records_fast(a.tpart, G, 1 + 2 * ii, s_red);
             if (tid == 0) {
                 float beta, tau, v0;
-                make_reflector(__ldcg(&a.sc->x0col), s_red[0], M - i, &beta, &tau, &v0);
+                make_reflector(x0, s_red[0], M - i, &beta, &tau, &v0);
                 a.d[i] = beta; a.tauq[i] = tau; a.inv_v0c[i] = 1.f / v0;
                 s_v0 = v0;
             }
             __syncthreads();
             if (tid < ii) {
                 float inv = 1.f / s_v0;
-                a.sc->t1[tid] = __ldcg(&a.W[(long)i * ldw + p0 + tid]) + s_red[1 + tid] * inv;
-                a.sc->t2[tid] = __ldcg(&a.X[(long)i * NB + tid]) + s_red[1 + NB + tid] * inv;
+                a.sc->t1[tid] = wi + s_red[1 + tid] * inv;
+                a.sc->t2[tid] = xi + s_red[1 + ii + tid] * inv;
             }
             pk_release(ctl);
         } else if (!pk_wait(ctl, s_gen, st, 300 + i, &s_ok)) {
             failed = true;
             break;
         }
+        stamp(i, 4);
         if (i >= N - 1) break; // no row reflector after the last column
 
         // --------------------------------------------------- column pass
@@ -347,7 +421,6 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
         }
         for (int t = tid; t < PR; t += RP_THREADS) s_cpart[t] = 0.f;
         __syncthreads();
-        const int nchunk = (N - i - 1 + 31) / 32;
         for (int ch = b; ch < nchunk; ch += G) {
             const int j = i + 1 + ch * 32 + lane;
             const bool valid = j < N;
@@ -363,12 +436,13 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
             cy[warp][lane] = ys;
             // warp w owns panel indices q in [2w, 2w+2)
             float Yq[2], Wq[2], pa = 0.f, pb = 0.f;
+            const bool first = (ch == b);
 #pragma unroll
             for (int e = 0; e < 2; e++) {
                 int q = 2 * warp + e;
                 bool use = valid && q < ii;
-                Yq[e] = use ? __ldcg(&a.Yt[(long)q * ldw + j]) : 0.f;
-                Wq[e] = use ? __ldcg(&a.W[(long)(p0 + q) * ldw + j]) : 0.f;
+                Yq[e] = first ? pY[e] : (use ? __ldcg(&a.Yt[(long)q * ldw + j]) : 0.f);
+                Wq[e] = first ? pW[e] : (use ? __ldcg(&a.W[(long)(p0 + q) * ldw + j]) : 0.f);
                 pa += Yq[e] * s_t1[q] + Wq[e] * s_t2[q];
                 pb += Yq[e] * s_ai[q] + Wq[e] * s_xi[q];
             }
@@ -380,7 +454,7 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
             for (int w = 0; w < RP_THREADS / 32; w++) { y += cy[w][lane]; sa += cA[w][lane]; sb += cB[w][lane]; }
             float Ynew = 0.f, aj = 0.f;
             if (valid) {
-                float wij = __ldcg(&a.W[(long)i * ldw + j]);
+                float wij = first ? pwij : __ldcg(&a.W[(long)i * ldw + j]);
                 Ynew = tq * (wij + y * invc_i - sa);
                 aj = wij - Ynew - sb;
                 if (warp == 0) {
@@ -395,7 +469,7 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
                 int q = 2 * warp + e;
                 if (q < ii) {
                     float g3 = warp_sum(Yq[e] * m), g4 = warp_sum(Wq[e] * m);
-                    if (lane == 0) { s_cpart[1 + q] += g3; s_cpart[NB + 2 + q] += g4; }
+                    if (lane == 0) { s_cpart[1 + q] += g3; s_cpart[2 + ii + q] += g4; }
                 }
             }
             if (warp == 0) {
@@ -404,24 +478,29 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
             }
             __syncthreads();
         }
+        stamp(i, 5);
         for (int t = tid; t < PR; t += RP_THREADS) a.cpart[(long)t * PCAP + b] = s_cpart[t];
         if (pk_arrive(ctl, G, &s_flag, &s_gen)) {
-            reduce_records(a.cpart, G, 2 * NB + 2, s_red);
+            const float yt = (tid <= ii) ? __ldcg(&a.Yt[(long)tid * ldw + i + 1]) : 0.f;
+            const float wt4 = (tid < ii) ? __ldcg(&a.W[(long)(p0 + tid) * ldw + i + 1]) : 0.f;
+            const float x0 = __ldcg(&a.sc->x0row);
+            reduce_records_fast(a.cpart, G, 2 + 2 * ii, s_red);
             if (tid == 0) {
                 float beta, tau, v0;
-                make_reflector(__ldcg(&a.sc->x0row), s_red[0], N - i - 1, &beta, &tau, &v0);
+                make_reflector(x0, s_red[0], N - i - 1, &beta, &tau, &v0);
                 a.e[i] = beta; a.taup[i] = tau; a.inv_v0r[i] = 1.f / v0;
                 s_v0 = v0;
             }
             __syncthreads();
             float inv = 1.f / s_v0;
-            if (tid <= ii) a.sc->t3[tid] = __ldcg(&a.Yt[(long)tid * ldw + i + 1]) + s_red[1 + tid] * inv;
-            if (tid < ii) a.sc->t4[tid] = __ldcg(&a.W[(long)(p0 + tid) * ldw + i + 1]) + s_red[NB + 2 + tid] * inv;
+            if (tid <= ii) a.sc->t3[tid] = yt + s_red[1 + tid] * inv;
+            if (tid < ii) a.sc->t4[tid] = wt4 + s_red[2 + ii + tid] * inv;
             pk_release(ctl);
         } else if (!pk_wait(ctl, s_gen, st, 400 + i, &s_ok)) {
             failed = true;
             break;
         }
+        stamp(i, 6);
     }
 }
 

@@ -56,6 +56,16 @@ extern "C" {
 
 unsigned long long paco_launch_count(void) { return g_launches; }
 
+// Byte offset, within the stage-1 workspace, of the phase timestamps written
+// when PACO_PK_TRACE is set (a debugging aid; not part of the public header).
+size_t paco_debug_trace_offset(int M, int N)
+{
+    BdWs w;
+    char *base = (char *)(uintptr_t)(1u << 20); // any 256-byte aligned base
+    bd_carve(base, M, N, &w);
+    return (size_t)((char *)w.trace - base);
+}
+
 const char *paco_version(void) { return "paco-svd-b200 1.0 (sm_100a)"; }
 
 void paco_profile_enable(int on)
@@ -260,7 +270,7 @@ int paco_svd(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws
 // loads the library holds these bytes until the process exits.
 #define PACO_NOALLOC_MAX_M 1024
 #define PACO_NOALLOC_MAX_N 512
-#define PACO_NOALLOC_BYTES (12u << 20)
+#define PACO_NOALLOC_BYTES (16u << 20)
 static __device__ __align__(256) unsigned char g_noalloc_scratch[PACO_NOALLOC_BYTES];
 
 namespace {

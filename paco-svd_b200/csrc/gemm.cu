@@ -2,19 +2,24 @@
 #include "gemm.cuh"
 
 __global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, float alpha, GemmOp A, GemmOp B,
-                                                   float beta, float *C, long ldc, int splits, float *scratch)
+                                                   float beta, float *C, long ldc, int splits, float *scratch,
+                                                   int fast)
 {
     using namespace gemm_cfg;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-    if (splits <= 1) {
-        gemm_tile(M, N, 0, K, alpha, A, B, beta, C, ldc, m0, n0);
-        return;
+    int kb = 0, ke = K;
+    float al = alpha, be = beta;
+    float *Cd = C;
+    long ld = ldc;
+    if (splits > 1) {
+        const int z = blockIdx.z;
+        int kchunk = ((K + splits - 1) / splits + 15) / 16 * 16;
+        kb = min(K, z * kchunk);
+        ke = min(K, kb + kchunk);
+        al = 1.f; be = 0.f; Cd = scratch + (long)z * M * N; ld = N;
     }
-    const int z = blockIdx.z;
-    int kchunk = ((K + splits - 1) / splits + BK - 1) / BK * BK;
-    int kb = z * kchunk, ke = min(K, kb + kchunk);
-    if (kb > K) kb = K;
-    gemm_tile(M, N, kb, ke, 1.0f, A, B, 0.f, scratch + (long)z * M * N, N, m0, n0);
+    if (fast) gemm_tile_fast(M, N, kb, ke, al, A, B, be, Cd, ld, m0, n0);
+    else gemm_tile(M, N, kb, ke, al, A, B, be, Cd, ld, m0, n0);
 }
 
 __global__ void gemm_splitk_reduce(int M, int N, int splits, float alpha, const float *scratch, float beta,
@@ -39,7 +44,8 @@ cudaError_t gemm_run(int M, int N, int K, float alpha, GemmOp A, GemmOp B, float
     if (M <= 0 || N <= 0) return cudaSuccess;
     if (splits < 1 || !scratch) splits = 1;
     dim3 grid(ceil_div(N, BN), ceil_div(M, BM), splits);
-    paco_count_launch(), gemm_kernel<<<grid, THREADS, 0, s>>>(M, N, K, alpha, A, B, beta, C, ldc, splits, scratch);
+    const int fast = gemm_fast_ok(A, B) ? 1 : 0;
+    paco_count_launch(), gemm_kernel<<<grid, THREADS, 0, s>>>(M, N, K, alpha, A, B, beta, C, ldc, splits, scratch, fast);
     if (splits > 1) {
         long total = (long)M * N;
         int blocks = (int)std::min<long>(4096, (total + 255) / 256);

@@ -101,3 +101,8 @@ def test_svd_main_reports_short_input(tmp_path):
     r = subprocess.run([exe, "--args", str(tmp_path / "args.txt"), "--input", str(tmp_path / "A.bin"),
                         "--output", str(tmp_path / "out")], capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "expected" in r.stderr
+
+
+def test_noalloc_scratch_covers_its_largest_shape():
+    # paco_svd_noalloc serves M <= 1024, N <= 512 from a 16 MiB device array
+    assert P.lib().paco_svd_workspace_size(1024, 512) <= 16 << 20
