@@ -718,6 +718,8 @@ int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, f
     a.W = w.W; a.Yt = w.Yt; a.X = w.X; a.ypart = w.ypart; a.tpart = w.tpart; a.cpart = w.cpart;
     a.rowbuf = w.rowbuf; a.inv_v0c = w.inv_v0c; a.inv_v0r = w.inv_v0r; a.sc = w.sc;
     a.d = d; a.e = e; a.tauq = tauq; a.taup = taup;
+    a.bcA = w.bcA; a.bcB = w.bcB;
+    unsigned pk_cnt = 0; // arrivals on the persistent kernel's barrier counter so far
     // PACO_PK_TRACE=<p0>: phase timestamps of the panel starting at column p0
     static int trace_env = -2;
     if (trace_env == -2) {
@@ -750,7 +752,7 @@ int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, f
         if (use_pk) {
             cudaEvent_t e0 = nullptr, e1 = nullptr;
             if (g_prof.on) prof_record(e0 = prof_event(), s);
-            pk = bd_panel_pk_launch(a, w.ctl, p0, p1, Gp, s);
+            pk = bd_panel_pk_launch(a, w.ctl, p0, p1, Gp, &pk_cnt, s);
             if (g_prof.on) {
                 prof_record(e1 = prof_event(), s);
                 g_prof.cur.ev.push_back(e0);

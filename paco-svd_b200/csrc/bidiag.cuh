@@ -43,6 +43,7 @@ struct BdArgs {
     float *d, *e, *tauq, *taup;
     unsigned long long *trace; // phase timestamps of one traced panel (or null)
     int trace_p0;
+    float *bcA, *bcB; // broadcast slots of the persistent kernel's reflectors
 };
 
 struct BdWs {
@@ -59,6 +60,7 @@ struct BdWs {
     StepScal *sc;
     PkCtl *ctl;
     unsigned long long *trace; // NB+1 steps x 8 phases x 2 CTAs
+    float *bcA, *bcB;          // PR each: pivot and panel entries of a reflector
     float *Vp;     // max(M,N) x NBF explicit reflector block (formation of U, V)
     float *T;      // NBF x NBF
     float *gram;   // NBF x NBF  Vp^T Vp
@@ -95,6 +97,8 @@ static inline size_t bd_carve(void *base, int M, int N, BdWs *w)
     w->sc = (StepScal *)take(sizeof(StepScal));
     w->ctl = (PkCtl *)take(sizeof(PkCtl));
     w->trace = (unsigned long long *)take(sizeof(unsigned long long) * (NB + 1) * 8 * 2);
+    w->bcA = (float *)take(sizeof(float) * PR);
+    w->bcB = (float *)take(sizeof(float) * PR);
     w->Vp = (float *)take(sizeof(float) * (size_t)mx * NBF);
     w->T = (float *)take(sizeof(float) * NBF * NBF);
     w->gram = (float *)take(sizeof(float) * NBF * NBF);
@@ -143,7 +147,7 @@ static __device__ __forceinline__ void reduce_records(const float *rec, int ncta
     __syncthreads();
 }
 
-bool bd_panel_pk_launch(const BdArgs &a, PkCtl *ctl, int p0, int p1, int G, cudaStream_t s);
+bool bd_panel_pk_launch(const BdArgs &a, PkCtl *ctl, int p0, int p1, int G, unsigned *cnt, cudaStream_t s);
 void bd_pk_init_attrs();
 
 size_t bd_workspace_bytes(int M, int N);

@@ -1,21 +1,29 @@
 // Persistent panel kernel of the stage-1 bidiagonalization.
 //
-// One cooperative launch (one CTA per SM) runs all NB column steps of a
-// panel [p0, p1).  Each step is the row pass (row-parallel: finish X for the
-// previous row reflector, update column i, accumulate A^T x) and the column
-// pass (column-parallel: Y(:, i), row i, row-reflector partials), separated
-// by grid barriers.  At each barrier the CTA that arrives last sums the
-// per-CTA partials in CTA order (bitwise reproducible), forms the reflector
-// and only then releases the others.  Barrier waits are bounded: a CTA that
-// waits for ~2 s of SM clock records PACO_ERR_TIMEOUT, raises the abort flag
-// and returns, and the others follow at their next barrier.
+// One cooperative launch (one CTA per SM at most) runs all NB column steps of
+// a panel [p0, p1).  Each step is
+//   row pass     (row-parallel)    finish X for the previous row reflector,
+//                                  update column i, accumulate A^T x
+//   barrier A    every CTA sums the row-pass partial records itself and forms
+//                the column reflector (same inputs, same order: identical in
+//                every CTA)
+//   column pass  (column-parallel) Y(:, i), row i, row-reflector partials
+//   barrier B    every CTA sums those records and forms the row reflector
+// The barriers count arrivals on one monotonic counter (barrier k of a launch
+// completes at cnt_base + (k+1)*G), so a barrier costs an arrival, a poll and
+// the one round trip that fetches the partial records.  The exact values a
+// reflector needs besides the sums (its pivot, the panel entries of row i,
+// the panel entries at column i+1) are written by their owner into small
+// broadcast slots.  Waits are bounded: a CTA that waits ~2 s of SM clock
+// records PACO_ERR_TIMEOUT, raises the abort flag and returns; the others
+// follow at their next barrier.
 //
 // Rows are owned cyclically (row r belongs to CTA (r - p0) % G).  When a
 // CTA's rows [p0, N) fit in shared memory they are staged once per panel and
-// kept resident for its NB steps, so the trailing matrix is read from HBM
-// once per panel instead of once per step; otherwise they are re-staged with
-// TMA bulk copies at every step (double-buffered).  Data that other CTAs wrote
-// earlier in the same launch is read with ld.global.cg (L2), never from L1.
+// stay resident for its NB steps, so the trailing matrix is read from HBM once
+// per panel instead of once per step; otherwise they are re-staged with TMA
+// bulk copies at every step (double-buffered).  Data other CTAs wrote earlier
+// in the same launch is read with ld.global.cg (L2), never from L1.
 #include "bidiag.cuh"
 #include "tma.cuh"
 
@@ -30,43 +38,23 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
     return v;
 }
 
-// Grid barrier, part 1: returns true in the CTA that arrived last.  That CTA
-// finishes the phase (its reduction) and then calls pk_release; every other
-// CTA calls pk_wait.
-__device__ bool pk_arrive(PkCtl *c, int G, int *s_flag, unsigned *s_gen)
+__device__ __forceinline__ unsigned long long gtimer()
 {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned g = ld_acquire(&c->gen);
-        __threadfence();
-        unsigned t = atomicAdd(&c->cnt, 1u);
-        *s_gen = g;
-        *s_flag = (t == (unsigned)G - 1);
-    }
-    __syncthreads();
-    const bool last = *s_flag != 0;
-    if (last) __threadfence();
-    return last;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
 }
 
-__device__ void pk_release(PkCtl *c)
+// Arrive at a grid barrier and wait (bounded) until `target` arrivals.
+__device__ bool pk_barrier(PkCtl *c, unsigned target, DevStatus *st, int where, int *s_ok)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
-        atomicExch(&c->cnt, 0u);
         __threadfence();
-        atomicAdd(&c->gen, 1u);
-    }
-    __syncthreads();
-}
-
-// Bounded wait for the generation to move past g; false if the launch aborts.
-__device__ bool pk_wait(PkCtl *c, unsigned g, DevStatus *st, int where, int *s_ok)
-{
-    if (threadIdx.x == 0) {
+        atomicAdd(&c->cnt, 1u);
         int ok = 1;
         long long t0 = clock64();
-        while (ld_acquire(&c->gen) == g) {
+        while (ld_acquire(&c->cnt) < target) {
             if (ld_acquire(&c->abort)) { ok = 0; break; }
             if (clock64() - t0 > 4000000000LL) {
                 atomicAdd(&st->wait_timeouts, 1);
@@ -85,8 +73,8 @@ __device__ bool pk_wait(PkCtl *c, unsigned g, DevStatus *st, int where, int *s_o
 
 // Sums the per-CTA partial records rec[t * PCAP + cta] (cta < G <= 160) into
 // out[t] for t < nval <= 80.  Every warp issues all of its loads before the
-// first add, so the whole reduction costs one L2 round trip; the sum order is
-// fixed (bitwise reproducible).  Called by every thread of the CTA.
+// first add, so the reduction costs one L2 round trip; the sum order is fixed
+// (bitwise reproducible).  Called by every thread of the CTA.
 __device__ __forceinline__ void reduce_records_fast(const float *rec, int G, int nval, float *out)
 {
     constexpr int NW = RP_THREADS / 32, VPW = 5, LPV = 5;
@@ -113,32 +101,24 @@ __device__ __forceinline__ void reduce_records_fast(const float *rec, int G, int
     __syncthreads();
 }
 
-__device__ __forceinline__ unsigned long long gtimer()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-    return t;
-}
-
 }  // namespace
 
 template <int CPT>
 __global__ void __launch_bounds__(RP_THREADS, 1)
-    bd_panel_pk(BdArgs a, PkCtl *ctl, int p0, int p1, int resident, int R)
+    bd_panel_pk(BdArgs a, PkCtl *ctl, int p0, int p1, int resident, int R, unsigned cnt_base)
 {
     extern __shared__ __align__(128) float tiles[];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ float red[RP_THREADS / 32][RMAX];
     __shared__ float xs[RMAX];
-    __shared__ float s_t3[NB + 1], s_t4[NB], s_ycol[NB], s_wcol[NB];
-    __shared__ float s_t1[NB], s_t2[NB], s_ai[NB], s_xi[NB];
+    __shared__ float s_t3[NB + 1], s_t4[NB], s_ycol[NB], s_wcol[NB]; // row reflector of step i-1
+    __shared__ float s_t1[NB], s_t2[NB], s_ai[NB], s_xi[NB];         // column reflector of step i
     __shared__ float s_part[RMAX][PR];
-    __shared__ float s_red[PR];
+    __shared__ float s_red[PR], s_bc[PR];
     __shared__ float cy[RP_THREADS / 32][32], cA[RP_THREADS / 32][32], cB[RP_THREADS / 32][32];
     __shared__ float s_cpart[PR];
-    __shared__ int s_flag, s_ok;
-    __shared__ unsigned s_gen;
-    __shared__ float s_v0;
+    __shared__ int s_ok;
+    __shared__ float s_rtaup, s_rinv, s_ctau, s_cinv, s_cinv_prev;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int M = a.M, N = a.N, G = gridDim.x, b = blockIdx.x;
@@ -148,11 +128,13 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
     // rows owned by this CTA: p0 + b + k*G, k < nown
     const int nown = (M - p0 - b + G - 1) / G > 0 ? (M - p0 - b + G - 1) / G : 0;
     auto own_row = [&](int k) { return p0 + b + k * G; };
+    unsigned nbar = 0;
 
     if (tid == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
         mbar_init_fence();
+        s_cinv_prev = 1.f;
     }
     __syncthreads();
     uint32_t phase0 = 0, phase1 = 0;
@@ -171,7 +153,6 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
 
     // the panel's steps, then (when a trailing matrix follows) the X-only pass
     const int last_step = (p1 < N) ? p1 : p1 - 1;
-    // optional phase timestamps (block 0 and the last block, thread 0)
     const bool tracing = a.trace && a.trace_p0 == p0 && tid == 0 && (b == 0 || b == G - 1);
     auto stamp = [&](int i, int ph) {
         if (tracing) a.trace[(((i - p0) * 8 + ph) * 2) + (b == 0 ? 0 : 1)] = gtimer();
@@ -182,43 +163,72 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
         const bool doX = (i > p0);
         const bool doCol = !xonly;
         const int ii = i - p0, iip = ii - 1;
-        const float invr = doX ? __ldcg(&a.inv_v0r[i - 1]) : 0.f;
-        const float taup_prev = doX ? __ldcg(&a.taup[i - 1]) : 0.f;
-        const float invc = (ii >= 1) ? __ldcg(&a.inv_v0c[i - 1]) : 1.f;
+
+        // ------------- finish the row reflector of step i-1 (every CTA)
+        float4 u4[CPT], acc4[CPT];
+        if (doX) {
+            // all loads of this phase in flight together
+            const int nbc = 2 + 2 * iip;
+            const float bcv = (tid < nbc) ? __ldcg(&a.bcB[tid]) : 0.f;
+            float4 rb[CPT];
+#pragma unroll
+            for (int k = 0; k < CPT; k++) {
+                int c = p0 + 4 * (tid + k * RP_THREADS);
+                rb[k] = (c < ldw) ? __ldcg(reinterpret_cast<const float4 *>(a.rowbuf + c))
+                                  : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            reduce_records_fast(a.cpart, G, nbc, s_red);
+            if (tid < nbc) s_bc[tid] = bcv;
+            __syncthreads();
+            if (tid == 0) {
+                float beta, tau, v0;
+                make_reflector(s_bc[0], s_red[0], N - (i - 1) - 1, &beta, &tau, &v0);
+                s_rtaup = tau;
+                s_rinv = 1.f / v0;
+                if (b == 0) { a.e[i - 1] = beta; a.taup[i - 1] = tau; a.inv_v0r[i - 1] = 1.f / v0; }
+            }
+            __syncthreads();
+            const float inv = s_rinv;
+            // t3 = Y^T u (ii values), t4 = U u (iip values); next column's panel entries
+            if (tid <= iip) {
+                s_t3[tid] = s_bc[1 + tid] + s_red[1 + tid] * inv;
+                s_ycol[tid] = s_bc[1 + tid];                              // Y[i, q], q < ii
+            }
+            if (tid < iip) {
+                s_t4[tid] = s_bc[2 + iip + tid] + s_red[2 + iip + tid] * inv;
+                s_wcol[tid] = s_bc[2 + iip + tid];                        // U[q, i], q < iip
+            }
+            if (tid == iip) s_wcol[tid] = 1.f;                            // implicit 1 of row i-1
+#pragma unroll
+            for (int k = 0; k < CPT; k++) {
+                int c = p0 + 4 * (tid + k * RP_THREADS);
+                float r[4] = {rb[k].x, rb[k].y, rb[k].z, rb[k].w};
+                float uv[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    int j = c + e;
+                    uv[e] = (j == i) ? 1.f : ((j > i && j < N) ? r[e] * inv : 0.f);
+                }
+                u4[k] = make_float4(uv[0], uv[1], uv[2], uv[3]);
+            }
+            // the scaled row reflector goes into row i-1 of W (later column passes
+            // and the panel's trailing update read it)
+            if (b == 0) {
+                for (int j = i + 1 + tid; j < N; j += RP_THREADS)
+                    a.W[(long)(i - 1) * ldw + j] = __ldcg(&a.rowbuf[j]) * inv;
+                if (xonly && tid == 0) a.W[(long)(i - 1) * ldw + i] = 1.f;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < CPT; k++) u4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int k = 0; k < CPT; k++) acc4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int t = tid; t < RMAX * PR; t += RP_THREADS) (&s_part[0][0])[t] = 0.f;
+        const float taup_prev = doX ? s_rtaup : 0.f;
+        const float invc = (ii >= 1) ? s_cinv_prev : 1.f;
 
         // ------------------------------------------------------ row pass
-        float4 u4[CPT], acc4[CPT];
-#pragma unroll
-        for (int k = 0; k < CPT; k++) {
-            int c = p0 + 4 * (tid + k * RP_THREADS);
-            float uv[4];
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-                int j = c + e;
-                float v = 0.f;
-                if (doX) {
-                    if (j == i) v = 1.f;
-                    else if (j > i && j < N) v = __ldcg(&a.rowbuf[j]) * invr;
-                }
-                uv[e] = v;
-            }
-            u4[k] = make_float4(uv[0], uv[1], uv[2], uv[3]);
-            acc4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        if (tid <= NB) s_t3[tid] = (doX && tid <= iip) ? __ldcg(&a.sc->t3[tid]) : 0.f;
-        if (tid < NB) {
-            s_t4[tid] = (doX && tid < iip) ? __ldcg(&a.sc->t4[tid]) : 0.f;
-            s_ycol[tid] = (doCol && tid < ii) ? __ldcg(&a.Yt[(long)tid * ldw + i]) : 0.f;
-            s_wcol[tid] = (doCol && tid < ii) ? ((tid == ii - 1) ? 1.f : __ldcg(&a.W[(long)(p0 + tid) * ldw + i]))
-                                               : 0.f;
-        }
-        for (int t = tid; t < RMAX * PR; t += RP_THREADS) (&s_part[0][0])[t] = 0.f;
-        if (doX && b == 0) {
-            for (int j = i + 1 + tid; j < N; j += RP_THREADS)
-                a.W[(long)(i - 1) * ldw + j] = __ldcg(&a.rowbuf[j]) * invr;
-            if (xonly && tid == 0) a.W[(long)(i - 1) * ldw + i] = 1.f;
-        }
-        // owned rows that are active in this step (r >= i)
         int kfirst = 0;
         while (kfirst < nown && own_row(kfirst) < i) kfirst++;
         const int nact = nown - kfirst;
@@ -245,6 +255,10 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
             const int k0 = kfirst + bb * R, nr = min(R, nown - k0);
             const float *T;
             const int stage = bb & 1;
+            // X entries of the staged rows, loaded before the dot products so
+            // their latency overlaps them
+            const float xq_pre =
+                (warp < nr && doX && lane < iip) ? a.X[(long)own_row(k0 + warp) * NB + lane] : 0.f;
             if (resident) {
                 T = tiles + (long)k0 * L;
             } else {
@@ -253,9 +267,6 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
                 if (__syncthreads_or(!ok)) { failed = true; break; }
                 T = tiles + (long)stage * R * L;
             }
-            // X entries of the staged rows, loaded before the dot products so
-            // their latency overlaps them
-            const float xq_pre = (warp < nr && doX && lane < iip) ? a.X[(long)own_row(k0 + warp) * NB + lane] : 0.f;
             if (doX) {
                 float pd[RMAX];
 #pragma unroll
@@ -310,9 +321,15 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
                         a.W[(long)r * ldw + i] = xr;
                         if (resident) trow[ii] = xr;
                         xs[rr] = xr;
-                        if (r == i) a.sc->x0col = xr;
                     }
-                    if (r > i) {
+                    if (r == i) {
+                        // pivot and row-i panel entries for every CTA's column reflector
+                        if (lane == 0) a.bcA[0] = xr;
+                        if (lane < ii) {
+                            a.bcA[1 + lane] = aq;
+                            a.bcA[1 + ii + lane] = xrq;
+                        }
+                    } else if (r > i) {
                         if (lane == 0) w_ss += xr * xr;
                         if (lane < ii) { w_g1 += aq * xr; w_g2 += xrq * xr; }
                     }
@@ -346,7 +363,7 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
         stamp(i, 2);
         if (xonly) break; // the X-only pass ends the panel
 
-        // row-pass partials and barrier A
+        // row-pass partials: A^T x (all tile columns), |x|^2, V^T x, X^T x
 #pragma unroll
         for (int k = 0; k < CPT; k++) {
             int c4 = tid + k * RP_THREADS;
@@ -384,43 +401,39 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
             }
         }
         stamp(i, 3);
-        if (pk_arrive(ctl, G, &s_flag, &s_gen)) {
-            // every load of this phase is issued before the first use
-            const float wi = (tid < ii) ? __ldcg(&a.W[(long)i * ldw + p0 + tid]) : 0.f;
-            const float xi = (tid < ii) ? __ldcg(&a.X[(long)i * NB + tid]) : 0.f;
-            const float x0 = __ldcg(&a.sc->x0col);
+        if (!pk_barrier(ctl, cnt_base + (++nbar) * G, st, 300 + i, &s_ok)) { failed = true; break; }
+
+        // ------------- column reflector of step i (every CTA)
+        {
+            const int nbc = 1 + 2 * ii;
+            const float bcv = (tid < nbc) ? __ldcg(&a.bcA[tid]) : 0.f;
             reduce_records_fast(a.tpart, G, 1 + 2 * ii, s_red);
+            if (tid < nbc) s_bc[tid] = bcv;
+            __syncthreads();
             if (tid == 0) {
                 float beta, tau, v0;
-                make_reflector(x0, s_red[0], M - i, &beta, &tau, &v0);
-                a.d[i] = beta; a.tauq[i] = tau; a.inv_v0c[i] = 1.f / v0;
-                s_v0 = v0;
+                make_reflector(s_bc[0], s_red[0], M - i, &beta, &tau, &v0);
+                s_ctau = tau;
+                s_cinv = 1.f / v0;
+                s_cinv_prev = 1.f / v0; // scales column i's entries in the next step
+                if (b == 0) { a.d[i] = beta; a.tauq[i] = tau; a.inv_v0c[i] = 1.f / v0; }
             }
             __syncthreads();
             if (tid < ii) {
-                float inv = 1.f / s_v0;
-                a.sc->t1[tid] = wi + s_red[1 + tid] * inv;
-                a.sc->t2[tid] = xi + s_red[1 + ii + tid] * inv;
+                const float inv = s_cinv;
+                s_ai[tid] = s_bc[1 + tid];                                  // V[i, q] (row i panel entries)
+                s_xi[tid] = s_bc[1 + ii + tid];                             // X[i, q]
+                s_t1[tid] = s_bc[1 + tid] + s_red[1 + tid] * inv;           // V^T v
+                s_t2[tid] = s_bc[1 + ii + tid] + s_red[1 + ii + tid] * inv; // X^T v
             }
-            pk_release(ctl);
-        } else if (!pk_wait(ctl, s_gen, st, 300 + i, &s_ok)) {
-            failed = true;
-            break;
+            for (int t = tid; t < PR; t += RP_THREADS) s_cpart[t] = 0.f;
+            __syncthreads();
         }
         stamp(i, 4);
         if (i >= N - 1) break; // no row reflector after the last column
 
         // --------------------------------------------------- column pass
-        const float tq = __ldcg(&a.tauq[i]), invc_i = __ldcg(&a.inv_v0c[i]);
-        if (tid < NB) {
-            bool q = tid < ii;
-            s_t1[tid] = q ? __ldcg(&a.sc->t1[tid]) : 0.f;
-            s_t2[tid] = q ? __ldcg(&a.sc->t2[tid]) : 0.f;
-            s_ai[tid] = q ? __ldcg(&a.W[(long)i * ldw + p0 + tid]) : 0.f;
-            s_xi[tid] = q ? __ldcg(&a.X[(long)i * NB + tid]) : 0.f;
-        }
-        for (int t = tid; t < PR; t += RP_THREADS) s_cpart[t] = 0.f;
-        __syncthreads();
+        const float tq = s_ctau, invc_i = s_cinv;
         for (int ch = b; ch < nchunk; ch += G) {
             const int j = i + 1 + ch * 32 + lane;
             const bool valid = j < N;
@@ -460,7 +473,21 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
                 if (warp == 0) {
                     a.Yt[(long)ii * ldw + j] = Ynew;
                     a.rowbuf[j] = aj;
-                    if (j == i + 1) a.sc->x0row = aj;
+                }
+            }
+            if (j == i + 1) {
+                // pivot and column-(i+1) panel entries for every CTA's row reflector
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    int q = 2 * warp + e;
+                    if (q < ii) {
+                        a.bcB[1 + q] = Yq[e];
+                        a.bcB[2 + ii + q] = Wq[e];
+                    }
+                }
+                if (warp == 0) {
+                    a.bcB[0] = aj;
+                    a.bcB[1 + ii] = Ynew;
                 }
             }
             float m = (valid && j >= i + 2) ? aj : 0.f;
@@ -480,33 +507,24 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
         }
         stamp(i, 5);
         for (int t = tid; t < PR; t += RP_THREADS) a.cpart[(long)t * PCAP + b] = s_cpart[t];
-        if (pk_arrive(ctl, G, &s_flag, &s_gen)) {
-            const float yt = (tid <= ii) ? __ldcg(&a.Yt[(long)tid * ldw + i + 1]) : 0.f;
-            const float wt4 = (tid < ii) ? __ldcg(&a.W[(long)(p0 + tid) * ldw + i + 1]) : 0.f;
-            const float x0 = __ldcg(&a.sc->x0row);
-            reduce_records_fast(a.cpart, G, 2 + 2 * ii, s_red);
-            if (tid == 0) {
-                float beta, tau, v0;
-                make_reflector(x0, s_red[0], N - i - 1, &beta, &tau, &v0);
-                a.e[i] = beta; a.taup[i] = tau; a.inv_v0r[i] = 1.f / v0;
-                s_v0 = v0;
-            }
-            __syncthreads();
-            float inv = 1.f / s_v0;
-            if (tid <= ii) a.sc->t3[tid] = yt + s_red[1 + tid] * inv;
-            if (tid < ii) a.sc->t4[tid] = wt4 + s_red[2 + ii + tid] * inv;
-            pk_release(ctl);
-        } else if (!pk_wait(ctl, s_gen, st, 400 + i, &s_ok)) {
-            failed = true;
-            break;
-        }
+        if (!pk_barrier(ctl, cnt_base + (++nbar) * G, st, 400 + i, &s_ok)) { failed = true; break; }
         stamp(i, 6);
     }
 }
 
+// Grid barriers one launch for panel [p0, p1) passes (host and kernel agree):
+// barrier A at every step, barrier B at every step but a last column.
+static unsigned pk_barriers(int N, int p0, int p1)
+{
+    const int nbp = p1 - p0;
+    return (unsigned)(2 * nbp - (p1 == N ? 1 : 0));
+}
+
 // Host side: launches the persistent kernel for panel [p0, p1) cooperatively.
-// Returns false when a cooperative launch of G CTAs is not possible.
-bool bd_panel_pk_launch(const BdArgs &a, PkCtl *ctl, int p0, int p1, int G, cudaStream_t s)
+// *cnt is the arrival counter's value before the launch; it is advanced by
+// the arrivals this launch makes.  Returns false when a cooperative launch of
+// G CTAs is not possible.
+bool bd_panel_pk_launch(const BdArgs &a, PkCtl *ctl, int p0, int p1, int G, unsigned *cnt, cudaStream_t s)
 {
     const int L = (int)(a.ldw - p0);
     const int own = (a.M - p0 + G - 1) / G;
@@ -521,9 +539,15 @@ bool bd_panel_pk_launch(const BdArgs &a, PkCtl *ctl, int p0, int p1, int G, cuda
     else if (chunks == 2) fn = (void *)bd_panel_pk<2>;
     else fn = (void *)bd_panel_pk<4>;
     BdArgs aa = a;
-    void *args[] = {&aa, &ctl, &p0, &p1, &resident, &R};
+    unsigned base = *cnt;
+    void *args[] = {&aa, &ctl, &p0, &p1, &resident, &R, &base};
     paco_count_launch();
-    return cudaLaunchCooperativeKernel(fn, dim3(G), dim3(RP_THREADS), args, smem, s) == cudaSuccess;
+    if (cudaLaunchCooperativeKernel(fn, dim3(G), dim3(RP_THREADS), args, smem, s) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    *cnt = base + pk_barriers(a.N, p0, p1) * (unsigned)G;
+    return true;
 }
 
 void bd_pk_init_attrs()
@@ -535,14 +559,4 @@ void bd_pk_init_attrs()
     cudaFuncSetAttribute(bd_panel_pk<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
     cudaFuncSetAttribute(bd_panel_pk<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
     done = true;
-}
-
-// CTAs per SM the persistent kernel can keep resident (for the grid size)
-int bd_pk_max_blocks_per_sm(int L)
-{
-    size_t smem = (size_t)200 * 1024;
-    (void)L;
-    int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, bd_panel_pk<4>, RP_THREADS, smem);
-    return nb;
 }
