@@ -704,6 +704,7 @@ void bdc_init_attrs()
 {
     if (!bdc_attrs_set) {
         cudaFuncSetAttribute(bdc_prepare, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        gemm_tc_init_attrs();
         bdc_attrs_set = true;
     }
 }
@@ -746,10 +747,11 @@ int bdc_run(int M, int N, float *a, float *u, float *vt, float *d, float *e, flo
     }
     paco_count_launch(), bdc_sort_desc<<<ceil_div(N, 256), 256, 0, s>>>(N, d, w.perm, w.sig);
     // U[:, :N] <- U[:, :N] Q with Q(:, r) = qt row perm[r]; result staged in a (M x N)
-    gemm_run(M, N, N, 1.f, gop(u, M, 1), gop(qt, 1, N, w.perm), 0.f, a, N, 1, nullptr, s);
+    gemm_any(M, N, N, 1.f, gop(u, M, 1), gop(qt, 1, N, w.perm), 0.f, a, N, 1, nullptr, w.tcs, w.tcs_floats, w.st, s);
     paco_count_launch(), bdc_copy_cols<<<std::min(8192, ceil_div((long)M * N, 256)), 256, 0, s>>>(a, N, u, M, M, N);
     // Vt <- W^T Vt with W^T row r = wt row perm[r]; staged in Us
-    gemm_run(N, N, N, 1.f, gop(wt, N, 1, w.perm), gop(vt, N, 1), 0.f, w.Us, N, 1, nullptr, s);
+    gemm_any(N, N, N, 1.f, gop(wt, N, 1, w.perm), gop(vt, N, 1), 0.f, w.Us, N, 1, nullptr, w.tcs, w.tcs_floats, w.st,
+             s);
     paco_count_launch(), bdc_copy_cols<<<std::min(8192, ceil_div((long)N * N, 256)), 256, 0, s>>>(w.Us, N, vt, N, N, N);
     paco_count_launch(), bdc_copy_vec<<<ceil_div(N, 256), 256, 0, s>>>(w.sig, d, N);
     return cudaGetLastError() == cudaSuccess ? PACO_OK : PACO_ERR_CUDA;

@@ -2,6 +2,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "gemm_tc.cuh"
 
 // Tiling blob written by GenerateTiling and read by svd_DC (replaces the
 // SVDTiling + SVDSubmatrixInfo stack of svd_tiling.cpp:21-26, 83-130).
@@ -35,6 +36,8 @@ struct BdcWs {
     int *mg_s, *mg_m, *mg_e;     // merges of all levels, level after level
     int *perm;        // N: final descending order
     float *sig;       // N: sorted singular values
+    float *tcs;       // tensor-core GEMM scratch of the final products; null when unused
+    size_t tcs_floats;
 };
 
 static inline size_t bdc_carve(void *base, int M, int N, BdcWs *w)
@@ -61,6 +64,9 @@ static inline size_t bdc_carve(void *base, int M, int N, BdcWs *w)
     w->mg_e = (int *)take(sizeof(int) * nleaf);
     w->perm = (int *)take(sizeof(int) * N);
     w->sig = (float *)take(sizeof(float) * N);
+    const int shapes[2][3] = {{M, N, N}, {N, N, N}};
+    w->tcs_floats = std::max(M, N) > 1024 ? gemm_tc_scratch_for(shapes, 2) : 0;
+    w->tcs = w->tcs_floats ? (float *)take(sizeof(float) * w->tcs_floats) : nullptr;
     return (off + 255) & ~(size_t)255;
 }
 

@@ -509,13 +509,16 @@ static cudaError_t apply_block_reflector(const BdWs &w, float *Q, long ldq, long
     paco_count_launch(), bd_build_t<<<1, 256, (NBF * (NBF + 1) + NBF) * sizeof(float), s>>>(w.gram, nbp, tau, w.T);
     float *Qs = Q + off * ldq + off;
     // G1 = Vp^T Q_sub  (nbp x Lp)
-    err = gemm_run(nbp, Lp, Lp, 1.f, gop(w.Vp, 1, NBF), gop(Qs, ldq, 1), 0.f, w.G1, Lp, splits, w.gscr, s);
+    err = gemm_any(nbp, Lp, Lp, 1.f, gop(w.Vp, 1, NBF), gop(Qs, ldq, 1), 0.f, w.G1, Lp, splits, w.gscr, w.tcs,
+                   w.tcs_floats, w.st, s);
     if (err) return err;
     // G2 = T G1
-    err = gemm_run(nbp, Lp, nbp, 1.f, gop(w.T, NBF, 1), gop(w.G1, Lp, 1), 0.f, w.G2, Lp, 1, nullptr, s);
+    err = gemm_any(nbp, Lp, nbp, 1.f, gop(w.T, NBF, 1), gop(w.G1, Lp, 1), 0.f, w.G2, Lp, 1, nullptr, w.tcs,
+                   w.tcs_floats, w.st, s);
     if (err) return err;
     // Q_sub -= Vp G2
-    return gemm_run(Lp, Lp, nbp, -1.f, gop(w.Vp, NBF, 1), gop(w.G2, Lp, 1), 1.f, Qs, ldq, 1, nullptr, s);
+    return gemm_any(Lp, Lp, nbp, -1.f, gop(w.Vp, NBF, 1), gop(w.G2, Lp, 1), 1.f, Qs, ldq, 1, nullptr, w.tcs,
+                    w.tcs_floats, w.st, s);
 }
 
 // ------------------------------------------------------------ host driver
@@ -703,6 +706,7 @@ void bd_init_attrs()
     cudaFuncSetAttribute(bd_row_pass<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
     cudaFuncSetAttribute(bd_build_t, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)((NBF * (NBF + 1) + NBF) * sizeof(float)));
+    gemm_tc_init_attrs();
     rp_attrs_set = true;
 }
 
@@ -776,7 +780,8 @@ int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, f
             A.p2 = w.X + (long)p1 * NB; A.rs2 = NB; A.cs2 = 1; A.ksplit = nbp;
             GemmOp B = gop(w.Yt + p1, w.ldw, 1);
             B.p2 = w.W + (long)p0 * w.ldw + p1; B.rs2 = w.ldw; B.cs2 = 1; B.ksplit = nbp;
-            gemm_run(M - p1, N - p1, 2 * nbp, -1.f, A, B, 1.f, w.W + (long)p1 * w.ldw + p1, w.ldw, 1, nullptr, s);
+            gemm_any(M - p1, N - p1, 2 * nbp, -1.f, A, B, 1.f, w.W + (long)p1 * w.ldw + p1, w.ldw, 1, nullptr, w.tcs,
+                     w.tcs_floats, w.st, s);
         } else if (M > N) {
             paco_count_launch(), bd_scale_last_col<<<std::min(1024, ceil_div(M - N, 256)), 256, 0, s>>>(w.W, w.ldw, M, N, w.inv_v0c);
         }

@@ -2,6 +2,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "gemm_tc.cuh"
 
 namespace bd {
 constexpr int NB = 32;             // panel width (reflectors per block update)
@@ -67,6 +68,8 @@ struct BdWs {
     float *G1, *G2;// NBF x max(M,N)
     float *gscr;   // SPLITS x NBF x max(M,N)  split-K partial products
     float *Vtmp;   // N x N  (V before the transpose into vt)
+    float *tcs;    // tensor-core GEMM scratch (operand images, split-K partials); null when unused
+    size_t tcs_floats;
 };
 
 // Lays the stage-1 buffers out in `base` (may be null to only measure);
@@ -106,6 +109,11 @@ static inline size_t bd_carve(void *base, int M, int N, BdWs *w)
     w->G2 = (float *)take(sizeof(float) * (size_t)NBF * mx);
     w->gscr = (float *)take(sizeof(float) * (size_t)SPLITS * NBF * mx);
     w->Vtmp = (float *)take(sizeof(float) * (size_t)N * N);
+    // products sent to the tensor cores: G1 = Vp^T Q, G2 = T G1, Q -= Vp G2 and
+    // the panel trailing update (matrices up to 1024 stay on the SIMT engine)
+    const int shapes[4][3] = {{NBF, (int)mx, (int)mx}, {NBF, (int)mx, NBF}, {(int)mx, (int)mx, NBF}, {M, N, 2 * NB}};
+    w->tcs_floats = mx > 1024 ? gemm_tc_scratch_for(shapes, 4) : 0;
+    w->tcs = w->tcs_floats ? (float *)take(sizeof(float) * w->tcs_floats) : nullptr;
     return (off + 255) & ~(size_t)255;
 }
 

@@ -66,6 +66,33 @@ size_t paco_debug_trace_offset(int M, int N)
     return (size_t)((char *)w.trace - base);
 }
 
+// Test hook (not part of the public header): one strided product
+// C = alpha * opA * opB + beta * C on the SIMT engine (mode 0) or the tensor
+// cores (mode 1), opA(m, k) = A[m * a_rs + k * a_cs], opB(k, n) = B[k * b_rs + n * b_cs].
+// `ws` starts with the status block; the rest is GEMM scratch.  Synchronous.
+size_t paco_debug_gemm_ws_bytes(int M, int N, int K)
+{
+    return 256 + sizeof(float) * std::max(gemm_tc_scratch_floats(M, N, K), (size_t)8 * M * N);
+}
+
+int paco_debug_gemm(int M, int N, int K, float alpha, const float *A, long a_rs, long a_cs, const float *B, long b_rs,
+                    long b_cs, float beta, float *C, long ldc, int mode, void *ws, size_t ws_bytes, void *stream)
+{
+    if (M <= 0 || N <= 0 || K <= 0 || !A || !B || !C || !ws || ws_bytes < paco_debug_gemm_ws_bytes(M, N, K))
+        return PACO_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    DevStatus *st = (DevStatus *)ws;
+    float *scr = (float *)((char *)ws + 256);
+    bd_init_attrs();
+    cudaMemsetAsync(st, 0, sizeof(DevStatus), s);
+    cudaError_t err = mode == 1 ? gemm_tc_run(M, N, K, alpha, gop(A, a_rs, a_cs), gop(B, b_rs, b_cs), beta, C, ldc,
+                                              scr, st, s)
+                                : gemm_run(M, N, K, alpha, gop(A, a_rs, a_cs), gop(B, b_rs, b_cs), beta, C, ldc,
+                                           std::min(8, std::max(1, K / 512)), scr, s);
+    if (err != cudaSuccess) return PACO_ERR_CUDA;
+    return paco_sync_status(ws, stream, nullptr);
+}
+
 const char *paco_version(void) { return "paco-svd-b200 1.0 (sm_100a)"; }
 
 void paco_profile_enable(int on)

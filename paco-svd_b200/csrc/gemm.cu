@@ -37,6 +37,15 @@ __global__ void gemm_splitk_reduce(int M, int N, int splits, float alpha, const 
     }
 }
 
+cudaError_t gemm_splitk_reduce_run(int M, int N, int splits, float alpha, const float *scratch, float beta,
+                                   float *C, long ldc, cudaStream_t s)
+{
+    long total = (long)M * N;
+    int blocks = (int)std::min<long>(4096, (total + 255) / 256);
+    paco_count_launch(), gemm_splitk_reduce<<<blocks, 256, 0, s>>>(M, N, splits, alpha, scratch, beta, C, ldc);
+    return cudaGetLastError();
+}
+
 cudaError_t gemm_run(int M, int N, int K, float alpha, GemmOp A, GemmOp B, float beta, float *C, long ldc,
                      int splits, float *scratch, cudaStream_t s)
 {
@@ -46,10 +55,6 @@ cudaError_t gemm_run(int M, int N, int K, float alpha, GemmOp A, GemmOp B, float
     dim3 grid(ceil_div(N, BN), ceil_div(M, BM), splits);
     const int fast = gemm_fast_ok(A, B) ? 1 : 0;
     paco_count_launch(), gemm_kernel<<<grid, THREADS, 0, s>>>(M, N, K, alpha, A, B, beta, C, ldc, splits, scratch, fast);
-    if (splits > 1) {
-        long total = (long)M * N;
-        int blocks = (int)std::min<long>(4096, (total + 255) / 256);
-        paco_count_launch(), gemm_splitk_reduce<<<blocks, 256, 0, s>>>(M, N, splits, alpha, scratch, beta, C, ldc);
-    }
+    if (splits > 1) return gemm_splitk_reduce_run(M, N, splits, alpha, scratch, beta, C, ldc, s);
     return cudaGetLastError();
 }

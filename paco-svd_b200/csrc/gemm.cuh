@@ -292,3 +292,8 @@ static inline bool gemm_fast_ok(const GemmOp &A, const GemmOp &B)
 // deterministic second pass sums them in split order.
 cudaError_t gemm_run(int M, int N, int K, float alpha, GemmOp A, GemmOp B, float beta, float *C,
                      long ldc, int splits, float *scratch, cudaStream_t s);
+
+// C = alpha * sum_z scratch[z] + beta * C over `splits` partial M x N products
+// (row-major, ld N), summed in split order.
+cudaError_t gemm_splitk_reduce_run(int M, int N, int splits, float alpha, const float *scratch, float beta,
+                                   float *C, long ldc, cudaStream_t s);

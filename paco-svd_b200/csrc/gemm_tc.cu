@@ -1,0 +1,358 @@
+// FP32 GEMM on the 5th-generation tensor cores (tcgen05, sm_100a), accurate
+// to about FP32 through a 3xTF32 split:  x = x_hi + x_lo with x_hi, x_lo TF32,
+//     A*B ~= A_lo*B_hi + A_hi*B_lo + A_hi*B_hi      (FP32 accumulation in TMEM)
+//
+// tc_pack  rounds one operand into its hi/lo TF32 parts and writes them as
+//          ready-made shared-memory tile images: 128 rows x 32 k, K-major,
+//          128-byte swizzle (16-byte chunk c of row r stored at chunk
+//          c ^ (r & 7)), so the GEMM kernel moves whole tiles with 1-D bulk
+//          copies.  One CTA per image, transposed through shared memory so
+//          both the reads and the writes are coalesced.
+// tc_gemm  one CTA per 128x128 tile of C (and per k-range with split-K):
+//          thread 0 runs a 3-stage pipeline of bulk copies (mbarrier
+//          complete_tx) and issues the MMAs (tcgen05.mma.cta_group::1
+//          .kind::tf32, M=128, N=128, K=8) into a TMEM accumulator; a
+//          tcgen05.commit per stage releases the stage.  The 4 warps then read
+//          the accumulator with tcgen05.ld, stage it through shared memory and
+//          write C = alpha*AB + beta*C with coalesced rows.
+// Every wait is bounded; a wait that gives up records PACO_ERR_TIMEOUT, the
+// copies still in flight are waited for (again bounded), the CTA frees its
+// tensor memory and returns.
+#include <algorithm>
+#include <cstdlib>
+
+#include "gemm_tc.cuh"
+#include "tma.cuh"
+
+namespace {
+
+constexpr int TM = 128, TN = 128, TK = 32;  // tile of C; k per image (128 bytes of TF32)
+constexpr int IMG = TM * TK;                // floats per tile image (16 KB)
+constexpr int STAGES = 3;
+constexpr int MAX_SPLITS = 8;
+constexpr uint32_t IDESC = (1u << 4)             // D format F32
+                           | (2u << 7)           // A format TF32
+                           | (2u << 10)          // B format TF32 (both K-major: bits 15, 16 clear)
+                           | ((TN >> 3) << 17)   // N >> 3
+                           | ((TM >> 4) << 24);  // M >> 4
+
+__device__ __forceinline__ float tf32_round(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// Shared-memory matrix descriptor for a K-major, 128-byte-swizzled tile whose
+// 8-row groups are 1024 bytes apart (start address 1024-aligned for k = 0).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFF) >> 4);  // start address >> 4
+    d |= (uint64_t)1 << 16;                   // leading byte offset (not used by this layout)
+    d |= (uint64_t)(1024 >> 4) << 32;         // stride byte offset >> 4
+    d |= (uint64_t)1 << 46;                   // descriptor version 1
+    d |= (uint64_t)2 << 61;                   // 128-byte swizzle
+    return d;
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t accum)
+{
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n}\n" ::"r"(tmem),
+        "l"(ad), "l"(bd), "r"(IDESC), "r"(accum), "r"(z));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
+          "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+          "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+struct TcGeom {
+    int MT, NT, KT, splits;
+};
+
+TcGeom tc_geom(int M, int N, int K)
+{
+    TcGeom g;
+    g.MT = ceil_div(M, TM);
+    g.NT = ceil_div(N, TN);
+    g.KT = ceil_div(K, TK);
+    // enough CTAs to cover the SMs, at least 4 images of k per split
+    const int tiles = g.MT * g.NT;
+    g.splits = std::max(1, std::min({MAX_SPLITS, ceil_div(148, tiles), g.KT / 4}));
+    return g;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ packing
+
+// Operand X with R rows and K columns, element (r, k) = opA(r, k) (or opB(k, r)
+// when `transposed`); writes hi and lo images, image (rt, kt) at
+// (rt * KT + kt) * IMG floats.  One CTA of 256 threads per image.
+__global__ void __launch_bounds__(256) tc_pack(GemmOp X, int transposed, int R, int K, int KT, float *hi,
+                                               float *lo)
+{
+    __shared__ float tile[TM][TK + 1];
+    const int img = blockIdx.x;
+    const int rt = img / KT, kt = img % KT;
+    const int t = threadIdx.x;
+    const bool kfast = transposed ? (X.rs == 1) : (X.cs == 1);
+#pragma unroll 4
+    for (int i = 0; i < 16; i++) {
+        int r, k;
+        if (kfast) { r = i * 8 + (t >> 5); k = t & 31; }
+        else { r = t & 127; k = i * 2 + (t >> 7); }
+        const int gr = rt * TM + r, gk = kt * TK + k;
+        float v = 0.f;
+        if (gr < R && gk < K) v = transposed ? gop_b(X, gk, gr) : gop_a(X, gr, gk);
+        tile[r][k] = v;
+    }
+    __syncthreads();
+    const long base = (long)img * IMG;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int chunk = i * 256 + t;         // 16-byte chunk of the image
+        const int r = chunk >> 3, pos = chunk & 7;
+        const int k0 = (pos ^ (r & 7)) << 2;   // logical k of that chunk
+        float4 h, l;
+        float v;
+        v = tile[r][k0 + 0]; h.x = tf32_round(v); l.x = tf32_round(v - h.x);
+        v = tile[r][k0 + 1]; h.y = tf32_round(v); l.y = tf32_round(v - h.y);
+        v = tile[r][k0 + 2]; h.z = tf32_round(v); l.z = tf32_round(v - h.z);
+        v = tile[r][k0 + 3]; h.w = tf32_round(v); l.w = tf32_round(v - h.w);
+        reinterpret_cast<float4 *>(hi + base)[chunk] = h;
+        reinterpret_cast<float4 *>(lo + base)[chunk] = l;
+    }
+}
+
+// ------------------------------------------------------------------ GEMM
+
+__global__ void __launch_bounds__(128, 1)
+    tc_gemm(int M, int N, int KT, int kper, float alpha, const float *Ahi, const float *Alo, const float *Bhi,
+            const float *Blo, float beta, float *C, long ldc, float *part, DevStatus *st)
+{
+    extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nt = blockIdx.x, mt = blockIdx.y, z = blockIdx.z;
+    const int kb0 = z * kper, kb1 = min(KT, kb0 + kper);
+    const int nk = max(0, kb1 - kb0);
+    // stage buffers [stage][Ahi, Alo, Bhi, Blo][IMG], 1024-byte aligned for the swizzle
+    float *stage = (float *)(tc_smem_raw + ((1024u - (smem_u32(tc_smem_raw) & 1023u)) & 1023u));
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(TN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&done, 1);
+        mbar_init_fence();
+        s_fail = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+
+    if (tid == 0) {
+        const long abase = (long)mt * KT * IMG, bbase = (long)nt * KT * IMG;
+        auto produce = [&](int j) {  // k-block j of this split into stage j % STAGES
+            float *dst = stage + (long)(j % STAGES) * 4 * IMG;
+            uint64_t *bar = &full[j % STAGES];
+            const long ko = (long)(kb0 + j) * IMG;
+            mbar_expect_tx(bar, 4u * IMG * 4u);
+            tma_load_1d(dst + 0 * IMG, Ahi + abase + ko, IMG * 4u, bar);
+            tma_load_1d(dst + 1 * IMG, Alo + abase + ko, IMG * 4u, bar);
+            tma_load_1d(dst + 2 * IMG, Bhi + bbase + ko, IMG * 4u, bar);
+            tma_load_1d(dst + 3 * IMG, Blo + bbase + ko, IMG * 4u, bar);
+        };
+        int issued = 0, consumed = 0;
+        for (; issued < nk && issued < STAGES; issued++) produce(issued);
+        bool ok = true;
+        for (int kb = 0; kb < nk && ok; kb++) {
+            const int s = kb % STAGES;
+            if (!mbar_wait_bounded(&full[s], (kb / STAGES) & 1, st, 500)) {
+                ok = false;
+                break;
+            }
+            consumed = kb + 1;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t base = smem_u32(stage + (long)s * 4 * IMG);
+            const uint64_t ahi = smem_desc(base), alo = smem_desc(base + IMG * 4);
+            const uint64_t bhi = smem_desc(base + 2 * IMG * 4), blo = smem_desc(base + 3 * IMG * 4);
+#pragma unroll
+            for (int j = 0; j < TK / 8; j++) {
+                const uint64_t dk = (uint64_t)(j * 32 >> 4);  // 8 TF32 = 32 bytes along k
+                mma_tf32(tmem, alo + dk, bhi + dk, (kb | j) ? 1u : 0u);
+                mma_tf32(tmem, ahi + dk, blo + dk, 1u);
+                mma_tf32(tmem, ahi + dk, bhi + dk, 1u);
+            }
+            mma_commit(&empty[s]);
+            // refill the stage the previous k-block used once its MMAs are done
+            if (kb >= 1 && issued < nk) {
+                const int pk = kb - 1;
+                if (!mbar_wait_bounded(&empty[pk % STAGES], (pk / STAGES) & 1, st, 501)) {
+                    ok = false;
+                    break;
+                }
+                produce(issued);
+                issued++;
+            }
+        }
+        if (!ok) {
+            s_fail = 1;
+            // copies still in flight land before the CTA may exit
+            for (int j = consumed; j < issued; j++)
+                mbar_wait_bounded(&full[j % STAGES], (j / STAGES) & 1, st, 503, 1000000000LL);
+        }
+        mma_commit(&done);  // arrives when every MMA issued above has completed
+    }
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(&done, 0, st, 502);
+    if (!ok) s_fail = 1;
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+    if (!s_fail) {
+        float *Cd = C;
+        long ld = ldc;
+        float al = alpha, be = beta;
+        if (part) {
+            Cd = part + (long)z * M * N;
+            ld = N;
+            al = 1.f;
+            be = 0.f;
+        }
+        const bool empty_k = (nk == 0);  // the accumulator was never written: the product is 0
+        // warp w owns TMEM lanes 32w..32w+31 (rows of the tile); staged per 32x32
+        // block through shared memory so each store instruction writes one row
+        float(*sb)[33] = reinterpret_cast<float(*)[33]>(stage + warp * 32 * 33);
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int c0 = 0; c0 < TN; c0 += 32) {
+            uint32_t v[32];
+            tmem_ld32(taddr + (uint32_t)c0, v);
+#pragma unroll
+            for (int q = 0; q < 32; q++) sb[lane][q] = __uint_as_float(v[q]);
+            __syncwarp();
+            const int n = nt * TN + c0 + lane;
+            if (n < N) {
+#pragma unroll 4
+                for (int rr = 0; rr < 32; rr++) {
+                    const int m = mt * TM + warp * 32 + rr;
+                    if (m >= M) break;
+                    float *c = Cd + (long)m * ld + n;
+                    float x = empty_k ? 0.f : al * sb[rr][lane];
+                    if (be != 0.f) x = fmaf(be, *c, x);
+                    *c = x;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN) : "memory");
+}
+
+// ------------------------------------------------------------------ host
+
+static size_t tc_smem_bytes() { return (size_t)STAGES * 4 * IMG * sizeof(float) + 1024; }
+
+size_t gemm_tc_scratch_floats(int M, int N, int K)
+{
+    if (M <= 0 || N <= 0 || K <= 0) return 0;
+    const TcGeom g = tc_geom(M, N, K);
+    size_t f = (size_t)2 * (g.MT + g.NT) * g.KT * IMG;
+    if (g.splits > 1) f += (size_t)g.splits * M * N;
+    return f;
+}
+
+bool gemm_tc_enabled()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *e = getenv("PACO_TC");
+        on = (e && e[0] == '0') ? 0 : 1;
+    }
+    return on == 1;
+}
+
+void gemm_tc_init_attrs()
+{
+    cudaFuncSetAttribute(tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes());
+}
+
+cudaError_t gemm_tc_run(int M, int N, int K, float alpha, GemmOp A, GemmOp B, float beta, float *C, long ldc,
+                        float *scratch, DevStatus *st, cudaStream_t s)
+{
+    if (M <= 0 || N <= 0) return cudaSuccess;
+    K = std::max(K, 1);
+    const TcGeom g = tc_geom(M, N, K);
+    float *Ahi = scratch, *Alo = Ahi + (size_t)g.MT * g.KT * IMG;
+    float *Bhi = Alo + (size_t)g.MT * g.KT * IMG, *Blo = Bhi + (size_t)g.NT * g.KT * IMG;
+    float *part = g.splits > 1 ? Blo + (size_t)g.NT * g.KT * IMG : nullptr;
+    const int kper = ceil_div(g.KT, g.splits);
+    paco_count_launch(), tc_pack<<<g.MT * g.KT, 256, 0, s>>>(A, 0, M, K, g.KT, Ahi, Alo);
+    paco_count_launch(), tc_pack<<<g.NT * g.KT, 256, 0, s>>>(B, 1, N, K, g.KT, Bhi, Blo);
+    paco_count_launch(), tc_gemm<<<dim3(g.NT, g.MT, g.splits), 128, tc_smem_bytes(), s>>>(
+                             M, N, g.KT, kper, alpha, Ahi, Alo, Bhi, Blo, beta, C, ldc, part, st);
+    if (part) return gemm_splitk_reduce_run(M, N, g.splits, alpha, part, beta, C, ldc, s);
+    return cudaGetLastError();
+}
+
+// Products below this many multiply-adds stay on the SIMT engine: the packing
+// passes and the 3 MMAs per k-step do not pay for themselves there.
+static constexpr double TC_MIN_MACS = (double)(1 << 26);
+
+static bool tc_shape_ok(int M, int N, int K)
+{
+    return M >= 64 && N >= 64 && K >= 32 && (double)M * N * K >= TC_MIN_MACS;
+}
+
+cudaError_t gemm_any(int M, int N, int K, float alpha, GemmOp A, GemmOp B, float beta, float *C, long ldc,
+                     int splits, float *simt_scratch, float *tc_scratch, size_t tc_floats, DevStatus *st,
+                     cudaStream_t s)
+{
+    if (tc_scratch && gemm_tc_enabled() && tc_shape_ok(M, N, K) && gemm_tc_scratch_floats(M, N, K) <= tc_floats)
+        return gemm_tc_run(M, N, K, alpha, A, B, beta, C, ldc, tc_scratch, st, s);
+    return gemm_run(M, N, K, alpha, A, B, beta, C, ldc, splits, simt_scratch, s);
+}
+
+size_t gemm_tc_scratch_for(const int (*shapes)[3], int n)
+{
+    size_t f = 0;
+    for (int i = 0; i < n; i++)
+        if (tc_shape_ok(shapes[i][0], shapes[i][1], shapes[i][2]))
+            f = std::max(f, gemm_tc_scratch_floats(shapes[i][0], shapes[i][1], shapes[i][2]));
+    return f;
+}

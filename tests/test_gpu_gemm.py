@@ -1,0 +1,86 @@
+"""The tensor-core (tcgen05, 3xTF32) product against a float64 product and the
+SIMT engine, on the operand layouts the SVD pipeline uses: row-major and
+transposed operands, partial 128-tiles, split-K, beta = 0 and beta = 1.
+Called through the library's test hook paco_debug_gemm."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import pacosvd as P
+
+pytestmark = pytest.mark.gpu
+
+
+def _hook():
+    L = P.lib()
+    if not hasattr(L, "_gemm_hook"):
+        vp, i, lg, f = ctypes.c_void_p, ctypes.c_int, ctypes.c_long, ctypes.c_float
+        L.paco_debug_gemm_ws_bytes.argtypes = [i, i, i]
+        L.paco_debug_gemm_ws_bytes.restype = ctypes.c_size_t
+        L.paco_debug_gemm.argtypes = [i, i, i, f, vp, lg, lg, vp, lg, lg, f, vp, lg, i, vp, ctypes.c_size_t, vp]
+        L.paco_debug_gemm.restype = i
+        L._gemm_hook = True
+    return L
+
+
+def run_gemm(A, B, C, alpha, beta, mode, a_trans=False, b_trans=False):
+    """C (M x N, torch cuda) <- alpha op(A) op(B) + beta C; op = transpose when *_trans."""
+    import torch
+    L = _hook()
+    M, N = C.shape
+    K = A.shape[0] if a_trans else A.shape[1]
+    a_rs, a_cs = (1, A.stride(0)) if a_trans else (A.stride(0), 1)
+    b_rs, b_cs = (1, B.stride(0)) if b_trans else (B.stride(0), 1)
+    nbytes = L.paco_debug_gemm_ws_bytes(M, N, K)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    rc = L.paco_debug_gemm(M, N, K, alpha, A.data_ptr(), a_rs, a_cs, B.data_ptr(), b_rs, b_cs, beta,
+                           C.data_ptr(), C.stride(0), mode, ws.data_ptr(), nbytes, None)
+    torch.cuda.synchronize()
+    assert rc == P.PACO_OK, rc
+
+
+SHAPES = [
+    (128, 128, 32, False, False),
+    (256, 384, 256, False, False),
+    (200, 130, 70, False, False),      # partial tiles in m, n, k
+    (128, 4096, 4096, True, False),    # G1 = Vp^T Q: one m-tile, split-K
+    (1000, 1100, 64, False, False),    # trailing update shape
+    (517, 517, 517, False, True),      # W^T-like transposed B
+    (96, 64, 1300, True, True),
+]
+
+
+@pytest.mark.parametrize("M,N,K,at,bt", SHAPES)
+@pytest.mark.parametrize("beta", [0.0, 1.0])
+def test_tensor_core_product_matches_float64(M, N, K, at, bt, beta):
+    import torch
+    g = torch.Generator().manual_seed(M * 7 + N * 3 + K)
+    A64 = torch.randn((K, M) if at else (M, K), generator=g, dtype=torch.float64)
+    B64 = torch.randn((N, K) if bt else (K, N), generator=g, dtype=torch.float64)
+    C64 = torch.randn((M, N), generator=g, dtype=torch.float64)
+    A, B = A64.float().cuda(), B64.float().cuda()
+    opA = (A64.float().double().T if at else A64.float().double())
+    opB = (B64.float().double().T if bt else B64.float().double())
+    ref = -1.0 * (opA @ opB) + beta * C64.float().double()
+    scale = (opA.abs() @ opB.abs()).max().item() + beta * C64.abs().max().item()
+    for mode in (1, 0):
+        C = C64.float().cuda()
+        run_gemm(A, B, C, -1.0, beta, mode, at, bt)
+        err = (C.double().cpu() - ref).abs().max().item()
+        # 3xTF32 keeps about FP32 accuracy: well under 1e-5 of the |A||B| scale
+        assert err <= 1e-5 * scale, (mode, err, scale)
+
+
+def test_tensor_core_product_is_deterministic():
+    import torch
+    g = torch.Generator().manual_seed(5)
+    A = torch.randn(128, 3000, generator=g).cuda()
+    B = torch.randn(3000, 640, generator=g).cuda()
+    outs = []
+    for _ in range(2):
+        C = torch.zeros(128, 640, device="cuda")
+        run_gemm(A, B, C, 1.0, 0.0, 1)
+        outs.append(C.cpu())
+    assert torch.equal(outs[0], outs[1])
