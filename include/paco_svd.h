@@ -110,6 +110,27 @@ void paco_ctx_destroy(paco_ctx *ctx);
  * and returns the device status of the run. */
 int paco_svd_noalloc(int M, int N, float *A, float *U, float *Vt, float *sigma, void *stream);
 
+/* Largest M (and so N) of a matrix of the batched form. */
+#define PACO_BATCH_MAX_M 512
+
+/* Batched form (the reference runs one matrix per launch; this replaces a
+ * host loop over main.cpp:126-158 for many independent small matrices).
+ * Bytes of workspace paco_svd_batched needs for these shapes; 0 if a shape
+ * is invalid (N < 1, M < N) or M > PACO_BATCH_MAX_M. */
+size_t paco_batched_workspace_size(int count, const int *M, const int *N);
+
+/* SVD of `count` independent row-major FP32 matrices in one persistent
+ * launch: each CTA takes the next matrix (largest first) from a work queue
+ * and runs bidiagonalization, divide and conquer and the back-transforms for
+ * it.  M, N and the pointer arrays are host arrays; A[b] (M x N), U[b]
+ * (M x M), Vt[b] (N x N) and sigma[b] (N) are device buffers; A is read only.
+ * `status` (device, count ints, may be null) receives each matrix's
+ * PACO_* code.  Asynchronous on `stream`; the workspace and outputs must stay
+ * alive until the stream has finished the call. */
+int paco_svd_batched(int count, const int *M, const int *N, const float *const *A, float *const *U,
+                     float *const *Vt, float *const *sigma, int *status, void *workspace, size_t ws_bytes,
+                     void *stream);
+
 /* Library version string. */
 const char *paco_version(void);
 

@@ -9,12 +9,14 @@
 //          copies.  One CTA per image, transposed through shared memory so
 //          both the reads and the writes are coalesced.
 // tc_gemm  one CTA per 128x128 tile of C (and per k-range with split-K):
-//          thread 0 runs a 3-stage pipeline of bulk copies (mbarrier
+//          thread 0 runs a 2-stage pipeline of bulk copies (mbarrier
 //          complete_tx) and issues the MMAs (tcgen05.mma.cta_group::1
 //          .kind::tf32, M=128, N=128, K=8) into a TMEM accumulator; a
-//          tcgen05.commit per stage releases the stage.  The 4 warps then read
-//          the accumulator with tcgen05.ld, stage it through shared memory and
-//          write C = alpha*AB + beta*C with coalesced rows.
+//          tcgen05.commit per stage releases the stage.  The C tile is
+//          bulk-copied into shared memory while the products run (beta != 0);
+//          the 4 warps then read the accumulator with tcgen05.ld, combine it
+//          with C in shared memory and the tile leaves by bulk stores, one
+//          per row (plain coalesced stores when rows are not 16-byte aligned).
 // Every wait is bounded; a wait that gives up records PACO_ERR_TIMEOUT, the
 // copies still in flight are waited for (again bounded), the CTA frees its
 // tensor memory and returns.
@@ -28,7 +30,7 @@ namespace {
 
 constexpr int TM = 128, TN = 128, TK = 32;  // tile of C; k per image (128 bytes of TF32)
 constexpr int IMG = TM * TK;                // floats per tile image (16 KB)
-constexpr int STAGES = 3;
+constexpr int STAGES = 2;
 constexpr int MAX_SPLITS = 8;
 constexpr uint32_t IDESC = (1u << 4)             // D format F32
                            | (2u << 7)           // A format TF32
@@ -149,18 +151,33 @@ __global__ void __launch_bounds__(256) tc_pack(GemmOp X, int transposed, int R, 
 
 __global__ void __launch_bounds__(128, 1)
     tc_gemm(int M, int N, int KT, int kper, float alpha, const float *Ahi, const float *Alo, const float *Bhi,
-            const float *Blo, float beta, float *C, long ldc, float *part, DevStatus *st)
+            const float *Blo, float beta, float *C, long ldc, float *part, int ctma, DevStatus *st)
 {
     extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
-    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done;
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done, cbar;
     __shared__ uint32_t s_tmem;
     __shared__ int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nt = blockIdx.x, mt = blockIdx.y, z = blockIdx.z;
     const int kb0 = z * kper, kb1 = min(KT, kb0 + kper);
     const int nk = max(0, kb1 - kb0);
-    // stage buffers [stage][Ahi, Alo, Bhi, Blo][IMG], 1024-byte aligned for the swizzle
+    const int m0 = mt * TM, n0 = nt * TN;
+    const int nrows = min(TM, M - m0), ncols = min(TN, N - n0);
+    // stage buffers [stage][Ahi, Alo, Bhi, Blo][IMG], 1024-byte aligned for the
+    // swizzle, then the C tile (TM x TN, row-major) for the bulk-copy epilogue
     float *stage = (float *)(tc_smem_raw + ((1024u - (smem_u32(tc_smem_raw) & 1023u)) & 1023u));
+    float *Csm = stage + (long)STAGES * 4 * IMG;
+    // destination of this CTA: C, or its split-K partial buffer
+    float *Cd = C;
+    long ld = ldc;
+    float al = alpha, be = beta;
+    if (part) {
+        Cd = part + (long)z * M * N;
+        ld = N;
+        al = 1.f;
+        be = 0.f;
+    }
+    const bool cload = ctma && be != 0.f;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
@@ -174,6 +191,7 @@ __global__ void __launch_bounds__(128, 1)
             mbar_init(&empty[s], 1);
         }
         mbar_init(&done, 1);
+        mbar_init(&cbar, 1);
         mbar_init_fence();
         s_fail = 0;
     }
@@ -183,6 +201,12 @@ __global__ void __launch_bounds__(128, 1)
     const uint32_t tmem = s_tmem;
 
     if (tid == 0) {
+        // the C tile streams in while the products run
+        if (cload) {
+            mbar_expect_tx(&cbar, (uint32_t)(nrows * ncols * 4));
+            for (int r = 0; r < nrows; r++)
+                tma_load_1d(Csm + r * TN, Cd + (long)(m0 + r) * ld + n0, (uint32_t)(ncols * 4), &cbar);
+        }
         const long abase = (long)mt * KT * IMG, bbase = (long)nt * KT * IMG;
         auto produce = [&](int j) {  // k-block j of this split into stage j % STAGES
             float *dst = stage + (long)(j % STAGES) * 4 * IMG;
@@ -236,24 +260,17 @@ __global__ void __launch_bounds__(128, 1)
         mma_commit(&done);  // arrives when every MMA issued above has completed
     }
     __syncthreads();
-    const bool ok = mbar_wait_bounded(&done, 0, st, 502);
+    bool ok = mbar_wait_bounded(&done, 0, st, 502);
+    if (cload) ok = mbar_wait_bounded(&cbar, 0, st, 504) && ok;
     if (!ok) s_fail = 1;
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
     if (!s_fail) {
-        float *Cd = C;
-        long ld = ldc;
-        float al = alpha, be = beta;
-        if (part) {
-            Cd = part + (long)z * M * N;
-            ld = N;
-            al = 1.f;
-            be = 0.f;
-        }
         const bool empty_k = (nk == 0);  // the accumulator was never written: the product is 0
-        // warp w owns TMEM lanes 32w..32w+31 (rows of the tile); staged per 32x32
-        // block through shared memory so each store instruction writes one row
+        // warp w owns TMEM lanes 32w..32w+31 (rows of the tile); each 32x32
+        // block is transposed through shared memory so that the lanes then
+        // walk the columns of one row
         float(*sb)[33] = reinterpret_cast<float(*)[33]>(stage + warp * 32 * 33);
         const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
@@ -263,19 +280,40 @@ __global__ void __launch_bounds__(128, 1)
 #pragma unroll
             for (int q = 0; q < 32; q++) sb[lane][q] = __uint_as_float(v[q]);
             __syncwarp();
-            const int n = nt * TN + c0 + lane;
-            if (n < N) {
+            const int cl = c0 + lane;
+            if (cl < ncols) {
+                if (ctma) {
 #pragma unroll 4
-                for (int rr = 0; rr < 32; rr++) {
-                    const int m = mt * TM + warp * 32 + rr;
-                    if (m >= M) break;
-                    float *c = Cd + (long)m * ld + n;
-                    float x = empty_k ? 0.f : al * sb[rr][lane];
-                    if (be != 0.f) x = fmaf(be, *c, x);
-                    *c = x;
+                    for (int rr = 0; rr < 32; rr++) {
+                        const int rl = warp * 32 + rr;
+                        if (rl >= nrows) break;
+                        float x = empty_k ? 0.f : al * sb[rr][lane];
+                        if (cload) x = fmaf(be, Csm[rl * TN + cl], x);
+                        Csm[rl * TN + cl] = x;
+                    }
+                } else {
+#pragma unroll 4
+                    for (int rr = 0; rr < 32; rr++) {
+                        const int m = m0 + warp * 32 + rr;
+                        if (m >= M) break;
+                        float *c = Cd + (long)m * ld + n0 + cl;
+                        float x = empty_k ? 0.f : al * sb[rr][lane];
+                        if (be != 0.f) x = fmaf(be, *c, x);
+                        *c = x;
+                    }
                 }
             }
             __syncwarp();
+        }
+        if (ctma) {
+            proxy_async_fence();
+            __syncthreads();
+            // one bulk store per row of the tile, spread over warp 0's lanes
+            if (warp == 0) {
+                for (int r = lane; r < nrows; r += 32)
+                    tma_store_1d(Cd + (long)(m0 + r) * ld + n0, Csm + r * TN, (uint32_t)(ncols * 4));
+                tma_store_commit_and_drain();
+            }
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -286,7 +324,8 @@ __global__ void __launch_bounds__(128, 1)
 
 // ------------------------------------------------------------------ host
 
-static size_t tc_smem_bytes() { return (size_t)STAGES * 4 * IMG * sizeof(float) + 1024; }
+// stages, the C tile, and slack for the 1024-byte alignment
+static size_t tc_smem_bytes() { return (size_t)(STAGES * 4 * IMG + TM * TN) * sizeof(float) + 1024; }
 
 size_t gemm_tc_scratch_floats(int M, int N, int K)
 {
@@ -324,8 +363,12 @@ cudaError_t gemm_tc_run(int M, int N, int K, float alpha, GemmOp A, GemmOp B, fl
     const int kper = ceil_div(g.KT, g.splits);
     paco_count_launch(), tc_pack<<<g.MT * g.KT, 256, 0, s>>>(A, 0, M, K, g.KT, Ahi, Alo);
     paco_count_launch(), tc_pack<<<g.NT * g.KT, 256, 0, s>>>(B, 1, N, K, g.KT, Bhi, Blo);
+    // bulk-copy epilogue when every row segment of the destination is 16-byte aligned
+    const float *dst = part ? part : C;
+    const long dld = part ? (long)N : ldc;
+    const int ctma = ((((uintptr_t)dst) & 15) == 0 && (dld % 4) == 0 && (N % 4) == 0) ? 1 : 0;
     paco_count_launch(), tc_gemm<<<dim3(g.NT, g.MT, g.splits), 128, tc_smem_bytes(), s>>>(
-                             M, N, g.KT, kper, alpha, Ahi, Alo, Bhi, Blo, beta, C, ldc, part, st);
+                             M, N, g.KT, kper, alpha, Ahi, Alo, Bhi, Blo, beta, C, ldc, part, ctma, st);
     if (part) return gemm_splitk_reduce_run(M, N, g.splits, alpha, part, beta, C, ldc, s);
     return cudaGetLastError();
 }

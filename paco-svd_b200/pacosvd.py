@@ -75,6 +75,12 @@ def lib():
         L.paco_ctx_svd_host.argtypes = [vp, vp, vp, vp, vp]; L.paco_ctx_svd_host.restype = i
         L.paco_ctx_destroy.argtypes = [vp]; L.paco_ctx_destroy.restype = None
         L.paco_version.argtypes = []; L.paco_version.restype = ctypes.c_char_p
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.paco_batched_workspace_size.argtypes = [i, ip, ip]
+        L.paco_batched_workspace_size.restype = ctypes.c_size_t
+        L.paco_svd_batched.argtypes = [i, ip, ip, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                       ctypes.POINTER(vp), vp, vp, ctypes.c_size_t, vp]
+        L.paco_svd_batched.restype = i
         _lib = L
     return _lib
 
@@ -223,6 +229,75 @@ def svd(A, check=True):
         rc, info = sync_status(w.ws)
         _check(rc, f"paco_svd (device, info={info})")
     return s.clone(), U.clone(), Vt.clone()
+
+
+PACO_BATCH_MAX_M = 512
+
+
+def _int_array(vals):
+    return (ctypes.c_int * len(vals))(*[int(v) for v in vals])
+
+
+def batched_workspace_size(shapes) -> int:
+    """Workspace bytes of paco_svd_batched for a list of (M, N); 0 if invalid."""
+    Ms, Ns = _int_array([m for m, _ in shapes]), _int_array([n for _, n in shapes])
+    return int(lib().paco_batched_workspace_size(len(shapes), Ms, Ns))
+
+
+class Batch:
+    """Device buffers of the batched form for a fixed list of shapes
+    (M <= 512, N <= M); reusable across calls."""
+
+    def __init__(self, shapes, device="cuda"):
+        torch = _torch()
+        self.shapes = [(int(m), int(n)) for m, n in shapes]
+        self.count = len(self.shapes)
+        self.nbytes = batched_workspace_size(self.shapes)
+        if self.nbytes == 0:
+            bad = any(n >= 1 and m >= n and m > PACO_BATCH_MAX_M for m, n in self.shapes)
+            raise PacoError(PACO_ERR_UNSUPPORTED if bad else PACO_ERR_INVALID_ARG, "paco_batched_workspace_size")
+        self.ws = torch.empty(self.nbytes, dtype=torch.uint8, device=device)
+        self.A = [torch.empty(m, n, device=device) for m, n in self.shapes]
+        self.U = [torch.empty(m, m, device=device) for m, _ in self.shapes]
+        self.Vt = [torch.empty(n, n, device=device) for _, n in self.shapes]
+        self.sigma = [torch.empty(n, device=device) for _, n in self.shapes]
+        self.status = torch.zeros(self.count, dtype=torch.int32, device=device)
+        vpa = ctypes.c_void_p * self.count
+        self._Ms = _int_array([m for m, _ in self.shapes])
+        self._Ns = _int_array([n for _, n in self.shapes])
+        self._pA = vpa(*[t.data_ptr() for t in self.A])
+        self._pU = vpa(*[t.data_ptr() for t in self.U])
+        self._pV = vpa(*[t.data_ptr() for t in self.Vt])
+        self._ps = vpa(*[t.data_ptr() for t in self.sigma])
+
+    def load(self, As):
+        for dst, src in zip(self.A, As):
+            dst.copy_(src if hasattr(src, "data_ptr") else _torch().from_numpy(src), non_blocking=True)
+
+    def run(self, stream=None):
+        """Enqueues the batched SVD of the resident A on `stream`."""
+        rc = lib().paco_svd_batched(self.count, self._Ms, self._Ns, self._pA, self._pU, self._pV, self._ps,
+                                    _ptr(self.status), _ptr(self.ws), self.nbytes, _stream(stream))
+        _check(rc, "paco_svd_batched")
+
+    def statuses(self):
+        return self.status.cpu().tolist()
+
+
+def svd_batched(As, check=True):
+    """SVD of a list of float32 CUDA (or numpy) matrices, M <= 512, N <= M, in
+    one batched launch.  Returns lists (sigma, U, Vt) and the per-matrix status."""
+    torch = _torch()
+    As = [a if hasattr(a, "data_ptr") else torch.from_numpy(np.ascontiguousarray(a, np.float32)) for a in As]
+    b = Batch([tuple(a.shape) for a in As])
+    b.load(As)
+    b.run()
+    torch.cuda.synchronize()
+    st = b.statuses()
+    if check:
+        for k, c in enumerate(st):
+            _check(c, f"paco_svd_batched matrix {k}")
+    return [s.clone() for s in b.sigma], [u.clone() for u in b.U], [v.clone() for v in b.Vt], st
 
 
 class HostContext:

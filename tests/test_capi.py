@@ -106,3 +106,20 @@ def test_svd_main_reports_short_input(tmp_path):
 def test_noalloc_scratch_covers_its_largest_shape():
     # paco_svd_noalloc serves M <= 1024, N <= 512 from a 16 MiB device array
     assert P.lib().paco_svd_workspace_size(1024, 512) <= 16 << 20
+
+
+def test_batched_workspace_rejects_bad_shapes():
+    assert P.batched_workspace_size([(4, 8)]) == 0               # M < N
+    assert P.batched_workspace_size([(10, 0)]) == 0              # N = 0
+    assert P.batched_workspace_size([(513, 10)]) == 0            # M beyond the batched limit
+    assert P.batched_workspace_size([]) == 0
+
+
+def test_batched_entry_validates_before_touching_the_device():
+    import ctypes as C
+    L = P.lib()
+    Ms, Ns = (C.c_int * 1)(600), (C.c_int * 1)(10)
+    nul = (C.c_void_p * 1)(None)
+    assert L.paco_svd_batched(1, Ms, Ns, nul, nul, nul, nul, None, None, 0, None) == P.PACO_ERR_UNSUPPORTED
+    Ms[0] = 3
+    assert L.paco_svd_batched(1, Ms, Ns, nul, nul, nul, nul, None, None, 0, None) == P.PACO_ERR_INVALID_ARG
