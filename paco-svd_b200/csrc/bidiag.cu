@@ -473,28 +473,47 @@ __global__ void bd_panel_vectors(const float *W, long ldw, int p0, int nbp, int 
 // T (NBF x NBF, upper triangular) of the forward block reflector
 // H_0 ... H_{nbp-1} = I - Vp T Vp^T, from the Gram matrix G = Vp^T Vp:
 //   T[q][q] = tau_q,  T[0:q, q] = -tau_q T[0:q, 0:q] G[0:q, q]
-// (the recurrence of LAPACK's larft).  One CTA, columns in sequence.
+// (the recurrence of LAPACK's larft).  Row r of T only needs its own earlier
+// entries and G, so every row is computed independently: one warp per row
+// (8 rows per CTA), lane l holding T[r][l + 32 j], each new entry a warp dot
+// product against column q of G, read as row q (G is symmetric, and the
+// GEMM that forms it computes both halves with the same summation order).
+// The rows of G a CTA reads are staged in shared memory first.
 __global__ void __launch_bounds__(256) bd_build_t(const float *gram, int nbp, const float *tau, float *T)
 {
-    extern __shared__ float sm_t[];
-    float *Ts = sm_t;                    // NBF x (NBF + 1)
-    float *w = sm_t + NBF * (NBF + 1);   // NBF
-    const int tid = threadIdx.x;
-    for (int t = tid; t < NBF * (NBF + 1); t += blockDim.x) Ts[t] = 0.f;
+    extern __shared__ float sm_t[];  // rows r0 .. nbp-1 of G
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r0 = blockIdx.x * 8;
+    const int r = r0 + warp;
+    for (int t = threadIdx.x; t < (nbp - r0) * NBF; t += blockDim.x)
+        sm_t[t] = gram[(long)r0 * NBF + t];
     __syncthreads();
-    for (int q = 0; q < nbp; q++) {
-        const float tq = tau[q];
-        if (tid < q) w[tid] = gram[tid * NBF + q];
-        __syncthreads();
-        if (tid < q) {
-            float acc = 0.f;
-            for (int b = tid; b < q; b++) acc += Ts[tid * (NBF + 1) + b] * w[b];
-            Ts[tid * (NBF + 1) + q] = -tq * acc;
+    constexpr int J = NBF / 32;
+    float t[J];
+#pragma unroll
+    for (int j = 0; j < J; j++) t[j] = 0.f;
+    if (r < nbp) {
+        const float tr = tau[r];
+#pragma unroll
+        for (int j = 0; j < J; j++)
+            if (lane + 32 * j == r) t[j] = tr;
+        for (int q = r + 1; q < nbp; q++) {
+            const float *g = sm_t + (long)(q - r0) * NBF;
+            float p = 0.f;
+#pragma unroll
+            for (int j = 0; j < J; j++) {
+                const int bb = lane + 32 * j;
+                if (bb >= r && bb < q) p = fmaf(t[j], g[bb], p);
+            }
+            p = warp_sum(p);
+            const float v = -tau[q] * p;
+#pragma unroll
+            for (int j = 0; j < J; j++)
+                if (lane + 32 * j == q) t[j] = v;
         }
-        if (tid == 0) Ts[q * (NBF + 1) + q] = tq;
-        __syncthreads();
     }
-    for (int t = tid; t < NBF * NBF; t += blockDim.x) T[t] = Ts[(t / NBF) * (NBF + 1) + t % NBF];
+#pragma unroll
+    for (int j = 0; j < J; j++) T[(long)r * NBF + lane + 32 * j] = t[j];
 }
 
 // Q_sub <- (I - Vp T Vp^T) Q_sub for Q_sub = Q[off:off+Lp, off:off+Lp] (ld ldq)
@@ -506,7 +525,7 @@ static cudaError_t apply_block_reflector(const BdWs &w, float *Q, long ldq, long
     cudaError_t err = gemm_run(nbp, nbp, Lp, 1.f, gop(w.Vp, 1, NBF), gop(w.Vp, NBF, 1), 0.f, w.gram, NBF, splits,
                                w.gscr, s);
     if (err) return err;
-    paco_count_launch(), bd_build_t<<<1, 256, (NBF * (NBF + 1) + NBF) * sizeof(float), s>>>(w.gram, nbp, tau, w.T);
+    paco_count_launch(), bd_build_t<<<NBF / 8, 256, (size_t)NBF * NBF * sizeof(float), s>>>(w.gram, nbp, tau, w.T);
     float *Qs = Q + off * ldq + off;
     // G1 = Vp^T Q_sub  (nbp x Lp)
     err = gemm_any(nbp, Lp, Lp, 1.f, gop(w.Vp, 1, NBF), gop(Qs, ldq, 1), 0.f, w.G1, Lp, splits, w.gscr, w.tcs,
@@ -704,8 +723,7 @@ void bd_init_attrs()
     cudaFuncSetAttribute(bd_row_pass<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
     cudaFuncSetAttribute(bd_row_pass<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
     cudaFuncSetAttribute(bd_row_pass<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
-    cudaFuncSetAttribute(bd_build_t, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)((NBF * (NBF + 1) + NBF) * sizeof(float)));
+    cudaFuncSetAttribute(bd_build_t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(NBF * NBF * sizeof(float)));
     gemm_tc_init_attrs();
     rp_attrs_set = true;
 }

@@ -425,6 +425,13 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
                 s_xi[tid] = s_bc[1 + ii + tid];                             // X[i, q]
                 s_t1[tid] = s_bc[1 + tid] + s_red[1 + tid] * inv;           // V^T v
                 s_t2[tid] = s_bc[1 + ii + tid] + s_red[1 + ii + tid] * inv; // X^T v
+            } else if (tid < NB) {
+                // the column pass multiplies every panel slot: the unused ones
+                // must hold zeros, not what an earlier kernel left in shared memory
+                s_ai[tid] = 0.f;
+                s_xi[tid] = 0.f;
+                s_t1[tid] = 0.f;
+                s_t2[tid] = 0.f;
             }
             for (int t = tid; t < PR; t += RP_THREADS) s_cpart[t] = 0.f;
             __syncthreads();

@@ -52,6 +52,23 @@ static unsigned long long g_launches = 0;
 static int g_prof_on = 0;
 void paco_count_launch() { g_launches++; }
 
+__global__ void dev_status_begin(DevStatus *st, int stage)
+{
+    const int t = threadIdx.x;
+    const bool keep = (stage == 2) && st->stage1_mark == PACO_STAGE1_MARK;
+    __syncthreads();
+    if (t < 60) st->counters[t] = 0;
+    if (t == 0) {
+        if (!keep) {
+            st->code = 0;
+            st->info = 0;
+            st->secular_nonconv = 0;
+            st->wait_timeouts = 0;
+        }
+        st->stage1_mark = (stage == 1) ? PACO_STAGE1_MARK : 0;
+    }
+}
+
 extern "C" {
 
 unsigned long long paco_launch_count(void) { return g_launches; }
@@ -72,7 +89,7 @@ size_t paco_debug_trace_offset(int M, int N)
 // `ws` starts with the status block; the rest is GEMM scratch.  Synchronous.
 size_t paco_debug_gemm_ws_bytes(int M, int N, int K)
 {
-    return 256 + sizeof(float) * std::max(gemm_tc_scratch_floats(M, N, K), (size_t)8 * M * N);
+    return 512 + sizeof(float) * std::max(gemm_tc_scratch_floats(M, N, K), (size_t)8 * M * N);
 }
 
 int paco_debug_gemm(int M, int N, int K, float alpha, const float *A, long a_rs, long a_cs, const float *B, long b_rs,
@@ -82,7 +99,7 @@ int paco_debug_gemm(int M, int N, int K, float alpha, const float *A, long a_rs,
         return PACO_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     DevStatus *st = (DevStatus *)ws;
-    float *scr = (float *)((char *)ws + 256);
+    float *scr = (float *)((char *)ws + 512);
     bd_init_attrs();
     cudaMemsetAsync(st, 0, sizeof(DevStatus), s);
     cudaError_t err = mode == 1 ? gemm_tc_run(M, N, K, alpha, gop(A, a_rs, a_cs), gop(B, b_rs, b_cs), beta, C, ldc,
@@ -91,6 +108,22 @@ int paco_debug_gemm(int M, int N, int K, float alpha, const float *A, long a_rs,
                                            std::min(8, std::max(1, K / 512)), scr, s);
     if (err != cudaSuccess) return PACO_ERR_CUDA;
     return paco_sync_status(ws, stream, nullptr);
+}
+
+// Test hook (not part of the public header): byte offsets of the stage-1
+// workspace fields, in the order of BdWs (st, W, Yt, X, ypart, tpart, cpart,
+// rowbuf, inv_v0c, inv_v0r, sc, ctl, trace, bcA, bcB, Vp, T, gram, G1, G2,
+// gscr, Vtmp, tcs), then the total; returns the number of values written.
+int paco_debug_bd_layout(int M, int N, size_t out[24])
+{
+    BdWs w;
+    char *base = (char *)(uintptr_t)(1u << 20);
+    const size_t total = bd_carve(base, M, N, &w);
+    const void *f[23] = {w.st, w.W, w.Yt, w.X, w.ypart, w.tpart, w.cpart, w.rowbuf, w.inv_v0c, w.inv_v0r, w.sc,
+                         w.ctl, w.trace, w.bcA, w.bcB, w.Vp, w.T, w.gram, w.G1, w.G2, w.gscr, w.Vtmp, w.tcs};
+    for (int k = 0; k < 23; k++) out[k] = f[k] ? (size_t)((const char *)f[k] - base) : total;
+    out[23] = total;
+    return 24;
 }
 
 const char *paco_version(void) { return "paco-svd-b200 1.0 (sm_100a)"; }
@@ -155,8 +188,9 @@ int upper_bidiagonalization(int M, int N, float *a, float *u, float *vt, float *
     if (!shape_ok(M, N)) return (N >= 1 && M >= N) ? PACO_ERR_UNSUPPORTED : PACO_ERR_INVALID_ARG;
     if (!a || !u || !vt || !d || !tauq || !workspace || (N > 1 && (!e || !taup))) return PACO_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
-    // a new factorization starts: clear the device status block
-    if (cudaMemsetAsync(workspace, 0, sizeof(DevStatus), s) != cudaSuccess) return PACO_ERR_CUDA;
+    // a new factorization starts: clear and mark the device status block
+    paco_count_launch(), dev_status_begin<<<1, 64, 0, s>>>((DevStatus *)workspace, 1);
+    if (cudaGetLastError() != cudaSuccess) return PACO_ERR_CUDA;
     return bd_run(M, N, a, a, u, vt, d, e, tauq, taup, workspace, s, device_sms());
 }
 
@@ -166,9 +200,8 @@ int svd_DC(int M, int N, float *a, float *u, float *vt, float *d, float *e, floa
     if (!shape_ok(M, N)) return (N >= 1 && M >= N) ? PACO_ERR_UNSUPPORTED : PACO_ERR_INVALID_ARG;
     if (!a || !u || !vt || !d || !qt || !wt || !idx || !workspace || (N > 1 && !e)) return PACO_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
-    if (cudaMemsetAsync((char *)workspace + offsetof(DevStatus, counters), 0, sizeof(((DevStatus *)0)->counters),
-                        s) != cudaSuccess)
-        return PACO_ERR_CUDA;
+    paco_count_launch(), dev_status_begin<<<1, 64, 0, s>>>((DevStatus *)workspace, 2);
+    if (cudaGetLastError() != cudaSuccess) return PACO_ERR_CUDA;
     return bdc_run(M, N, a, u, vt, d, e, qt, wt, idx, workspace, tiling, s);
 }
 

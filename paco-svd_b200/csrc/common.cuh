@@ -19,7 +19,17 @@ struct DevStatus {
     int secular_nonconv; // secular roots that hit the iteration limit
     int wait_timeouts;   // bounded waits that gave up
     int counters[60];    // arrival tickets for last-block reductions
+    int stage1_mark;     // PACO_STAGE1_MARK while a stage-1 run's status awaits stage 2
 };
+
+#define PACO_STAGE1_MARK 0x31474B42  // "BKG1"
+
+// Opens a run on a workspace whose status block may hold anything.  Stage 1
+// (stage = 1) starts a new factorization: the block is cleared and marked.
+// Stage 2 (stage = 2) keeps the codes of a stage-1 run on the same workspace
+// (the two-kernel flow reads both through one paco_sync_status) and clears
+// them otherwise; either way the marker is consumed and the counters reset.
+__global__ void dev_status_begin(DevStatus *st, int stage);
 
 __device__ __forceinline__ void dev_fail(DevStatus *st, int code, int info)
 {
