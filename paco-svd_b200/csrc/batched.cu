@@ -1,24 +1,29 @@
-// Batched SVD of many small matrices (1 <= N <= M <= 512) in one persistent
-// launch.  Every CTA (256 threads) takes the next matrix from a work queue
-// (matrices sorted by cost, largest first) and runs the whole pipeline of
-// the single-matrix path for it:
-//   1. Golub-Kahan Householder bidiagonalization, unblocked, with the reflector
-//      convention of upper_bidiagonalization.cpp:182-218.  One fused sweep per
-//      column step: each warp owns whole rows (held in registers, lane l has
-//      columns l, l+32, ...), applies the left reflector H_i and the right
-//      reflector G_i to them, and in the same sweep accumulates the column
-//      norm and the products  S_j = sum_r x_r a_rj  that the next step's left
-//      reflector needs (w_j = a_ij + S_j / v0), so the trailing block is read
-//      and written once per step.
-//   2. Bidiagonal divide and conquer with the device bodies of bdc_dev.cuh
-//      (the same code the level kernels of the large path run), levels in
-//      sequence, merges of a level one after another, every phase spread over
-//      the CTA's threads or warps.
-//   3. U = H_0 ... H_{N-1} blockdiag(Q, I) and V = G_0 ... G_{N-2} W, applied
-//      backward to the divide-and-conquer vectors with one fused sweep per
-//      reflector (apply H_i, accumulate the w of H_{i-1}), which replaces the
-//      formation of U, V and the two final products of svd.cpp:1911-1981.
-// Per-matrix scratch lives in one slot per CTA, carved for the matrix at hand.
+// Batched SVD of many small matrices (1 <= N <= M <= 512): three persistent
+// launches, each with a work queue over the matrices (largest first), so the
+// whole batch takes three kernels whatever its size:
+//   1. bt_bidiag_k (512 threads per matrix)  Golub-Kahan Householder
+//      bidiagonalization, unblocked, with the reflector convention of
+//      upper_bidiagonalization.cpp:182-218.  One fused sweep per column step:
+//      each warp owns whole rows (held in registers, lane l has columns l,
+//      l+32, ... of the active chunks), applies the left reflector H_i and the
+//      right reflector G_i to them, and in the same sweep accumulates the
+//      column norm and the products S_j = sum_r x_r a_rj that the next step's
+//      left reflector needs (w_j = a_ij + S_j / v0), so the trailing block is
+//      read and written once per step.
+//   2. bt_bdc_k (256 threads per matrix, two CTAs per SM)  bidiagonal divide
+//      and conquer with the device bodies of bdc_dev.cuh (the code the level
+//      kernels of the large path run): levels in sequence, every phase spread
+//      over the CTA's threads or warps (a secular root per thread for small
+//      merges, per warp for large ones), back-transform products through
+//      64x64 shared-memory tiles.
+//   3. bt_apply_k (512 threads per matrix)  U = H_0 ... H_{N-1} blockdiag(Q, I)
+//      and V = G_0 ... G_{N-2} W applied backward to the divide-and-conquer
+//      vectors with one fused sweep per reflector (apply H_i, accumulate the w
+//      of H_{i-1}); this replaces the formation of U, V and the two final
+//      products of svd.cpp:1911-1981.
+// Each matrix keeps its Householder vectors, d/e/tau and Q^T/W^T in its own
+// area of the workspace between the launches; the divide-and-conquer and
+// back-transform scratch lives in one slot per CTA.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -27,29 +32,64 @@
 #include "bdc_dev.cuh"
 
 namespace bt {
-constexpr int THREADS = 256;
-constexpr int WARPS = THREADS / 32;
-constexpr int VPL = PACO_BATCH_MAX_M / 32;  // row values per lane
+constexpr int T_SWEEP = 512;            // threads of kernels 1 and 3
+constexpr int W_SWEEP = T_SWEEP / 32;
+constexpr int T_BDC = 256;              // threads of kernel 2 (the bdc bodies assume 256)
+constexpr int MAXC = PACO_BATCH_MAX_M;  // widest row
+constexpr int KSMALL = 32;              // merges up to this k solve a secular root per thread
 }  // namespace bt
 
 struct BtItem {
     int M, N, index, pad;
     const float *A;
     float *U, *Vt, *sigma;
+    size_t moff;  // byte offset of the matrix's area in the arena
 };
 
-struct BtSlot {
-    float *W;       // M x ldw  working copy of A, then the Householder vectors
+// per-matrix area, alive from kernel 1 to kernel 3
+struct BtMat {
+    float *W;  // M x ldw: Householder vectors, d on the diagonal, e on the superdiagonal
     long ldw;
     float *d, *e, *tauq, *taup;
-    float *qt, *wt; // 2 N^2 each: Q^T / st and W^T / gt of the divide and conquer
-    int *idx;       // 16 N
-    float *diff;    // N x N  d_j^2 - sigma_i^2 of the secular roots
-    float *X;       // N x N  V W before the transpose into Vt
-    BdcWs bw;
+    float *QT, *WT;  // N x N (ld N): Q^T and W^T of the divide and conquer
+    int *perm;       // N: descending order of the singular values
+    float *sig;      // N: sorted singular values
+    int *code;       // PACO_* status of the matrix
 };
 
-__host__ __device__ static size_t bt_carve(char *base, int M, int N, BtSlot *s)
+__host__ __device__ static size_t bt_mat_carve(char *base, int M, int N, BtMat *m)
+{
+    size_t off = 0;
+    auto take = [&](size_t bytes) -> char * {
+        off = (off + 255) & ~(size_t)255;
+        char *p = base ? base + off : nullptr;
+        off += bytes;
+        return p;
+    };
+    const size_t nn = (size_t)N * N;
+    m->ldw = (N + 3) & ~3;
+    m->W = (float *)take(sizeof(float) * (size_t)M * m->ldw);
+    m->d = (float *)take(sizeof(float) * N);
+    m->e = (float *)take(sizeof(float) * N);
+    m->tauq = (float *)take(sizeof(float) * N);
+    m->taup = (float *)take(sizeof(float) * N);
+    m->QT = (float *)take(sizeof(float) * nn);
+    m->WT = (float *)take(sizeof(float) * nn);
+    m->perm = (int *)take(sizeof(int) * N);
+    m->sig = (float *)take(sizeof(float) * N);
+    m->code = (int *)take(sizeof(int));
+    return (off + 255) & ~(size_t)255;
+}
+
+// divide-and-conquer scratch of one CTA of kernel 2
+struct BtBdcSlot {
+    float *ST, *GT;  // N x N gather targets
+    int *idx;        // 16 N: idxq, f, l, dsig, zhat, srow
+    float *diff;     // N x N: d_j^2 - sigma_i^2 of the secular roots
+    BdcWs bw;        // perm and sig are pointed at the matrix's area per matrix
+};
+
+__host__ __device__ static size_t bt_bdc_carve(char *base, int N, BtBdcSlot *s)
 {
     size_t off = 0;
     auto take = [&](size_t bytes) -> char * {
@@ -60,17 +100,10 @@ __host__ __device__ static size_t bt_carve(char *base, int M, int N, BtSlot *s)
     };
     const size_t nn = (size_t)N * N;
     const int nleaf = N / 3 + 2;
-    s->ldw = (N + 3) & ~3;
-    s->W = (float *)take(sizeof(float) * (size_t)M * s->ldw);
-    s->d = (float *)take(sizeof(float) * N);
-    s->e = (float *)take(sizeof(float) * N);
-    s->tauq = (float *)take(sizeof(float) * N);
-    s->taup = (float *)take(sizeof(float) * N);
-    s->qt = (float *)take(sizeof(float) * 2 * nn);
-    s->wt = (float *)take(sizeof(float) * 2 * nn);
+    s->ST = (float *)take(sizeof(float) * nn);
+    s->GT = (float *)take(sizeof(float) * nn);
     s->idx = (int *)take(sizeof(int) * 16 * (size_t)N);
     s->diff = (float *)take(sizeof(float) * nn);
-    s->X = (float *)take(sizeof(float) * nn);
     BdcWs &w = s->bw;
     w.st = (DevStatus *)take(sizeof(DevStatus));
     w.Us = (float *)take(sizeof(float) * nn);
@@ -83,8 +116,8 @@ __host__ __device__ static size_t bt_carve(char *base, int M, int N, BtSlot *s)
     w.mg_s = (int *)take(sizeof(int) * nleaf);
     w.mg_m = (int *)take(sizeof(int) * nleaf);
     w.mg_e = (int *)take(sizeof(int) * nleaf);
-    w.perm = (int *)take(sizeof(int) * N);
-    w.sig = (float *)take(sizeof(float) * N);
+    w.perm = nullptr;
+    w.sig = nullptr;
     w.tcs = nullptr;
     w.tcs_floats = 0;
     return (off + 255) & ~(size_t)255;
@@ -105,139 +138,180 @@ static __device__ __forceinline__ void bt_reflector(float x0, float sigma, int l
     *beta = mu;
 }
 
-struct BtShared {
-    float part[bt::WARPS][PACO_BATCH_MAX_M]; // per-warp partial column sums
-    float wv[PACO_BATCH_MAX_M];              // w of the current left reflector
-    float uv[PACO_BATCH_MAX_M];              // current right reflector (u_{i+1} = 1)
-    float rv[PACO_BATCH_MAX_M];              // pivot row after its left update
-    float ssig[bt::WARPS];
-    int lv_off[BDC_MAX_LEVELS], lv_nm[BDC_MAX_LEVELS];
-    int nlev, item, bad;
+// shared memory of the sweep kernels (1 and 3)
+struct BtSweepSh {
+    float part[bt::W_SWEEP][bt::MAXC];  // per-warp partial column sums
+    float wv[bt::MAXC];                 // w of the current left reflector
+    float uv[bt::MAXC];                 // current right reflector (u_{i+1} = 1)
+    float rv[bt::MAXC];                 // pivot row after its left update
+    float ssig[bt::W_SWEEP];
+    int item, bad;
 };
 
-// ---------------------------------------------------------------- stage 1
+// rows in flight per warp for NA active 32-column chunks (<= 48 row values
+// per lane in registers)
+template <int NA>
+struct BtRows {
+    static constexpr int RB = 48 / NA > 8 ? 8 : (48 / NA < 2 ? 2 : 48 / NA);
+};
 
-// a[q] for a run-time q without indexing the register array dynamically
-static __device__ __forceinline__ float bt_pick(const float (&a)[bt::VPL], int q)
+// the persistent work queue: the next matrix for this CTA, or -1
+static __device__ __forceinline__ int bt_next(unsigned *queue, int count, int *s_item)
 {
-    float x = 0.f;
-#pragma unroll
-    for (int j = 0; j < bt::VPL; j++)
-        if (j == q) x = a[j];
-    return x;
+    __syncthreads();
+    if (threadIdx.x == 0) *s_item = (int)atomicAdd(queue, 1u);
+    __syncthreads();
+    const int b = *s_item;
+    return b < count ? b : -1;
 }
 
-// Sweep of the rows r in [r0, M): optional left/right updates of columns
-// >= c0, then the accumulation for the next column reflector (column cn,
-// rows > cn):  ssig += a_r,cn^2,  part[c] += a_r,cn * a_rc  (c > cn).
-// mode 0: copy-in from A (NaN/Inf -> 0, flagged), no updates.
-template <int MODE>
-static __device__ void bt_sweep(BtShared &sh, const float *A, float *W, long ldw, int M, int N, int r0, int ci,
-                                float inv_v0, float tq, float tp, int *bad)
+// ---------------------------------------------------------------- kernel 1
+
+// Sweep of the rows r in [r0, M) over the column chunks q0 .. q0+NA-1 (lane l
+// holds column 32 (q0 + j) + l): the left update (H_ci) and the right update
+// (G_ci) of the columns > ci, then the accumulation for the next column
+// reflector (column cn = ci + 1, rows > cn):  ssig += a_r,cn^2,
+// part[c] += a_r,cn * a_rc  (c > cn).  MODE 0 copies the rows in from A
+// instead (NaN/Inf -> 0, flagged) and does no update.  Each warp has RB rows
+// in flight (rows base + rb * W_SWEEP + warp).  Column ci lies in chunk q0.
+template <int MODE, int NA>
+static __device__ void bt_sweep(BtSweepSh &sh, const float *A, float *W, long ldw, int M, int N, int r0, int ci,
+                                int q0, float inv_v0, float tq, float tp, int *bad)
 {
     using namespace bt;
+    constexpr int RBn = BtRows<NA>::RB;
+    constexpr int NW = W_SWEEP;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int cn = ci + 1;  // next column (MODE 0: ci = -1, cn = 0)
-    float acc[VPL];
+    const int c0 = 32 * q0 + lane;
+    const bool cn_hi = (cn >> 5) > q0;  // column cn in the second active chunk
+    float acc[NA];
 #pragma unroll
-    for (int q = 0; q < VPL; q++) acc[q] = 0.f;
+    for (int j = 0; j < NA; j++) acc[j] = 0.f;
     float ssig = 0.f;
-    for (int r = r0 + warp; r < M; r += WARPS) {
-        float a[VPL];
-        float *row = W + (long)r * ldw;
-        if (MODE == 0) {
-            const float *src = A + (long)r * N;
+    for (int base = r0; base < M; base += NW * RBn) {
+        float a[RBn][NA];
 #pragma unroll
-            for (int q = 0; q < VPL; q++) {
-                const int c = lane + 32 * q;
-                float x = (c < N) ? src[c] : 0.f;
-                if (!isfinite(x)) { x = 0.f; *bad = 1; }
-                a[q] = x;
-                if (c < N) row[c] = x;
-            }
-        } else {
+        for (int rb = 0; rb < RBn; rb++) {
+            const int r = base + rb * NW + warp;
+            const float *src = (MODE == 0) ? A + (long)r * N : W + (long)r * ldw;
 #pragma unroll
-            for (int q = 0; q < VPL; q++) {
-                const int c = lane + 32 * q;
-                a[q] = (c >= ci && c < N) ? row[c] : 0.f;
-            }
-            // Householder vector entry of column ci
-            const float x = __shfl_sync(0xffffffffu, bt_pick(a, ci >> 5), ci & 31);
-            const float vr = x * inv_v0;
-            if (lane == (ci & 31)) row[ci] = vr;
-            // left update (H_ci) then right update (G_ci) of columns > ci
-            const float lf = tq * vr;
-            float dot = 0.f;
-#pragma unroll
-            for (int q = 0; q < VPL; q++) {
-                const int c = lane + 32 * q;
-                if (c > ci && c < N) {
-                    a[q] -= lf * sh.wv[c];
-                    dot += a[q] * sh.uv[c];
-                }
-            }
-            dot = warp_sum(dot) * tp;
-#pragma unroll
-            for (int q = 0; q < VPL; q++) {
-                const int c = lane + 32 * q;
-                if (c > ci && c < N) {
-                    a[q] -= dot * sh.uv[c];
-                    row[c] = a[q];
-                }
+            for (int j = 0; j < NA; j++) {
+                const int c = c0 + 32 * j;
+                a[rb][j] = (r < M && c >= ci && c < N) ? src[c] : 0.f;
             }
         }
-        if (cn < N && r > cn) {
-            const float xn = __shfl_sync(0xffffffffu, bt_pick(a, cn >> 5), cn & 31);
-            ssig += xn * xn;
 #pragma unroll
-            for (int q = 0; q < VPL; q++) {
-                const int c = lane + 32 * q;
-                if (c > cn) acc[q] += xn * a[q];
+        for (int rb = 0; rb < RBn; rb++) {
+            const int r = base + rb * NW + warp;
+            if (r >= M) break;
+            float *row = W + (long)r * ldw;
+            if (MODE == 0) {
+#pragma unroll
+                for (int j = 0; j < NA; j++) {
+                    const int c = c0 + 32 * j;
+                    if (!isfinite(a[rb][j])) { a[rb][j] = 0.f; *bad = 1; }
+                    if (c < N) row[c] = a[rb][j];
+                }
+            } else {
+                // Householder vector entry of column ci (chunk q0)
+                const float x = __shfl_sync(0xffffffffu, a[rb][0], ci & 31);
+                const float vr = x * inv_v0;
+                if (lane == (ci & 31)) row[ci] = vr;
+                const float lf = tq * vr;
+                float dot = 0.f;
+#pragma unroll
+                for (int j = 0; j < NA; j++) {
+                    const int c = c0 + 32 * j;
+                    if (c > ci && c < N) {
+                        a[rb][j] -= lf * sh.wv[c];
+                        dot += a[rb][j] * sh.uv[c];
+                    }
+                }
+                dot = warp_sum(dot) * tp;
+#pragma unroll
+                for (int j = 0; j < NA; j++) {
+                    const int c = c0 + 32 * j;
+                    if (c > ci && c < N) {
+                        a[rb][j] -= dot * sh.uv[c];
+                        row[c] = a[rb][j];
+                    }
+                }
+            }
+            if (cn < N && r > cn) {
+                float xs = a[rb][0];
+                if (NA > 1 && cn_hi) xs = a[rb][NA > 1 ? 1 : 0];
+                const float xn = __shfl_sync(0xffffffffu, xs, cn & 31);
+                ssig += xn * xn;
+#pragma unroll
+                for (int j = 0; j < NA; j++) {
+                    const int c = c0 + 32 * j;
+                    if (c > cn) acc[j] += xn * a[rb][j];
+                }
             }
         }
     }
 #pragma unroll
-    for (int q = 0; q < VPL; q++) {
-        const int c = lane + 32 * q;
-        if (c < N) sh.part[warp][c] = acc[q];
+    for (int j = 0; j < NA; j++) {
+        const int c = c0 + 32 * j;
+        if (c < N) sh.part[warp][c] = acc[j];
     }
     if (lane == 0) sh.ssig[warp] = ssig;
 }
 
+// bt_sweep over the chunks q0 .. (N-1)/32
+template <int MODE>
+static __device__ void bt_sweep_any(BtSweepSh &sh, const float *A, float *W, long ldw, int M, int N, int r0,
+                                    int ci, float inv_v0, float tq, float tp, int *bad)
+{
+    const int q0 = ci < 0 ? 0 : ci >> 5;
+    const int na = ((N - 1) >> 5) - q0 + 1;
+#define BT_SWEEP_CASE(K) \
+    case K: bt_sweep<MODE, K>(sh, A, W, ldw, M, N, r0, ci, q0, inv_v0, tq, tp, bad); break;
+    switch (na) {
+        BT_SWEEP_CASE(1) BT_SWEEP_CASE(2) BT_SWEEP_CASE(3) BT_SWEEP_CASE(4)
+        BT_SWEEP_CASE(5) BT_SWEEP_CASE(6) BT_SWEEP_CASE(7) BT_SWEEP_CASE(8)
+        BT_SWEEP_CASE(9) BT_SWEEP_CASE(10) BT_SWEEP_CASE(11) BT_SWEEP_CASE(12)
+        BT_SWEEP_CASE(13) BT_SWEEP_CASE(14) BT_SWEEP_CASE(15) BT_SWEEP_CASE(16)
+        default: break;
+    }
+#undef BT_SWEEP_CASE
+}
+
 // Stage 1 for one matrix: d, e, tauq, taup and the Householder vectors in W.
-static __device__ void bt_bidiag(BtShared &sh, const float *A, const BtSlot &s, int M, int N)
+static __device__ void bt_bidiag(BtSweepSh &sh, const float *A, const BtMat &m, int M, int N)
 {
     using namespace bt;
+    constexpr int NT = T_SWEEP, NW = W_SWEEP;
     const int tid = threadIdx.x;
-    float *W = s.W;
-    const long ldw = s.ldw;
-    bt_sweep<0>(sh, A, W, ldw, M, N, 0, -1, 0.f, 0.f, 0.f, &sh.bad);
+    float *W = m.W;
+    const long ldw = m.ldw;
+    bt_sweep_any<0>(sh, A, W, ldw, M, N, 0, -1, 0.f, 0.f, 0.f, &sh.bad);
     __syncthreads();
     for (int i = 0; i < N; i++) {
         // column reflector i from the sums of the previous sweep (every
         // thread computes the same scalars, in the same order)
         float sig = 0.f;
 #pragma unroll
-        for (int w = 0; w < WARPS; w++) sig += sh.ssig[w];
+        for (int w = 0; w < NW; w++) sig += sh.ssig[w];
         const float x0 = W[(long)i * ldw + i];
         float beta, tq, v0;
         bt_reflector(x0, sig, M - i, &beta, &tq, &v0);
         const float inv_v0 = 1.f / v0;
         // w_j = a_ij + S_j / v0 and the left update of the pivot row
-        for (int c = tid; c < N; c += THREADS) {
-            if (c > i) {
-                float S = 0.f;
+        for (int c = i + 1 + tid; c < N; c += NT) {
+            float S = 0.f;
 #pragma unroll
-                for (int w = 0; w < WARPS; w++) S += sh.part[w][c];
-                const float wj = W[(long)i * ldw + c] + inv_v0 * S;
-                sh.wv[c] = wj;
-                sh.rv[c] = W[(long)i * ldw + c] - tq * wj;
-            }
+            for (int w = 0; w < NW; w++) S += sh.part[w][c];
+            const float aic = W[(long)i * ldw + c];
+            const float wj = aic + inv_v0 * S;
+            sh.wv[c] = wj;
+            sh.rv[c] = aic - tq * wj;
         }
         __syncthreads();
         if (tid == 0) {  // after every thread has read x0
-            s.d[i] = beta;
-            s.tauq[i] = tq;
+            m.d[i] = beta;
+            m.tauq[i] = tq;
             W[(long)i * ldw + i] = beta;
         }
         // row reflector i on the pivot row's columns > i (every warp sums the
@@ -250,125 +324,263 @@ static __device__ void bt_bidiag(BtShared &sh, const float *A, const BtSlot &s, 
             float eb, v0r;
             bt_reflector(sh.rv[i + 1], rs, N - i - 1, &eb, &tp, &v0r);
             const float inv_r = 1.f / v0r;
-            for (int c = tid; c < N; c += THREADS) {
-                if (c == i + 1) {
-                    sh.uv[c] = 1.f;
-                    W[(long)i * ldw + c] = eb;
-                } else if (c > i + 1) {
-                    const float u = sh.rv[c] * inv_r;
-                    sh.uv[c] = u;
-                    W[(long)i * ldw + c] = u;
-                }
+            for (int c = i + 1 + tid; c < N; c += NT) {
+                const float u = (c == i + 1) ? 1.f : sh.rv[c] * inv_r;
+                sh.uv[c] = u;
+                W[(long)i * ldw + c] = (c == i + 1) ? eb : u;
             }
             if (tid == 0) {
-                s.e[i] = eb;
-                s.taup[i] = tp;
+                m.e[i] = eb;
+                m.taup[i] = tp;
             }
         }
         __syncthreads();
-        bt_sweep<1>(sh, nullptr, W, ldw, M, N, i + 1, i, inv_v0, tq, tp, nullptr);
+        bt_sweep_any<1>(sh, nullptr, W, ldw, M, N, i + 1, i, inv_v0, tq, tp, nullptr);
         __syncthreads();
     }
 }
 
-// ---------------------------------------------------------------- stage 2
+// prof[0]: SM cycles of kernel 1 per matrix, summed
+__global__ void __launch_bounds__(bt::T_SWEEP, 1) bt_bidiag_k(const BtItem *items, int count, unsigned *queue,
+                                                              char *arena, unsigned long long *prof)
+{
+    __shared__ BtSweepSh sh;
+    for (;;) {
+        const int b = bt_next(queue, count, &sh.item);
+        if (b < 0) break;
+        const BtItem it = items[b];
+        BtMat m;
+        bt_mat_carve(arena + it.moff, it.M, it.N, &m);
+        if (threadIdx.x == 0) sh.bad = 0;
+        __syncthreads();
+        const long long t0 = clock64();
+        bt_bidiag(sh, it.A, m, it.M, it.N);
+        if (threadIdx.x == 0) {
+            *m.code = sh.bad ? PACO_ERR_NONFINITE : 0;
+            atomicAdd(&prof[0], (unsigned long long)(clock64() - t0));
+        }
+    }
+}
 
-static __device__ void bt_bdc(BtShared &sh, const BtSlot &s, int N, unsigned char *dyn)
+// ---------------------------------------------------------------- kernel 2
+
+// C (M x Nc) = X (M x K) Y (K x Nc), all row-major with the given leading
+// dimensions: 64 x 64 output tiles, 16-deep k slices staged in shared memory,
+// a 4 x 4 block of outputs per thread.  All 256 threads of the CTA call it.
+static __device__ void bt_gemm64(int M, int Nc, int K, const float *X, long ldx, const float *Y, long ldy, float *C,
+                                 long ldc)
+{
+    __shared__ __align__(16) float Xs[16][68];
+    __shared__ __align__(16) float Ys[16][68];
+    const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+    for (int m0 = 0; m0 < M; m0 += 64)
+        for (int n0 = 0; n0 < Nc; n0 += 64) {
+            float acc[4][4];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
+            for (int k0 = 0; k0 < K; k0 += 16) {
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const int e = tid + 256 * q;
+                    const int r = e >> 4, kk = e & 15;
+                    const int gm = m0 + r, gk = k0 + kk;
+                    Xs[kk][r] = (gm < M && gk < K) ? X[(long)gm * ldx + gk] : 0.f;
+                    const int kr = e >> 6, c = e & 63;
+                    const int gk2 = k0 + kr, gn = n0 + c;
+                    Ys[kr][c] = (gk2 < K && gn < Nc) ? Y[(long)gk2 * ldy + gn] : 0.f;
+                }
+                __syncthreads();
+#pragma unroll
+                for (int kk = 0; kk < 16; kk++) {
+                    const float4 a = *reinterpret_cast<const float4 *>(&Xs[kk][ty * 4]);
+                    const float4 b = *reinterpret_cast<const float4 *>(&Ys[kk][tx * 4]);
+                    const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+                    for (int i = 0; i < 4; i++)
+#pragma unroll
+                        for (int j = 0; j < 4; j++) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+                }
+                __syncthreads();
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int gm = m0 + ty * 4 + i;
+                if (gm >= M) continue;
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int gn = n0 + tx * 4 + j;
+                    if (gn < Nc) C[(long)gm * ldc + gn] = acc[i][j];
+                }
+            }
+        }
+}
+
+// qt/wt rows [0, k) of a merge = Us / Vs times st / gt
+static __device__ void bt_btgemm(const LevelArgs &A, int mg)
+{
+    const int s = A.w.mg_s[A.off + mg];
+    const MergeMeta mm = A.w.meta[s];
+    const int N = A.N;
+    const long off = (long)s * N + s;
+    bt_gemm64(mm.k, mm.n, mm.k, A.w.Us + off, N, A.ST + off, N, A.QT + off, N);
+    bt_gemm64(mm.k, mm.nc, mm.k, A.w.Vs + off, N, A.GT + off, N, A.WT + off, N);
+}
+
+// Stage 2 for one matrix.  prof[6..11]: cycles of set-up and leaves,
+// prepare, rotate + gather, secular roots, Loewner z + vectors + copy-back,
+// back-transform products + finalize (thread 0's clock).
+static __device__ void bt_bdc(const BtMat &m, const BtBdcSlot &sl, int N, unsigned char *dyn, int *lv_off,
+                              int *lv_nm, int *s_nlev, unsigned long long *prof)
 {
     using namespace bt;
+    constexpr int NT = T_BDC, NW = T_BDC / 32;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    long long tc = clock64();
+    auto lap = [&](int k) {
+        if (tid == 0) {
+            const long long t = clock64();
+            atomicAdd(&prof[k], (unsigned long long)(t - tc));
+            tc = t;
+        }
+    };
     LevelArgs A;
-    A.N = N; A.off = 0; A.d_e = s.e; A.d = s.d;
-    A.QT = s.qt; A.ST = s.qt + (size_t)N * N; A.WT = s.wt; A.GT = s.wt + (size_t)N * N;
-    int *ib = s.idx;
+    A.N = N; A.off = 0; A.d_e = m.e; A.d = m.d;
+    A.QT = m.QT; A.ST = sl.ST; A.WT = m.WT; A.GT = sl.GT;
+    int *ib = sl.idx;
     A.idxq = ib; A.f = (float *)(ib + N); A.l = (float *)(ib + 2 * N); A.dsig = (float *)(ib + 3 * N);
     A.zhat = (float *)(ib + 4 * N); A.srow = ib + 5 * N;
-    A.diff = s.diff;
-    A.w = s.bw;
-    if (tid == 0) sh.nlev = bdc_schedule_dev(N, nullptr, s.bw, sh.lv_off, sh.lv_nm);
-    for (long t = tid; t < (long)N * N; t += THREADS) {
+    A.diff = sl.diff;
+    A.w = sl.bw;
+    A.w.perm = m.perm;
+    A.w.sig = m.sig;
+    if (tid == 0) *s_nlev = bdc_schedule_dev(N, nullptr, A.w, lv_off, lv_nm);
+    for (long t = tid; t < (long)N * N; t += NT) {
         const float v = (t / N == t % N) ? 1.f : 0.f;
-        s.qt[t] = v;
-        s.wt[t] = v;
+        m.QT[t] = v;
+        m.WT[t] = v;
     }
     __syncthreads();
     const int nleaf = leaf_partition(N, nullptr, nullptr);
-    for (int t = tid; t < nleaf; t += THREADS)
-        bdc_leaf_dev(t, N, s.bw, s.d, s.e, A.QT, A.WT, A.idxq, A.f, A.l);
+    for (int t = tid; t < nleaf; t += NT) bdc_leaf_dev(t, N, A.w, m.d, m.e, A.QT, A.WT, A.idxq, A.f, A.l);
     __syncthreads();
-    const int nlev = min(sh.nlev, BDC_MAX_LEVELS);
+    const int nlev = min(*s_nlev, BDC_MAX_LEVELS);
+    lap(6);
     for (int lv = 0; lv < nlev; lv++) {
-        A.off = sh.lv_off[lv];
-        const int nm = sh.lv_nm[lv];
+        A.off = lv_off[lv];
+        const int nm = lv_nm[lv];
         for (int mg = 0; mg < nm; mg++) bdc_prepare_dev(A, mg, dyn);
+        lap(7);
         for (int mg = 0; mg < nm; mg++)
-            for (int c = tid; c < N; c += THREADS) bdc_rotate_dev(A, mg, c);
-        __syncthreads();
-        for (int mg = 0; mg < nm; mg++)
-            for (int c = tid; c < N; c += THREADS) bdc_gather_dev(A, mg, c, 0, N);
-        __syncthreads();
-        for (int g = warp; g < N; g += WARPS) bdc_secular_dev(A, nm, g, lane);
-        __syncthreads();
-        for (int g = warp; g < N; g += WARPS) bdc_lowner_dev(A, nm, g, lane);
-        __syncthreads();
-        for (int g = warp; g < N; g += WARPS) bdc_vectors_dev(A, nm, g, lane);
-        __syncthreads();
-        for (int mg = 0; mg < nm; mg++)
-            for (int c = tid; c < N; c += THREADS) bdc_copyback_dev(A, mg, c, 0, N);
+            for (int c = tid; c < N; c += NT) bdc_rotate_dev(A, mg, c);
         __syncthreads();
         for (int mg = 0; mg < nm; mg++) {
-            const MergeMeta mm = A.w.meta[A.w.mg_s[A.off + mg]];
-            for (int which = 0; which < 2; which++) {
-                const int ncols = which ? mm.nc : mm.n;
-                for (int tm = 0; tm * 128 < mm.k; tm++)
-                    for (int tn = 0; tn * 128 < ncols; tn++) bdc_btgemm_dev(A, mg, which, tm, tn);
-            }
+            const int nc = A.w.meta[A.w.mg_s[A.off + mg]].nc;
+            for (int x = tid; x < nc * nc; x += NT) bdc_gather_dev(A, mg, x % nc, x / nc, x / nc + 1);
         }
         __syncthreads();
+        lap(8);
+        // roots of small merges one per thread, of large merges one per warp
+        for (int g = tid; g < N; g += NT) bdc_secular_dev<1>(A, nm, g, 0, 0, KSMALL);
+        for (int g = warp; g < N; g += NW) bdc_secular_dev<32>(A, nm, g, lane, KSMALL, 0x7fffffff);
+        __syncthreads();
+        lap(9);
+        for (int g = tid; g < N; g += NT) bdc_lowner_dev<1>(A, nm, g, 0, 0, KSMALL);
+        for (int g = warp; g < N; g += NW) bdc_lowner_dev<32>(A, nm, g, lane, KSMALL, 0x7fffffff);
+        __syncthreads();
+        for (int g = tid; g < N; g += NT) bdc_vectors_dev<1>(A, nm, g, 0, 0, KSMALL);
+        for (int g = warp; g < N; g += NW) bdc_vectors_dev<32>(A, nm, g, lane, KSMALL, 0x7fffffff);
+        __syncthreads();
+        for (int mg = 0; mg < nm; mg++) {
+            const int nc = A.w.meta[A.w.mg_s[A.off + mg]].nc;
+            for (int x = tid; x < nc * nc; x += NT) bdc_copyback_dev(A, mg, x % nc, x / nc, x / nc + 1);
+        }
+        __syncthreads();
+        lap(10);
+        for (int mg = 0; mg < nm; mg++) bt_btgemm(A, mg);
+        __syncthreads();
         for (int mg = 0; mg < nm; mg++) bdc_finalize_dev(A, mg);
+        lap(11);
     }
-    for (int base = 0; base < N; base += THREADS) bdc_rank_desc_dev(N, s.d, s.bw.perm, s.bw.sig, base);
+    for (int base = 0; base < N; base += NT) bdc_rank_desc_dev(N, m.d, m.perm, m.sig, base);
     __syncthreads();
 }
 
-// ---------------------------------------------------------------- stage 3
+// prof[1]: SM cycles of kernel 2 per matrix, summed
+__global__ void __launch_bounds__(bt::T_BDC, 2) bt_bdc_k(const BtItem *items, int count, unsigned *queue,
+                                                         char *arena, char *slots, size_t slot_bytes,
+                                                         unsigned long long *prof)
+{
+    extern __shared__ __align__(16) unsigned char bt_dyn[];  // bdc_prepare scratch
+    __shared__ int s_item, s_nlev;
+    __shared__ int lv_off[BDC_MAX_LEVELS], lv_nm[BDC_MAX_LEVELS];
+    char *slot = slots + (size_t)blockIdx.x * slot_bytes;
+    for (;;) {
+        const int b = bt_next(queue, count, &s_item);
+        if (b < 0) break;
+        const BtItem it = items[b];
+        BtMat m;
+        bt_mat_carve(arena + it.moff, it.M, it.N, &m);
+        BtBdcSlot sl;
+        bt_bdc_carve(slot, it.N, &sl);
+        if (threadIdx.x == 0) {
+            sl.bw.st->code = 0;
+            sl.bw.st->secular_nonconv = 0;
+        }
+        __syncthreads();
+        const long long t0 = clock64();
+        bt_bdc(m, sl, it.N, bt_dyn, lv_off, lv_nm, &s_nlev, prof);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int code = *m.code;
+            if (!code) code = sl.bw.st->code;
+            if (!code && sl.bw.st->secular_nonconv) code = PACO_ERR_NONCONVERGENCE;
+            *m.code = code;
+            atomicAdd(&prof[1], (unsigned long long)(clock64() - t0));
+        }
+    }
+}
+
+// ---------------------------------------------------------------- kernel 3
 
 // Backward application of reflectors k = k1, k1-1, ..., 0 to the rows of Y
-// (R rows, C <= 512 columns, ld ldy): reflector k acts on rows >= k + sh_off
+// (R rows, C <= 32 NA columns, ld ldy): reflector k acts on rows >= k + sh_off
 // with v_{k+sh_off} = 1 and v_r = vec(k, r) for r > k + sh_off.  Each sweep
 // applies reflector k and accumulates the w of reflector k-1.
-template <typename Vec>
-static __device__ void bt_apply_back(BtShared &sh, float *Y, long ldy, int R, int C, int k1, int sh_off,
-                                     const float *tau, Vec vec)
+template <int NA, typename Vec>
+static __device__ void bt_apply_back_n(BtSweepSh &sh, float *Y, long ldy, int R, int C, int k1, int sh_off,
+                                       const float *tau, Vec vec)
 {
     using namespace bt;
+    constexpr int RBn = BtRows<NA>::RB;
+    constexpr int NT = T_SWEEP, NW = W_SWEEP;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (k1 < 0) return;
     // w of reflector k1
     {
         const int p = k1 + sh_off;
-        float acc[VPL];
+        float acc[NA];
 #pragma unroll
-        for (int q = 0; q < VPL; q++) acc[q] = 0.f;
-        for (int r = p + warp; r < R; r += WARPS) {
+        for (int j = 0; j < NA; j++) acc[j] = 0.f;
+        for (int r = p + warp; r < R; r += NW) {
             const float vr = (r == p) ? 1.f : vec(k1, r);
             const float *row = Y + (long)r * ldy;
 #pragma unroll
-            for (int q = 0; q < VPL; q++) {
-                const int c = lane + 32 * q;
-                if (c < C) acc[q] += vr * row[c];
+            for (int j = 0; j < NA; j++) {
+                const int c = lane + 32 * j;
+                if (c < C) acc[j] += vr * row[c];
             }
         }
 #pragma unroll
-        for (int q = 0; q < VPL; q++) {
-            const int c = lane + 32 * q;
-            if (c < C) sh.part[warp][c] = acc[q];
+        for (int j = 0; j < NA; j++) {
+            const int c = lane + 32 * j;
+            if (c < C) sh.part[warp][c] = acc[j];
         }
         __syncthreads();
-        for (int c = tid; c < C; c += THREADS) {
+        for (int c = tid; c < C; c += NT) {
             float w = 0.f;
 #pragma unroll
-            for (int x = 0; x < WARPS; x++) w += sh.part[x][c];
+            for (int x = 0; x < NW; x++) w += sh.part[x][c];
             sh.wv[c] = w;
         }
         __syncthreads();
@@ -377,41 +589,74 @@ static __device__ void bt_apply_back(BtShared &sh, float *Y, long ldy, int R, in
         const int p = k + sh_off;
         const float tk = tau[k];
         const bool nxt = k > 0;
-        float acc[VPL];
+        float acc[NA];
 #pragma unroll
-        for (int q = 0; q < VPL; q++) acc[q] = 0.f;
-        for (int r = p + warp; r < R; r += WARPS) {
-            const float vr = (r == p) ? 1.f : vec(k, r);
-            const float vn = nxt ? vec(k - 1, r) : 0.f;  // r > p - 1: entry of reflector k-1
-            const float f = tk * vr;
-            float *row = Y + (long)r * ldy;
+        for (int j = 0; j < NA; j++) acc[j] = 0.f;
+        for (int base = p; base < R; base += NW * RBn) {
+            float y[RBn][NA];
 #pragma unroll
-            for (int q = 0; q < VPL; q++) {
-                const int c = lane + 32 * q;
-                if (c < C) {
-                    const float y = row[c] - f * sh.wv[c];
-                    row[c] = y;
-                    acc[q] += vn * y;
+            for (int rb = 0; rb < RBn; rb++) {
+                const int r = base + rb * NW + warp;
+                const float *row = Y + (long)r * ldy;
+#pragma unroll
+                for (int j = 0; j < NA; j++) {
+                    const int c = lane + 32 * j;
+                    y[rb][j] = (r < R && c < C) ? row[c] : 0.f;
+                }
+            }
+#pragma unroll
+            for (int rb = 0; rb < RBn; rb++) {
+                const int r = base + rb * NW + warp;
+                if (r >= R) break;
+                const float vr = (r == p) ? 1.f : vec(k, r);
+                const float vn = nxt ? vec(k - 1, r) : 0.f;  // r > p - 1: entry of reflector k-1
+                const float f = tk * vr;
+                float *row = Y + (long)r * ldy;
+#pragma unroll
+                for (int j = 0; j < NA; j++) {
+                    const int c = lane + 32 * j;
+                    if (c < C) {
+                        const float v = y[rb][j] - f * sh.wv[c];
+                        row[c] = v;
+                        acc[j] += vn * v;
+                    }
                 }
             }
         }
         if (!nxt) break;
 #pragma unroll
-        for (int q = 0; q < VPL; q++) {
-            const int c = lane + 32 * q;
-            if (c < C) sh.part[warp][c] = acc[q];
+        for (int j = 0; j < NA; j++) {
+            const int c = lane + 32 * j;
+            if (c < C) sh.part[warp][c] = acc[j];
         }
         __syncthreads();
         // row p - 1 is untouched by reflector k: w' = Y[p-1] + sum of the partials
-        for (int c = tid; c < C; c += THREADS) {
+        for (int c = tid; c < C; c += NT) {
             float w = Y[(long)(p - 1) * ldy + c];
 #pragma unroll
-            for (int x = 0; x < WARPS; x++) w += sh.part[x][c];
+            for (int x = 0; x < NW; x++) w += sh.part[x][c];
             sh.wv[c] = w;
         }
         __syncthreads();
     }
     __syncthreads();
+}
+
+template <typename Vec>
+static __device__ void bt_apply_back(BtSweepSh &sh, float *Y, long ldy, int R, int C, int k1, int sh_off,
+                                     const float *tau, Vec vec)
+{
+    if (k1 < 0) return;
+#define BT_APPLY_CASE(K) \
+    case K: bt_apply_back_n<K>(sh, Y, ldy, R, C, k1, sh_off, tau, vec); break;
+    switch ((C + 31) >> 5) {
+        BT_APPLY_CASE(1) BT_APPLY_CASE(2) BT_APPLY_CASE(3) BT_APPLY_CASE(4)
+        BT_APPLY_CASE(5) BT_APPLY_CASE(6) BT_APPLY_CASE(7) BT_APPLY_CASE(8)
+        BT_APPLY_CASE(9) BT_APPLY_CASE(10) BT_APPLY_CASE(11) BT_APPLY_CASE(12)
+        BT_APPLY_CASE(13) BT_APPLY_CASE(14) BT_APPLY_CASE(15) BT_APPLY_CASE(16)
+        default: break;
+    }
+#undef BT_APPLY_CASE
 }
 
 // entry r of column reflector k (below the diagonal of W) / row reflector k
@@ -427,63 +672,57 @@ struct BtRowVec {
     __device__ float operator()(int k, int r) const { return W[(long)k * ldw + r]; }
 };
 
-// ---------------------------------------------------------------- kernel
-
-__global__ void __launch_bounds__(bt::THREADS) bt_svd(const BtItem *items, int count, unsigned *queue,
-                                                      int *status, char *slots, size_t slot_bytes)
+// prof[2..5]: SM cycles of the U/X set-up, the U sweeps, the V sweeps and
+// the outputs; matrices finished
+__global__ void __launch_bounds__(bt::T_SWEEP, 1) bt_apply_k(const BtItem *items, int count, unsigned *queue,
+                                                             char *arena, float *xslots, size_t xslot_floats,
+                                                             int *status, unsigned long long *prof)
 {
     using namespace bt;
-    extern __shared__ __align__(16) unsigned char bt_dyn[];  // bdc_prepare scratch
-    __shared__ BtShared sh;
+    constexpr int NT = T_SWEEP;
+    __shared__ BtSweepSh sh;
     const int tid = threadIdx.x;
-    char *slot = slots + (size_t)blockIdx.x * slot_bytes;
+    float *X = xslots + (size_t)blockIdx.x * xslot_floats;
     for (;;) {
-        if (tid == 0) sh.item = (int)atomicAdd(queue, 1u);
-        __syncthreads();
-        const int b = sh.item;
-        if (b >= count) break;
+        const int b = bt_next(queue, count, &sh.item);
+        if (b < 0) break;
         const BtItem it = items[b];
         const int M = it.M, N = it.N;
-        BtSlot s;
-        bt_carve(slot, M, N, &s);
-        if (tid == 0) {
-            sh.bad = 0;
-            s.bw.st->code = 0;
-            s.bw.st->secular_nonconv = 0;
-        }
-        __syncthreads();
-        bt_bidiag(sh, it.A, s, M, N);
-        bt_bdc(sh, s, N, bt_dyn);
+        BtMat m;
+        bt_mat_carve(arena + it.moff, M, N, &m);
+        const long long t0 = clock64();
         // U = H blockdiag(Q, I): Q(:, r) = qt row perm[r]
-        const int *perm = s.bw.perm;
-        for (long t = tid; t < (long)M * M; t += THREADS) {
+        for (long t = tid; t < (long)M * M; t += NT) {
             const int row = (int)(t / M), col = (int)(t % M);
             float v;
-            if (col < N) v = (row < N) ? s.qt[(long)perm[col] * N + row] : 0.f;
+            if (col < N) v = (row < N) ? m.QT[(long)m.perm[col] * N + row] : 0.f;
             else v = (row == col) ? 1.f : 0.f;
             it.U[t] = v;
         }
         // X = W: W(:, r) = wt row perm[r]
-        for (long t = tid; t < (long)N * N; t += THREADS) {
+        for (long t = tid; t < (long)N * N; t += NT) {
             const int row = (int)(t / N), col = (int)(t % N);
-            s.X[t] = s.wt[(long)perm[col] * N + row];
+            X[t] = m.WT[(long)m.perm[col] * N + row];
         }
         __syncthreads();
-        bt_apply_back(sh, it.U, M, M, M, N - 1, 0, s.tauq, BtColVec{s.W, s.ldw});
-        bt_apply_back(sh, s.X, N, N, N, N - 2, 1, s.taup, BtRowVec{s.W, s.ldw});
-        for (long t = tid; t < (long)N * N; t += THREADS) {
+        const long long t1 = clock64();
+        bt_apply_back(sh, it.U, M, M, M, N - 1, 0, m.tauq, BtColVec{m.W, m.ldw});
+        const long long t2 = clock64();
+        bt_apply_back(sh, X, N, N, N, N - 2, 1, m.taup, BtRowVec{m.W, m.ldw});
+        for (long t = tid; t < (long)N * N; t += NT) {
             const int r = (int)(t / N), j = (int)(t % N);
-            it.Vt[t] = s.X[(long)j * N + r];
+            it.Vt[t] = X[(long)j * N + r];
         }
-        for (int t = tid; t < N; t += THREADS) it.sigma[t] = s.bw.sig[t];
+        for (int t = tid; t < N; t += NT) it.sigma[t] = m.sig[t];
         __syncthreads();
-        if (tid == 0 && status) {
-            int code = s.bw.st->code;
-            if (!code && sh.bad) code = PACO_ERR_NONFINITE;
-            if (!code && s.bw.st->secular_nonconv) code = PACO_ERR_NONCONVERGENCE;
-            status[it.index] = code;
+        if (tid == 0) {
+            const long long t3 = clock64();
+            atomicAdd(&prof[2], (unsigned long long)(t1 - t0));
+            atomicAdd(&prof[3], (unsigned long long)(t2 - t1));
+            atomicAdd(&prof[4], (unsigned long long)(t3 - t2));
+            atomicAdd(&prof[5], 1ull);
+            if (status) status[it.index] = *m.code;
         }
-        __syncthreads();
     }
 }
 
@@ -492,23 +731,19 @@ __global__ void __launch_bounds__(bt::THREADS) bt_svd(const BtItem *items, int c
 static size_t bt_dyn_smem(int maxN) { return (size_t)20 * std::max(1, maxN) + 64; }
 
 struct BtPlan {
-    int Mx, Nx, slots;
-    size_t slot_bytes, items_off, slots_off, total;
+    int Mx, Nx, slots1, slots2, slots3;
+    size_t items_off, arena_off, arena_bytes, bdc_off, bdc_slot, x_off, x_slot, total;
+    std::vector<size_t> moff;
 };
 
-static int bt_blocks_per_sm(size_t dyn)
+static int bt_occupancy(const void *fn, int threads, size_t dyn)
 {
-    static int cached = -1;
-    static size_t cached_dyn = 0;
-    if (cached < 0 || cached_dyn != dyn) {
-        cudaFuncSetAttribute(bt_svd, cudaFuncAttributeMaxDynamicSharedMemorySize, 48 * 1024);
-        int n = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bt_svd, bt::THREADS, dyn) != cudaSuccess || n < 1)
-            n = 1;
-        cached = n;
-        cached_dyn = dyn;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, dyn) != cudaSuccess || n < 1) {
+        cudaGetLastError();
+        n = 1;
     }
-    return cached;
+    return n;
 }
 
 static bool bt_plan(int count, const int *M, const int *N, BtPlan *p)
@@ -521,17 +756,53 @@ static bool bt_plan(int count, const int *M, const int *N, BtPlan *p)
         Nx = std::max(Nx, N[b]);
     }
     int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    BtSlot s;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        sms = 148;
+    }
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(bt_bdc_k, cudaFuncAttributeMaxDynamicSharedMemorySize, 48 * 1024);
+        cudaGetLastError();
+        attr = true;
+    }
     p->Mx = Mx;
     p->Nx = Nx;
-    p->slot_bytes = bt_carve(nullptr, Mx, Nx, &s);
-    p->slots = std::min(count, sms * bt_blocks_per_sm(bt_dyn_smem(Nx)));
     p->items_off = 256;
-    p->slots_off = (p->items_off + sizeof(BtItem) * (size_t)count + 255) & ~(size_t)255;
-    p->total = p->slots_off + p->slot_bytes * p->slots;
+    p->arena_off = (p->items_off + sizeof(BtItem) * (size_t)count + 255) & ~(size_t)255;
+    p->moff.resize(count);
+    size_t a = 0;
+    for (int b = 0; b < count; b++) {
+        BtMat m;
+        p->moff[b] = a;
+        a += bt_mat_carve(nullptr, M[b], N[b], &m);
+    }
+    p->arena_bytes = a;
+    BtBdcSlot sl;
+    p->bdc_slot = bt_bdc_carve(nullptr, Nx, &sl);
+    p->x_slot = (size_t)Nx * Nx;
+    p->slots1 = std::min(count, sms * bt_occupancy((const void *)bt_bidiag_k, bt::T_SWEEP, 0));
+    p->slots2 = std::min(count, sms * bt_occupancy((const void *)bt_bdc_k, bt::T_BDC, bt_dyn_smem(Nx)));
+    p->slots3 = std::min(count, sms * bt_occupancy((const void *)bt_apply_k, bt::T_SWEEP, 0));
+    p->bdc_off = p->arena_off + a;
+    p->x_off = p->bdc_off + p->bdc_slot * p->slots2;
+    p->total = p->x_off + ((sizeof(float) * p->x_slot * p->slots3 + 255) & ~(size_t)255);
     return true;
+}
+
+// Test hook (not in the public header): the cycle counters of the last batched
+// call on this workspace (synchronizes the device).  out[0] stage 1, out[1]
+// stage 2, out[2..4] set-up, U sweeps, V sweeps + outputs, out[5] matrices,
+// out[6..11] the stage-2 phases.
+extern "C" int paco_debug_batched_phases(const void *workspace, double out[12])
+{
+    unsigned long long v[12];
+    if (!workspace || cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpy(v, (const char *)workspace + 64, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return PACO_ERR_CUDA;
+    for (int k = 0; k < 12; k++) out[k] = (double)v[k];
+    return PACO_OK;
 }
 
 size_t paco_batched_workspace_size(int count, const int *M, const int *N)
@@ -560,6 +831,7 @@ int paco_svd_batched(int count, const int *M, const int *N, const float *const *
         BtItem &it = items[b];
         it.M = M[b]; it.N = N[b]; it.index = b; it.pad = 0;
         it.A = A[b]; it.U = U[b]; it.Vt = Vt[b]; it.sigma = sigma[b];
+        it.moff = p.moff[b];
     }
     std::stable_sort(items.begin(), items.end(), [](const BtItem &x, const BtItem &y) {
         const double cx = (double)x.M * x.M * x.N + (double)x.M * x.N * x.N;
@@ -567,13 +839,18 @@ int paco_svd_batched(int count, const int *M, const int *N, const float *const *
         return cx > cy;
     });
     char *ws = (char *)workspace;
-    const size_t dyn = bt_dyn_smem(p.Nx);
+    unsigned *queues = (unsigned *)ws;  // one counter per kernel
+    unsigned long long *prof = (unsigned long long *)(ws + 64);
+    const BtItem *dit = (const BtItem *)(ws + p.items_off);
     if (cudaMemsetAsync(ws, 0, 256, s) != cudaSuccess) return PACO_ERR_CUDA;
     if (cudaMemcpyAsync(ws + p.items_off, items.data(), sizeof(BtItem) * count, cudaMemcpyHostToDevice, s) !=
         cudaSuccess)
         return PACO_ERR_CUDA;
-    paco_count_launch();
-    bt_svd<<<p.slots, bt::THREADS, dyn, s>>>((const BtItem *)(ws + p.items_off), count, (unsigned *)ws, status,
-                                             ws + p.slots_off, p.slot_bytes);
+    char *arena = ws + p.arena_off;
+    paco_count_launch(), bt_bidiag_k<<<p.slots1, bt::T_SWEEP, 0, s>>>(dit, count, queues + 0, arena, prof);
+    paco_count_launch(), bt_bdc_k<<<p.slots2, bt::T_BDC, bt_dyn_smem(p.Nx), s>>>(
+                             dit, count, queues + 1, arena, ws + p.bdc_off, p.bdc_slot, prof);
+    paco_count_launch(), bt_apply_k<<<p.slots3, bt::T_SWEEP, 0, s>>>(
+                             dit, count, queues + 2, arena, (float *)(ws + p.x_off), p.x_slot, status, prof);
     return cudaGetLastError() == cudaSuccess ? PACO_OK : PACO_ERR_CUDA;
 }

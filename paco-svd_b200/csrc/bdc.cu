@@ -98,17 +98,17 @@ __global__ void bdc_copyback(LevelArgs A)
 
 __global__ void __launch_bounds__(256) bdc_secular(LevelArgs A, int nm)
 {
-    bdc_secular_dev(A, nm, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, threadIdx.x & 31);
+    bdc_secular_dev<32>(A, nm, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, threadIdx.x & 31, 0, 0x7fffffff);
 }
 
 __global__ void __launch_bounds__(256) bdc_lowner(LevelArgs A, int nm)
 {
-    bdc_lowner_dev(A, nm, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, threadIdx.x & 31);
+    bdc_lowner_dev<32>(A, nm, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, threadIdx.x & 31, 0, 0x7fffffff);
 }
 
 __global__ void __launch_bounds__(256) bdc_vectors(LevelArgs A, int nm)
 {
-    bdc_vectors_dev(A, nm, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, threadIdx.x & 31);
+    bdc_vectors_dev<32>(A, nm, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, threadIdx.x & 31, 0, 0x7fffffff);
 }
 
 __global__ void __launch_bounds__(256) bdc_btgemm(LevelArgs A, int tiles_n)

@@ -389,11 +389,21 @@ static __device__ __forceinline__ int bdc_merge_of(const LevelArgs &A, int nm, i
     return mg;
 }
 
+// Sum over a group of G lanes (G = 32: the warp, G = 1: one thread).
+template <int G, typename T>
+static __device__ __forceinline__ T gsum(T v)
+{
+    if (G == 32) return warp_sum(v);
+    return v;
+}
+
 // FP64 root i of 1 + sum_j z_j^2 / ((d_j - s)(d_j + s)) = 0 for the column gw
-// of the level, one warp.  sigma = o + tau with o the nearer pole, so
+// of the level, one group of G lanes (a warp, or one thread for small merges);
+// only merges with klo < k <= khi are handled.  sigma = o + tau with o the nearer pole, so
 // d_j - sigma = (d_j - o) - tau keeps its relative accuracy (d_j, o are FP32
 // values: d_j - o is exact).
-static __device__ void bdc_secular_dev(const LevelArgs &A, int nm, int gw, int lane)
+template <int G>
+static __device__ void bdc_secular_dev(const LevelArgs &A, int nm, int gw, int lane, int klo, int khi)
 {
     const int N = A.N;
     if (gw >= N) return;
@@ -402,7 +412,7 @@ static __device__ void bdc_secular_dev(const LevelArgs &A, int nm, int gw, int l
     const int s = A.w.mg_s[A.off + mg];
     const MergeMeta mm = A.w.meta[s];
     const int i = gw - s, k = mm.k;
-    if (i >= k || i >= mm.n) return;
+    if (i >= k || i >= mm.n || k <= klo || k > khi) return;
     const float *ds = A.dsig + s;
     const double *z = A.w.zsec + s;
     float *drow = A.diff + (long)(s + i) * N + s;
@@ -414,17 +424,17 @@ static __device__ void bdc_secular_dev(const LevelArgs &A, int nm, int gw, int l
     if (i < k - 1) {
         double dlo = ds[i], dhi = ds[i + 1], h = dhi - dlo, mid = dlo + 0.5 * h;
         double fm = 0.0;
-        for (int j = lane; j < k; j += 32) {
+        for (int j = lane; j < k; j += G) {
             double dj = ds[j];
             fm += z[j] * z[j] / ((dj - mid) * (dj + mid));
         }
-        fm = 1.0 + warp_sum(fm);
+        fm = 1.0 + gsum<G>(fm);
         if (fm > 0) { o = dlo; tlo = 0.0; thi = 0.5 * h; }
         else { o = dhi; tlo = -0.5 * h; thi = 0.0; }
     } else {
         double zn2 = 0.0;
-        for (int j = lane; j < k; j += 32) zn2 += z[j] * z[j];
-        zn2 = warp_sum(zn2);
+        for (int j = lane; j < k; j += G) zn2 += z[j] * z[j];
+        zn2 = gsum<G>(zn2);
         o = ds[k - 1];
         tlo = 0.0;
         thi = zn2 / (sqrt(o * o + zn2) + o);
@@ -434,14 +444,14 @@ static __device__ void bdc_secular_dev(const LevelArgs &A, int nm, int gw, int l
     bool conv = false;
     for (int it = 0; it < BDC_SEC_MAXIT; it++) {
         double p1 = 0, p2 = 0, q1 = 0, q2 = 0;
-        for (int j = lane; j < k; j += 32) {
+        for (int j = lane; j < k; j += G) {
             double dj = ds[j];
             double D = ((dj - o) - tau) * (dj + o + tau);
             double r = 1.0 / D;
             double t = z[j] * z[j] * r;
             if (j <= i) { p1 += t; q1 += t * r; } else { p2 += t; q2 += t * r; }
         }
-        p1 = warp_sum(p1); p2 = warp_sum(p2); q1 = warp_sum(q1); q2 = warp_sum(q2);
+        p1 = gsum<G>(p1); p2 = gsum<G>(p2); q1 = gsum<G>(q1); q2 = gsum<G>(q2);
         const double Di = ((di - o) - tau) * (di + o + tau);
         const double Dn = ((dn - o) - tau) * (dn + o + tau);
         const double fv = 1.0 + p1 + p2;
@@ -478,18 +488,19 @@ static __device__ void bdc_secular_dev(const LevelArgs &A, int nm, int gw, int l
         tau = tn;
     }
     if (!conv && lane == 0) atomicAdd(&A.w.st->secular_nonconv, 1);
-    for (int j = lane; j < k; j += 32) {
+    for (int j = lane; j < k; j += G) {
         double dj = ds[j];
         drow[j] = (float)(((dj - o) - tau) * (dj + o + tau));
     }
     if (lane == 0) A.d[s + i] = (float)(o + tau);
 }
 
-// Loewner (Gu-Eisenstat) z of the pole at column g, one warp: each lane
-// multiplies the FP64 ratios of its share of j, then a butterfly product
-// combines the lanes (the same product in every lane, so the result is
-// reproducible) (svd.cpp:1422-1438)
-static __device__ void bdc_lowner_dev(const LevelArgs &A, int nm, int g, int lane)
+// Loewner (Gu-Eisenstat) z of the pole at column g, one group of G lanes:
+// each lane multiplies the FP64 ratios of its share of j, then a butterfly
+// product combines the lanes (the same product in every lane, so the result
+// is reproducible) (svd.cpp:1422-1438); only merges with klo < k <= khi.
+template <int G>
+static __device__ void bdc_lowner_dev(const LevelArgs &A, int nm, int g, int lane, int klo, int khi)
 {
     const int N = A.N;
     if (g >= N) return;
@@ -498,24 +509,27 @@ static __device__ void bdc_lowner_dev(const LevelArgs &A, int nm, int g, int lan
     const int s = A.w.mg_s[A.off + mg];
     const MergeMeta mm = A.w.meta[s];
     const int i = g - s, k = mm.k;
-    if (i >= k || k < 2) return;
+    if (i >= k || k < 2 || k <= klo || k > khi) return;
     const float *ds = A.dsig + s;
     const float *D = A.diff + (long)s * N + s; // D[j*N + i] = d_i^2 - sigma_j^2
     const double dii = ds[i];
     double p = 1.0;
-    for (int j = lane; j < k - 1; j += 32) {
+    for (int j = lane; j < k - 1; j += G) {
         double dj = (j < i) ? (double)ds[j] : (double)ds[j + 1];
         p *= (double)D[(long)j * N + i] / ((dii - dj) * (dii + dj));
     }
+    if (G == 32) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) p *= __shfl_xor_sync(0xffffffffu, p, o);
+        for (int o = 16; o > 0; o >>= 1) p *= __shfl_xor_sync(0xffffffffu, p, o);
+    }
     p *= (double)D[(long)(k - 1) * N + i];
     if (lane == 0) A.zhat[s + i] = (float)copysign(sqrt(fabs(p)), A.w.zsec[s + i]);
 }
 
-// normalized singular vectors of the secular problem for column gw, one warp
-// (svd.cpp:1440-1496)
-static __device__ void bdc_vectors_dev(const LevelArgs &A, int nm, int gw, int lane)
+// normalized singular vectors of the secular problem for column gw, one group
+// of G lanes (svd.cpp:1440-1496); only merges with klo < k <= khi.
+template <int G>
+static __device__ void bdc_vectors_dev(const LevelArgs &A, int nm, int gw, int lane, int klo, int khi)
 {
     const int N = A.N;
     if (gw >= N) return;
@@ -524,7 +538,7 @@ static __device__ void bdc_vectors_dev(const LevelArgs &A, int nm, int gw, int l
     const int s = A.w.mg_s[A.off + mg];
     const MergeMeta mm = A.w.meta[s];
     const int i = gw - s, k = mm.k;
-    if (i >= k || i >= mm.n) return;
+    if (i >= k || i >= mm.n || k <= klo || k > khi) return;
     float *us = A.w.Us + (long)(s + i) * N + s, *vs = A.w.Vs + (long)(s + i) * N + s;
     if (k == 1) {
         if (lane == 0) { us[0] = (float)sgn1(A.w.zsec[s]); vs[0] = 1.f; }
@@ -533,14 +547,14 @@ static __device__ void bdc_vectors_dev(const LevelArgs &A, int nm, int gw, int l
     const float *ds = A.dsig + s, *zh = A.zhat + s;
     const float *Drow = A.diff + (long)(s + i) * N + s;
     double nv = 0.0, nu = 0.0;
-    for (int j = lane; j < k; j += 32) {
+    for (int j = lane; j < k; j += G) {
         double v = (double)zh[j] / (double)Drow[j];
         double u = (j == 0) ? -1.0 : (double)ds[j] * v;
         nv += v * v; nu += u * u;
     }
-    nv = 1.0 / sqrt(warp_sum(nv));
-    nu = 1.0 / sqrt(warp_sum(nu));
-    for (int j = lane; j < k; j += 32) {
+    nv = 1.0 / sqrt(gsum<G>(nv));
+    nu = 1.0 / sqrt(gsum<G>(nu));
+    for (int j = lane; j < k; j += G) {
         double v = (double)zh[j] / (double)Drow[j];
         double u = (j == 0) ? -1.0 : (double)ds[j] * v;
         vs[j] = (float)(v * nv);
