@@ -40,17 +40,23 @@ WORKLOADS = {
     "cfg2b": dict(M=4096, N=4096, gen="graded"),
     "cfg1": dict(M=64, N=32, gen="uniform"),
     "cfg3": dict(M=8192, N=4096, gen="clustered"),
+    # batched form: 10,000 matrices, M uniform on [32, 512], N uniform on [16, M], iid N(0,1)
+    "cfg4": dict(kind="batched", count=10000, Mlo=32, Mhi=512, Nlo=16, gen="normal"),
 }
 CPU_SAMPLE_N = 768  # oracle sample size (about 5 s of single-thread work)
 
 
-def make_matrix(wl, seed=1234):
+def make_matrix(wl, seed=1234, with_sigma=False):
+    """The workload's seeded matrix; with_sigma also returns its exact
+    singular values (descending) for the generators that construct them."""
     M, N, gen = wl["M"], wl["N"], wl["gen"]
     rng = np.random.default_rng(seed)
     if gen == "uniform":
-        return rng.uniform(-1, 1, (M, N)).astype(np.float32)
+        A = rng.uniform(-1, 1, (M, N)).astype(np.float32)
+        return (A, None) if with_sigma else A
     if gen == "normal":
-        return rng.standard_normal((M, N), dtype=np.float32)
+        A = rng.standard_normal((M, N), dtype=np.float32)
+        return (A, None) if with_sigma else A
 
     def haar(n, m):
         Q, R = np.linalg.qr(rng.standard_normal((n, m)))
@@ -61,7 +67,8 @@ def make_matrix(wl, seed=1234):
     else:  # 512 clusters of 8, centres log-uniform in [1e-4, 1], spacing 1e-7
         centres = 10.0 ** rng.uniform(-4, 0, N // 8)
         sig = np.sort((centres[:, None] * (1 + 1e-7 * np.arange(8))[None, :]).ravel())[::-1]
-    return ((haar(M, N) * sig[None, :]) @ haar(N, N).T).astype(np.float32)
+    A = ((haar(M, N) * sig[None, :]) @ haar(N, N).T).astype(np.float32)
+    return (A, np.sort(sig)[::-1].copy()) if with_sigma else A
 
 
 class ClockSampler:
@@ -150,6 +157,30 @@ def whole_job_value(world, steps, total_ms):
     return world * steps / (total_ms / 1000.0)
 
 
+def batched_shapes(wl, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(wl["count"]):
+        M = int(rng.integers(wl["Mlo"], wl["Mhi"] + 1))
+        out.append((M, int(rng.integers(wl["Nlo"], M + 1))))
+    return out
+
+
+def cpu_baseline_batched(wl, nsample=30):
+    """Oracle port (FP64 C restatement, 1 thread) on `nsample` matrices drawn
+    from the batch's size distribution: SVDs/s of that sample."""
+    import oracle
+    rng = np.random.default_rng(77)
+    shapes = batched_shapes(dict(wl, count=nsample), 99)
+    t = time.perf_counter()
+    for M, N in shapes:
+        oracle.svd(rng.standard_normal((M, N)).astype(np.float32))
+    t = time.perf_counter() - t
+    return {"value": nsample / t, "unit": "SVDs/s", "cores": 1, "kind": "port",
+            "sample": f"oracle.svd on {nsample} N(0,1) matrices drawn from the batch's size distribution "
+                      f"({t:.1f} s)"}
+
+
 def cpu_baseline(wl, steps=1):
     """Oracle port (FP64 C restatement, 1 thread) on a CPU_SAMPLE_N^2 sample,
     scaled to the workload's SVDs/s by the n^3 work ratio."""
@@ -171,14 +202,15 @@ def cpu_baseline(wl, steps=1):
 def run_reference(args, wl, rank):
     if rank != 0:
         return
-    for _ in range(args.warmup if args.warmup < 1 else 1):
-        pass
-    cb = cpu_baseline(wl, steps=args.steps)
+    batched = wl.get("kind") == "batched"
+    cb = cpu_baseline_batched(wl) if batched else cpu_baseline(wl, steps=args.steps)
     line = {"metric": "SVDs/sec", "value": cb["value"], "unit": "SVDs/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 / cb["value"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{args.workload}: {wl['M']}x{wl['N']} FP32 {wl['gen']}, plain single-matrix SVD"},
+            "config": {"workload": (f"{args.workload}: {wl['count']} FP32 N(0,1) matrices, M in [{wl['Mlo']}, "
+                                    f"{wl['Mhi']}], N in [{wl['Nlo']}, M], batched SVD") if batched else
+                                   f"{args.workload}: {wl['M']}x{wl['N']} FP32 {wl['gen']}, plain single-matrix SVD"},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "SVDs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -213,8 +245,11 @@ def main():
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if wl.get("kind") == "batched":
+        run_batched(args, wl, rank, world, local, dist)
+        return
     M, N = wl["M"], wl["N"]
-    A_host = make_matrix(wl, seed=1234 + rank)
+    A_host, sig_exact = make_matrix(wl, seed=1234 + rank, with_sigma=True)
     A0 = torch.from_numpy(A_host).cuda()
     W = P.Workspace(M, N)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
@@ -267,8 +302,24 @@ def main():
     if rc:
         raise SystemExit(f"device status {rc} ({info}) in the timed region")
 
-    # correctness of the last step, against LAPACK where affordable
+    # accuracy of the last step (FP64 on the device; Frobenius norms): sigma
+    # against the exact spectrum the generator built (graded, clustered), the
+    # reconstruction residual and the orthogonality of U and V
     s = W.sigma.float().cpu().numpy().astype(np.float64)
+    acc = None
+    if rank == 0:
+        Ad = A0.double()
+        Ud, Vd, sd = W.U.double(), W.Vt.double(), W.sigma.double()
+        nA = torch.linalg.norm(Ad).item()
+        res = torch.linalg.norm(Ad - (Ud[:, :N] * sd[None, :]) @ Vd).item() / nA
+        eye_m = torch.eye(M, dtype=torch.float64, device="cuda")
+        eye_n = torch.eye(N, dtype=torch.float64, device="cuda")
+        acc = {"residual": res, "orth_U": torch.linalg.norm(Ud.T @ Ud - eye_m).item(),
+               "orth_V": torch.linalg.norm(Vd @ Vd.T - eye_n).item(), "tolerance": 1e-5 * N,
+               "sigma_err": (float(np.max(np.abs(s - sig_exact)) / sig_exact[0]) if sig_exact is not None
+                             else None),
+               "sigma_reference": "exact spectrum of the generator" if sig_exact is not None else None}
+        del Ad, Ud, Vd, eye_m, eye_n
 
     # end to end through the host-buffer C ABI (H2D of A, D2H of U, Vt, sigma)
     e2e_t = None
@@ -320,7 +371,7 @@ def main():
                                    f"(bidiagonalization + U/Vt formation + divide and conquer)",
                        "M": M, "N": N, "l2": "512 MiB buffer written between timed steps",
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
-            "sigma_max": float(s[0]), "sigma_min": float(s[-1]),
+            "sigma_max": float(s[0]), "sigma_min": float(s[-1]), "accuracy": acc,
             "roofline": roof, "clocks": clk,
             "e2e": ({"value": 1000.0 / e2e_t * world, "unit": "SVDs/s",
                      "h2d_bytes_per_step": 4 * M * N, "d2h_bytes_per_step": 4 * (M * M + N * N + N)}
@@ -328,6 +379,131 @@ def main():
             "gpu_launches": int(launches)}
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(wl)
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_batched(args, wl, rank, world, local, dist):
+    """cfg4: one step = one paco_svd_batched call over the whole batch."""
+    import torch
+    import pacosvd as P
+
+    lib = P.lib()
+    lib.paco_launch_count.restype = ctypes.c_ulonglong
+    lib.paco_debug_batched_timing.argtypes = [ctypes.c_int]
+    lib.paco_debug_batched_times.argtypes = [ctypes.POINTER(ctypes.c_float)]
+    shapes = batched_shapes(wl, 4321 + rank)
+    count = len(shapes)
+    b = P.Batch(shapes)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(1234 + rank)
+    b.A_flat.normal_(generator=gen)  # A is read only: every step sees the same inputs
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream()
+    for _ in range(max(3, args.warmup)):
+        b.run(stream)
+    stream.synchronize()
+    bad = sum(1 for c in b.statuses() if c)
+    if bad:
+        raise SystemExit(f"{bad} matrices reported a non-zero status during warm-up")
+    lib.paco_debug_batched_timing(1)
+    kt = (ctypes.c_float * 3)()
+    ksum = [0.0, 0.0, 0.0]
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = lib.paco_launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.fill_(k & 0xff)  # L2 flush, outside the timed window
+            ev[k][0].record(stream)
+            b.run(stream)
+            ev[k][1].record(stream)
+            stream.synchronize()
+            lib.paco_debug_batched_times(kt)
+            for j in range(3):
+                ksum[j] += kt[j]
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = lib.paco_launch_count() - launches0
+    lib.paco_debug_batched_timing(0)
+    clk = clocks.stop()
+    total_ms = max_over_ranks(sum(a.elapsed_time(c) for a, c in ev), dist)
+
+    # end to end: host (pinned) inputs in, host outputs back, every step
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda t: torch.empty(t.shape, dtype=t.dtype).pin_memory()
+        Ah, Uh, Vh, sh = pin(b.A_flat), pin(b.U_flat), pin(b.Vt_flat), pin(b.sigma_flat)
+        Ah.copy_(b.A_flat.cpu())
+        times = []
+        for k in range(max(1, min(args.steps, 3))):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+                b.A_flat.copy_(Ah, non_blocking=True)
+                b.run(stream)
+                Uh.copy_(b.U_flat, non_blocking=True)
+                Vh.copy_(b.Vt_flat, non_blocking=True)
+                sh.copy_(b.sigma_flat, non_blocking=True)
+                e1.record(stream)
+            stream.synchronize()
+            times.append(e0.elapsed_time(e1))
+        e2e = {"value": world * count / (statistics.median(times) / 1000.0), "unit": "SVDs/s",
+               "h2d_bytes_per_step": 4 * b.A_flat.numel(),
+               "d2h_bytes_per_step": 4 * (b.U_flat.numel() + b.Vt_flat.numel() + b.sigma_flat.numel())}
+
+    # the plain single-matrix path (paco_svd, direct launches) over a sample of the shapes
+    plain = None
+    if rank == 0:
+        sample = shapes[:: max(1, count // 60)][:60]
+        ws = [P.Workspace(m, n) for m, n in sample]
+        for w, (m, n) in zip(ws, sample):
+            w.A.normal_(generator=gen)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for w in ws:
+            w.run()
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t
+        plain = {"value": len(sample) / t, "unit": "SVDs/s",
+                 "sample": f"{len(sample)} matrices of the batch, one paco_svd call each, direct launches"}
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    peaks, peak_kind = measured_peaks()
+    steps = args.steps
+    # GEMV-phase algorithmic bytes: 8 * sum_i (M-i)(N-i) per matrix
+    alg = sum(8.0 * sum((m - i) * (n - i) for i in range(n)) for m, n in shapes)
+    k1 = ksum[0] / steps
+    achieved = alg / 1e9 / (k1 / 1e3)
+    value = world * steps * count / (total_ms / 1000.0)
+    line = {"metric": "SVDs/sec", "value": value, "unit": "SVDs/s", "n_gpus": world, "steps": steps,
+            "warmup": max(3, args.warmup), "ms_per_step": total_ms / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: {count} FP32 N(0,1) matrices, M uniform on [{wl['Mlo']}, "
+                                   f"{wl['Mhi']}], N uniform on [{wl['Nlo']}, M], one batched call per step",
+                       "count": count, "l2": "512 MiB buffer written between timed steps",
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+            "roofline": {"kernel": "bt_bidiag_k (batched bidiagonalization, one CTA per matrix)", "bound": "hbm",
+                         "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                         "alg_bytes_per_launch": alg,
+                         "alg_bytes_definition": "sum over matrices of 8*sum_i (M-i)(N-i)",
+                         "kernel_ms": {"bt_bidiag_k": k1, "bt_bdc_k": ksum[1] / steps, "bt_apply_k": ksum[2] / steps},
+                         "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)"},
+            "clocks": clk, "e2e": e2e, "gpu_launches": int(launches),
+            "plain_single_matrix": plain,
+            "batched_over_plain": (value / world / plain["value"]) if plain else None}
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline_batched(wl)
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()

@@ -805,6 +805,27 @@ extern "C" int paco_debug_batched_phases(const void *workspace, double out[12])
     return PACO_OK;
 }
 
+// Test hook (not in the public header): while enabled, the three launches of
+// each batched call are bracketed by CUDA events on the call's stream;
+// paco_debug_batched_times waits for the last call and returns the three
+// kernels' durations in milliseconds.
+static bool g_bt_timing = false;
+static cudaEvent_t g_bt_ev[4];
+
+extern "C" void paco_debug_batched_timing(int on)
+{
+    if (on && !g_bt_timing)
+        for (auto &e : g_bt_ev) cudaEventCreate(&e);
+    g_bt_timing = on != 0;
+}
+
+extern "C" int paco_debug_batched_times(float out[3])
+{
+    if (!g_bt_timing || cudaEventSynchronize(g_bt_ev[3]) != cudaSuccess) return PACO_ERR_CUDA;
+    for (int k = 0; k < 3; k++) cudaEventElapsedTime(&out[k], g_bt_ev[k], g_bt_ev[k + 1]);
+    return PACO_OK;
+}
+
 size_t paco_batched_workspace_size(int count, const int *M, const int *N)
 {
     BtPlan p;
@@ -847,10 +868,14 @@ int paco_svd_batched(int count, const int *M, const int *N, const float *const *
         cudaSuccess)
         return PACO_ERR_CUDA;
     char *arena = ws + p.arena_off;
+    if (g_bt_timing) cudaEventRecord(g_bt_ev[0], s);
     paco_count_launch(), bt_bidiag_k<<<p.slots1, bt::T_SWEEP, 0, s>>>(dit, count, queues + 0, arena, prof);
+    if (g_bt_timing) cudaEventRecord(g_bt_ev[1], s);
     paco_count_launch(), bt_bdc_k<<<p.slots2, bt::T_BDC, bt_dyn_smem(p.Nx), s>>>(
                              dit, count, queues + 1, arena, ws + p.bdc_off, p.bdc_slot, prof);
+    if (g_bt_timing) cudaEventRecord(g_bt_ev[2], s);
     paco_count_launch(), bt_apply_k<<<p.slots3, bt::T_SWEEP, 0, s>>>(
                              dit, count, queues + 2, arena, (float *)(ws + p.x_off), p.x_slot, status, prof);
+    if (g_bt_timing) cudaEventRecord(g_bt_ev[3], s);
     return cudaGetLastError() == cudaSuccess ? PACO_OK : PACO_ERR_CUDA;
 }

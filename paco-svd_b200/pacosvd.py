@@ -246,7 +246,10 @@ def batched_workspace_size(shapes) -> int:
 
 class Batch:
     """Device buffers of the batched form for a fixed list of shapes
-    (M <= 512, N <= M); reusable across calls."""
+    (M <= 512, N <= M); reusable across calls.  A, U, Vt and sigma of all
+    matrices live in four flat buffers (A_flat, U_flat, Vt_flat, sigma_flat),
+    so a whole batch moves between host and device in one copy each; the
+    per-matrix tensors in A, U, Vt, sigma are views into them."""
 
     def __init__(self, shapes, device="cuda"):
         torch = _torch()
@@ -257,10 +260,22 @@ class Batch:
             bad = any(n >= 1 and m >= n and m > PACO_BATCH_MAX_M for m, n in self.shapes)
             raise PacoError(PACO_ERR_UNSUPPORTED if bad else PACO_ERR_INVALID_ARG, "paco_batched_workspace_size")
         self.ws = torch.empty(self.nbytes, dtype=torch.uint8, device=device)
-        self.A = [torch.empty(m, n, device=device) for m, n in self.shapes]
-        self.U = [torch.empty(m, m, device=device) for m, _ in self.shapes]
-        self.Vt = [torch.empty(n, n, device=device) for _, n in self.shapes]
-        self.sigma = [torch.empty(n, device=device) for _, n in self.shapes]
+
+        def flat(sizes):
+            buf = torch.empty(max(1, sum(sizes)), device=device)
+            views, off = [], 0
+            for n in sizes:
+                views.append(buf.narrow(0, off, n))
+                off += n
+            return buf, views
+
+        self.A_flat, a = flat([m * n for m, n in self.shapes])
+        self.U_flat, u = flat([m * m for m, _ in self.shapes])
+        self.Vt_flat, v = flat([n * n for _, n in self.shapes])
+        self.sigma_flat, self.sigma = flat([n for _, n in self.shapes])
+        self.A = [t.view(m, n) for t, (m, n) in zip(a, self.shapes)]
+        self.U = [t.view(m, m) for t, (m, _) in zip(u, self.shapes)]
+        self.Vt = [t.view(n, n) for t, (_, n) in zip(v, self.shapes)]
         self.status = torch.zeros(self.count, dtype=torch.int32, device=device)
         vpa = ctypes.c_void_p * self.count
         self._Ms = _int_array([m for m, _ in self.shapes])
