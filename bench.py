@@ -130,9 +130,10 @@ def measured_peaks():
 
 
 def traffic_ratio():
-    """DRAM bytes per algorithmic byte of the row pass, from the committed ncu
-    summary (profiles/bd_row_pass.txt, line 'dram_per_alg_byte: X')."""
-    path = os.path.join(ROOT, "profiles", "bd_row_pass.txt")  # ncu, 8192x4096 row pass
+    """DRAM bytes per streamed byte of the persistent panel kernel, from the
+    committed ncu summary (profiles/bd_panel_pk_8192x4096.txt, line
+    'dram_per_alg_byte: X')."""
+    path = os.path.join(ROOT, "profiles", "bd_panel_pk_8192x4096.txt")
     try:
         for ln in open(path):
             if ln.startswith("dram_per_alg_byte:"):

@@ -111,7 +111,7 @@ void paco_ctx_destroy(paco_ctx *ctx);
 int paco_svd_noalloc(int M, int N, float *A, float *U, float *Vt, float *sigma, void *stream);
 
 /* Largest M (and so N) of a matrix of the batched form. */
-#define PACO_BATCH_MAX_M 512
+#define PACO_BATCH_MAX_M 2048
 
 /* Batched form (the reference runs one matrix per launch; this replaces a
  * host loop over main.cpp:126-158 for many independent small matrices).

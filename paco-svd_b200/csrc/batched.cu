@@ -1,11 +1,12 @@
-// Batched SVD of many small matrices (1 <= N <= M <= 512): three persistent
+// Batched SVD of many small matrices (1 <= N <= M <= 2048): three persistent
 // launches, each with a work queue over the matrices (largest first), so the
 // whole batch takes three kernels whatever its size:
 //   1. bt_bidiag_k (512 threads per matrix)  Golub-Kahan Householder
 //      bidiagonalization, unblocked, with the reflector convention of
 //      upper_bidiagonalization.cpp:182-218.  One fused sweep per column step:
 //      each warp owns whole rows (held in registers, lane l has columns l,
-//      l+32, ... of the active chunks), applies the left reflector H_i and the
+//      l+32, ... of the active chunks; rows wider than 512 columns go in
+//      segments, in two passes), applies the left reflector H_i and the
 //      right reflector G_i to them, and in the same sweep accumulates the
 //      column norm and the products S_j = sum_r x_r a_rj that the next step's
 //      left reflector needs (w_j = a_ij + S_j / v0), so the trailing block is
@@ -35,7 +36,6 @@ namespace bt {
 constexpr int T_SWEEP = 512;            // threads of kernels 1 and 3
 constexpr int W_SWEEP = T_SWEEP / 32;
 constexpr int T_BDC = 256;              // threads of kernel 2 (the bdc bodies assume 256)
-constexpr int MAXC = PACO_BATCH_MAX_M;  // widest row
 constexpr int KSMALL = 32;              // merges up to this k solve a secular root per thread
 }  // namespace bt
 
@@ -138,15 +138,37 @@ static __device__ __forceinline__ void bt_reflector(float x0, float sigma, int l
     *beta = mu;
 }
 
-// shared memory of the sweep kernels (1 and 3)
+// shared memory of the sweep kernels (1 and 3), carved from dynamic shared
+// memory for rows of at most maxc columns
 struct BtSweepSh {
-    float part[bt::W_SWEEP][bt::MAXC];  // per-warp partial column sums
-    float wv[bt::MAXC];                 // w of the current left reflector
-    float uv[bt::MAXC];                 // current right reflector (u_{i+1} = 1)
-    float rv[bt::MAXC];                 // pivot row after its left update
-    float ssig[bt::W_SWEEP];
-    int item, bad;
+    float *part;  // W_SWEEP x maxc per-warp partial column sums
+    float *wv;    // maxc: w of the current left reflector
+    float *uv;    // maxc: current right reflector (u_{i+1} = 1)
+    float *rv;    // maxc: pivot row after its left update
+    float *ssig;  // W_SWEEP
+    int *item, *bad;
+    int maxc;
 };
+
+__host__ __device__ static size_t bt_sweep_smem(int maxc)
+{
+    return sizeof(float) * ((size_t)(bt::W_SWEEP + 3) * maxc + bt::W_SWEEP) + 4 * sizeof(int);
+}
+
+static __device__ BtSweepSh bt_sweep_sh(unsigned char *raw, int maxc)
+{
+    BtSweepSh sh;
+    float *f = reinterpret_cast<float *>(raw);
+    sh.maxc = maxc;
+    sh.part = f;
+    sh.wv = f + (size_t)bt::W_SWEEP * maxc;
+    sh.uv = sh.wv + maxc;
+    sh.rv = sh.uv + maxc;
+    sh.ssig = sh.rv + maxc;
+    sh.item = reinterpret_cast<int *>(sh.ssig + bt::W_SWEEP);
+    sh.bad = sh.item + 1;
+    return sh;
+}
 
 // rows in flight per warp for NA active 32-column chunks (<= 48 row values
 // per lane in registers)
@@ -175,7 +197,7 @@ static __device__ __forceinline__ int bt_next(unsigned *queue, int count, int *s
 // instead (NaN/Inf -> 0, flagged) and does no update.  Each warp has RB rows
 // in flight (rows base + rb * W_SWEEP + warp).  Column ci lies in chunk q0.
 template <int MODE, int NA>
-static __device__ void bt_sweep(BtSweepSh &sh, const float *A, float *W, long ldw, int M, int N, int r0, int ci,
+static __device__ void bt_sweep(const BtSweepSh &sh, const float *A, float *W, long ldw, int M, int N, int r0, int ci,
                                 int q0, float inv_v0, float tq, float tp, int *bad)
 {
     using namespace bt;
@@ -254,20 +276,120 @@ static __device__ void bt_sweep(BtSweepSh &sh, const float *A, float *W, long ld
 #pragma unroll
     for (int j = 0; j < NA; j++) {
         const int c = c0 + 32 * j;
-        if (c < N) sh.part[warp][c] = acc[j];
+        if (c < N) sh.part[warp * sh.maxc + c] = acc[j];
+    }
+    if (lane == 0) sh.ssig[warp] = ssig;
+}
+
+// bt_sweep for rows wider than 16 chunks: each warp takes one row at a time
+// in segments of 512 columns, in two passes (left update and the dot with
+// the right reflector, then the right update and the sums for the next
+// column reflector, which go straight into the warp's row of part).
+template <int MODE>
+static __device__ void bt_sweep_wide(const BtSweepSh &sh, const float *A, float *W, long ldw, int M, int N, int r0,
+                                     int ci, float inv_v0, float tq, float tp, int *bad)
+{
+    using namespace bt;
+    constexpr int SEG = 16, NW = W_SWEEP;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int cn = ci + 1;
+    const int q0 = ci < 0 ? 0 : ci >> 5;
+    const int cbeg = 32 * q0;
+    float *mypart = sh.part + warp * sh.maxc;
+    for (int c = cbeg + lane; c < N; c += 32) mypart[c] = 0.f;
+    float ssig = 0.f;
+    for (int r = r0 + warp; r < M; r += NW) {
+        float *row = W + (long)r * ldw;
+        float xn = 0.f;
+        if (MODE == 0) {
+            const float *src = A + (long)r * N;
+            for (int s0 = cbeg; s0 < N; s0 += 32 * SEG) {
+                float a[SEG];
+#pragma unroll
+                for (int j = 0; j < SEG; j++) {
+                    const int c = s0 + 32 * j + lane;
+                    float x = (c < N) ? src[c] : 0.f;
+                    if (!isfinite(x)) { x = 0.f; *bad = 1; }
+                    a[j] = x;
+                    if (c < N) row[c] = x;
+                }
+                if (s0 == cbeg) xn = __shfl_sync(0xffffffffu, a[0], 0);
+                if (r > cn) {
+#pragma unroll
+                    for (int j = 0; j < SEG; j++) {
+                        const int c = s0 + 32 * j + lane;
+                        if (c > cn && c < N) mypart[c] += xn * a[j];
+                    }
+                }
+            }
+        } else {
+            float vr = 0.f, dot = 0.f;
+            for (int s0 = cbeg; s0 < N; s0 += 32 * SEG) {
+                float a[SEG];
+#pragma unroll
+                for (int j = 0; j < SEG; j++) {
+                    const int c = s0 + 32 * j + lane;
+                    a[j] = (c >= ci && c < N) ? row[c] : 0.f;
+                }
+                if (s0 == cbeg) {
+                    vr = __shfl_sync(0xffffffffu, a[0], ci & 31) * inv_v0;
+                    if (lane == (ci & 31)) row[ci] = vr;
+                }
+                const float lf = tq * vr;
+#pragma unroll
+                for (int j = 0; j < SEG; j++) {
+                    const int c = s0 + 32 * j + lane;
+                    if (c > ci && c < N) {
+                        a[j] -= lf * sh.wv[c];
+                        dot += a[j] * sh.uv[c];
+                        row[c] = a[j];
+                    }
+                }
+            }
+            dot = warp_sum(dot) * tp;
+            for (int s0 = cbeg; s0 < N; s0 += 32 * SEG) {
+                float a[SEG];
+#pragma unroll
+                for (int j = 0; j < SEG; j++) {
+                    const int c = s0 + 32 * j + lane;
+                    if (c > ci && c < N) {
+                        a[j] = row[c] - dot * sh.uv[c];
+                        row[c] = a[j];
+                    } else {
+                        a[j] = 0.f;
+                    }
+                }
+                if (s0 == cbeg) {
+                    const float xs = ((cn >> 5) > q0) ? a[1] : a[0];
+                    xn = __shfl_sync(0xffffffffu, xs, cn & 31);
+                }
+                if (cn < N && r > cn) {
+#pragma unroll
+                    for (int j = 0; j < SEG; j++) {
+                        const int c = s0 + 32 * j + lane;
+                        if (c > cn && c < N) mypart[c] += xn * a[j];
+                    }
+                }
+            }
+        }
+        if (cn < N && r > cn) ssig += xn * xn;
     }
     if (lane == 0) sh.ssig[warp] = ssig;
 }
 
 // bt_sweep over the chunks q0 .. (N-1)/32
 template <int MODE>
-static __device__ void bt_sweep_any(BtSweepSh &sh, const float *A, float *W, long ldw, int M, int N, int r0,
+static __device__ void bt_sweep_any(const BtSweepSh &sh, const float *A, float *W, long ldw, int M, int N, int r0,
                                     int ci, float inv_v0, float tq, float tp, int *bad)
 {
     const int q0 = ci < 0 ? 0 : ci >> 5;
     const int na = ((N - 1) >> 5) - q0 + 1;
 #define BT_SWEEP_CASE(K) \
     case K: bt_sweep<MODE, K>(sh, A, W, ldw, M, N, r0, ci, q0, inv_v0, tq, tp, bad); break;
+    if (na > 16) {
+        bt_sweep_wide<MODE>(sh, A, W, ldw, M, N, r0, ci, inv_v0, tq, tp, bad);
+        return;
+    }
     switch (na) {
         BT_SWEEP_CASE(1) BT_SWEEP_CASE(2) BT_SWEEP_CASE(3) BT_SWEEP_CASE(4)
         BT_SWEEP_CASE(5) BT_SWEEP_CASE(6) BT_SWEEP_CASE(7) BT_SWEEP_CASE(8)
@@ -279,14 +401,14 @@ static __device__ void bt_sweep_any(BtSweepSh &sh, const float *A, float *W, lon
 }
 
 // Stage 1 for one matrix: d, e, tauq, taup and the Householder vectors in W.
-static __device__ void bt_bidiag(BtSweepSh &sh, const float *A, const BtMat &m, int M, int N)
+static __device__ void bt_bidiag(const BtSweepSh &sh, const float *A, const BtMat &m, int M, int N)
 {
     using namespace bt;
     constexpr int NT = T_SWEEP, NW = W_SWEEP;
     const int tid = threadIdx.x;
     float *W = m.W;
     const long ldw = m.ldw;
-    bt_sweep_any<0>(sh, A, W, ldw, M, N, 0, -1, 0.f, 0.f, 0.f, &sh.bad);
+    bt_sweep_any<0>(sh, A, W, ldw, M, N, 0, -1, 0.f, 0.f, 0.f, sh.bad);
     __syncthreads();
     for (int i = 0; i < N; i++) {
         // column reflector i from the sums of the previous sweep (every
@@ -302,7 +424,7 @@ static __device__ void bt_bidiag(BtSweepSh &sh, const float *A, const BtMat &m, 
         for (int c = i + 1 + tid; c < N; c += NT) {
             float S = 0.f;
 #pragma unroll
-            for (int w = 0; w < NW; w++) S += sh.part[w][c];
+            for (int w = 0; w < NW; w++) S += sh.part[w * sh.maxc + c];
             const float aic = W[(long)i * ldw + c];
             const float wj = aic + inv_v0 * S;
             sh.wv[c] = wj;
@@ -342,21 +464,22 @@ static __device__ void bt_bidiag(BtSweepSh &sh, const float *A, const BtMat &m, 
 
 // prof[0]: SM cycles of kernel 1 per matrix, summed
 __global__ void __launch_bounds__(bt::T_SWEEP, 1) bt_bidiag_k(const BtItem *items, int count, unsigned *queue,
-                                                              char *arena, unsigned long long *prof)
+                                                              char *arena, int maxc, unsigned long long *prof)
 {
-    __shared__ BtSweepSh sh;
+    extern __shared__ __align__(16) unsigned char bt_sm1[];
+    const BtSweepSh sh = bt_sweep_sh(bt_sm1, maxc);
     for (;;) {
-        const int b = bt_next(queue, count, &sh.item);
+        const int b = bt_next(queue, count, sh.item);
         if (b < 0) break;
         const BtItem it = items[b];
         BtMat m;
         bt_mat_carve(arena + it.moff, it.M, it.N, &m);
-        if (threadIdx.x == 0) sh.bad = 0;
+        if (threadIdx.x == 0) *sh.bad = 0;
         __syncthreads();
         const long long t0 = clock64();
         bt_bidiag(sh, it.A, m, it.M, it.N);
         if (threadIdx.x == 0) {
-            *m.code = sh.bad ? PACO_ERR_NONFINITE : 0;
+            *m.code = *sh.bad ? PACO_ERR_NONFINITE : 0;
             atomicAdd(&prof[0], (unsigned long long)(clock64() - t0));
         }
     }
@@ -549,7 +672,7 @@ __global__ void __launch_bounds__(bt::T_BDC, 2) bt_bdc_k(const BtItem *items, in
 // with v_{k+sh_off} = 1 and v_r = vec(k, r) for r > k + sh_off.  Each sweep
 // applies reflector k and accumulates the w of reflector k-1.
 template <int NA, typename Vec>
-static __device__ void bt_apply_back_n(BtSweepSh &sh, float *Y, long ldy, int R, int C, int k1, int sh_off,
+static __device__ void bt_apply_back_n(const BtSweepSh &sh, float *Y, long ldy, int R, int C, int k1, int sh_off,
                                        const float *tau, Vec vec)
 {
     using namespace bt;
@@ -574,13 +697,13 @@ static __device__ void bt_apply_back_n(BtSweepSh &sh, float *Y, long ldy, int R,
 #pragma unroll
         for (int j = 0; j < NA; j++) {
             const int c = lane + 32 * j;
-            if (c < C) sh.part[warp][c] = acc[j];
+            if (c < C) sh.part[warp * sh.maxc + c] = acc[j];
         }
         __syncthreads();
         for (int c = tid; c < C; c += NT) {
             float w = 0.f;
 #pragma unroll
-            for (int x = 0; x < NW; x++) w += sh.part[x][c];
+            for (int x = 0; x < NW; x++) w += sh.part[x * sh.maxc + c];
             sh.wv[c] = w;
         }
         __syncthreads();
@@ -627,14 +750,71 @@ static __device__ void bt_apply_back_n(BtSweepSh &sh, float *Y, long ldy, int R,
 #pragma unroll
         for (int j = 0; j < NA; j++) {
             const int c = lane + 32 * j;
-            if (c < C) sh.part[warp][c] = acc[j];
+            if (c < C) sh.part[warp * sh.maxc + c] = acc[j];
         }
         __syncthreads();
         // row p - 1 is untouched by reflector k: w' = Y[p-1] + sum of the partials
         for (int c = tid; c < C; c += NT) {
             float w = Y[(long)(p - 1) * ldy + c];
 #pragma unroll
-            for (int x = 0; x < NW; x++) w += sh.part[x][c];
+            for (int x = 0; x < NW; x++) w += sh.part[x * sh.maxc + c];
+            sh.wv[c] = w;
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+}
+
+// bt_apply_back_n for rows wider than 16 chunks: one row at a time per warp,
+// the sums for the next reflector accumulated in the warp's row of part.
+template <typename Vec>
+static __device__ void bt_apply_back_wide(const BtSweepSh &sh, float *Y, long ldy, int R, int C, int k1, int sh_off,
+                                          const float *tau, Vec vec)
+{
+    using namespace bt;
+    constexpr int NT = T_SWEEP, NW = W_SWEEP;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    float *mypart = sh.part + warp * sh.maxc;
+    {
+        const int p = k1 + sh_off;
+        for (int c = lane; c < C; c += 32) mypart[c] = 0.f;
+        for (int r = p + warp; r < R; r += NW) {
+            const float vr = (r == p) ? 1.f : vec(k1, r);
+            const float *row = Y + (long)r * ldy;
+            for (int c = lane; c < C; c += 32) mypart[c] += vr * row[c];
+        }
+        __syncthreads();
+        for (int c = tid; c < C; c += NT) {
+            float w = 0.f;
+#pragma unroll
+            for (int x = 0; x < NW; x++) w += sh.part[x * sh.maxc + c];
+            sh.wv[c] = w;
+        }
+        __syncthreads();
+    }
+    for (int k = k1; k >= 0; k--) {
+        const int p = k + sh_off;
+        const float tk = tau[k];
+        const bool nxt = k > 0;
+        for (int c = lane; c < C; c += 32) mypart[c] = 0.f;
+        for (int r = p + warp; r < R; r += NW) {
+            const float vr = (r == p) ? 1.f : vec(k, r);
+            const float vn = nxt ? vec(k - 1, r) : 0.f;
+            const float f = tk * vr;
+            float *row = Y + (long)r * ldy;
+#pragma unroll 4
+            for (int c = lane; c < C; c += 32) {
+                const float v = row[c] - f * sh.wv[c];
+                row[c] = v;
+                mypart[c] += vn * v;
+            }
+        }
+        if (!nxt) break;
+        __syncthreads();
+        for (int c = tid; c < C; c += NT) {
+            float w = Y[(long)(p - 1) * ldy + c];
+#pragma unroll
+            for (int x = 0; x < NW; x++) w += sh.part[x * sh.maxc + c];
             sh.wv[c] = w;
         }
         __syncthreads();
@@ -643,10 +823,14 @@ static __device__ void bt_apply_back_n(BtSweepSh &sh, float *Y, long ldy, int R,
 }
 
 template <typename Vec>
-static __device__ void bt_apply_back(BtSweepSh &sh, float *Y, long ldy, int R, int C, int k1, int sh_off,
+static __device__ void bt_apply_back(const BtSweepSh &sh, float *Y, long ldy, int R, int C, int k1, int sh_off,
                                      const float *tau, Vec vec)
 {
     if (k1 < 0) return;
+    if (C > 512) {
+        bt_apply_back_wide(sh, Y, ldy, R, C, k1, sh_off, tau, vec);
+        return;
+    }
 #define BT_APPLY_CASE(K) \
     case K: bt_apply_back_n<K>(sh, Y, ldy, R, C, k1, sh_off, tau, vec); break;
     switch ((C + 31) >> 5) {
@@ -676,15 +860,16 @@ struct BtRowVec {
 // the outputs; matrices finished
 __global__ void __launch_bounds__(bt::T_SWEEP, 1) bt_apply_k(const BtItem *items, int count, unsigned *queue,
                                                              char *arena, float *xslots, size_t xslot_floats,
-                                                             int *status, unsigned long long *prof)
+                                                             int maxc, int *status, unsigned long long *prof)
 {
     using namespace bt;
     constexpr int NT = T_SWEEP;
-    __shared__ BtSweepSh sh;
+    extern __shared__ __align__(16) unsigned char bt_sm3[];
+    const BtSweepSh sh = bt_sweep_sh(bt_sm3, maxc);
     const int tid = threadIdx.x;
     float *X = xslots + (size_t)blockIdx.x * xslot_floats;
     for (;;) {
-        const int b = bt_next(queue, count, &sh.item);
+        const int b = bt_next(queue, count, sh.item);
         if (b < 0) break;
         const BtItem it = items[b];
         const int M = it.M, N = it.N;
@@ -731,7 +916,7 @@ __global__ void __launch_bounds__(bt::T_SWEEP, 1) bt_apply_k(const BtItem *items
 static size_t bt_dyn_smem(int maxN) { return (size_t)20 * std::max(1, maxN) + 64; }
 
 struct BtPlan {
-    int Mx, Nx, slots1, slots2, slots3;
+    int Mx, Nx, slots1, slots2, slots3, maxc1, maxc3;
     size_t items_off, arena_off, arena_bytes, bdc_off, bdc_slot, x_off, x_slot, total;
     std::vector<size_t> moff;
 };
@@ -764,9 +949,14 @@ static bool bt_plan(int count, const int *M, const int *N, BtPlan *p)
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(bt_bdc_k, cudaFuncAttributeMaxDynamicSharedMemorySize, 48 * 1024);
+        const int big = (int)bt_sweep_smem(PACO_BATCH_MAX_M);
+        cudaFuncSetAttribute(bt_bidiag_k, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+        cudaFuncSetAttribute(bt_apply_k, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaGetLastError();
         attr = true;
     }
+    p->maxc1 = (Nx + 31) & ~31;
+    p->maxc3 = (Mx + 31) & ~31;
     p->Mx = Mx;
     p->Nx = Nx;
     p->items_off = 256;
@@ -782,9 +972,11 @@ static bool bt_plan(int count, const int *M, const int *N, BtPlan *p)
     BtBdcSlot sl;
     p->bdc_slot = bt_bdc_carve(nullptr, Nx, &sl);
     p->x_slot = (size_t)Nx * Nx;
-    p->slots1 = std::min(count, sms * bt_occupancy((const void *)bt_bidiag_k, bt::T_SWEEP, 0));
+    p->slots1 = std::min(count, sms * bt_occupancy((const void *)bt_bidiag_k, bt::T_SWEEP, bt_sweep_smem(p->maxc1)));
     p->slots2 = std::min(count, sms * bt_occupancy((const void *)bt_bdc_k, bt::T_BDC, bt_dyn_smem(Nx)));
-    p->slots3 = std::min(count, sms * bt_occupancy((const void *)bt_apply_k, bt::T_SWEEP, 0));
+    // divide-and-conquer scratch is N^2-sized per CTA: at most about 4 GiB of it
+    p->slots2 = std::max(1, std::min(p->slots2, (int)std::max<size_t>(sms / 4, ((size_t)4 << 30) / p->bdc_slot)));
+    p->slots3 = std::min(count, sms * bt_occupancy((const void *)bt_apply_k, bt::T_SWEEP, bt_sweep_smem(p->maxc3)));
     p->bdc_off = p->arena_off + a;
     p->x_off = p->bdc_off + p->bdc_slot * p->slots2;
     p->total = p->x_off + ((sizeof(float) * p->x_slot * p->slots3 + 255) & ~(size_t)255);
@@ -869,13 +1061,14 @@ int paco_svd_batched(int count, const int *M, const int *N, const float *const *
         return PACO_ERR_CUDA;
     char *arena = ws + p.arena_off;
     if (g_bt_timing) cudaEventRecord(g_bt_ev[0], s);
-    paco_count_launch(), bt_bidiag_k<<<p.slots1, bt::T_SWEEP, 0, s>>>(dit, count, queues + 0, arena, prof);
+    paco_count_launch(), bt_bidiag_k<<<p.slots1, bt::T_SWEEP, bt_sweep_smem(p.maxc1), s>>>(dit, count, queues + 0,
+                                                                                           arena, p.maxc1, prof);
     if (g_bt_timing) cudaEventRecord(g_bt_ev[1], s);
     paco_count_launch(), bt_bdc_k<<<p.slots2, bt::T_BDC, bt_dyn_smem(p.Nx), s>>>(
                              dit, count, queues + 1, arena, ws + p.bdc_off, p.bdc_slot, prof);
     if (g_bt_timing) cudaEventRecord(g_bt_ev[2], s);
-    paco_count_launch(), bt_apply_k<<<p.slots3, bt::T_SWEEP, 0, s>>>(
-                             dit, count, queues + 2, arena, (float *)(ws + p.x_off), p.x_slot, status, prof);
+    paco_count_launch(), bt_apply_k<<<p.slots3, bt::T_SWEEP, bt_sweep_smem(p.maxc3), s>>>(
+                             dit, count, queues + 2, arena, (float *)(ws + p.x_off), p.x_slot, p.maxc3, status, prof);
     if (g_bt_timing) cudaEventRecord(g_bt_ev[3], s);
     return cudaGetLastError() == cudaSuccess ? PACO_OK : PACO_ERR_CUDA;
 }

@@ -231,7 +231,7 @@ def svd(A, check=True):
     return s.clone(), U.clone(), Vt.clone()
 
 
-PACO_BATCH_MAX_M = 512
+PACO_BATCH_MAX_M = 2048
 
 
 def _int_array(vals):
@@ -246,7 +246,7 @@ def batched_workspace_size(shapes) -> int:
 
 class Batch:
     """Device buffers of the batched form for a fixed list of shapes
-    (M <= 512, N <= M); reusable across calls.  A, U, Vt and sigma of all
+    (M <= 2048, N <= M); reusable across calls.  A, U, Vt and sigma of all
     matrices live in four flat buffers (A_flat, U_flat, Vt_flat, sigma_flat),
     so a whole batch moves between host and device in one copy each; the
     per-matrix tensors in A, U, Vt, sigma are views into them."""
@@ -300,7 +300,7 @@ class Batch:
 
 
 def svd_batched(As, check=True):
-    """SVD of a list of float32 CUDA (or numpy) matrices, M <= 512, N <= M, in
+    """SVD of a list of float32 CUDA (or numpy) matrices, M <= 2048, N <= M, in
     one batched launch.  Returns lists (sigma, U, Vt) and the per-matrix status."""
     torch = _torch()
     As = [a if hasattr(a, "data_ptr") else torch.from_numpy(np.ascontiguousarray(a, np.float32)) for a in As]

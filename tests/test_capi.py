@@ -111,14 +111,14 @@ def test_noalloc_scratch_covers_its_largest_shape():
 def test_batched_workspace_rejects_bad_shapes():
     assert P.batched_workspace_size([(4, 8)]) == 0               # M < N
     assert P.batched_workspace_size([(10, 0)]) == 0              # N = 0
-    assert P.batched_workspace_size([(513, 10)]) == 0            # M beyond the batched limit
+    assert P.batched_workspace_size([(2049, 10)]) == 0           # M beyond the batched limit
     assert P.batched_workspace_size([]) == 0
 
 
 def test_batched_entry_validates_before_touching_the_device():
     import ctypes as C
     L = P.lib()
-    Ms, Ns = (C.c_int * 1)(600), (C.c_int * 1)(10)
+    Ms, Ns = (C.c_int * 1)(3000), (C.c_int * 1)(10)
     nul = (C.c_void_p * 1)(None)
     assert L.paco_svd_batched(1, Ms, Ns, nul, nul, nul, nul, None, None, 0, None) == P.PACO_ERR_UNSUPPORTED
     Ms[0] = 3

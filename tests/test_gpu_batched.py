@@ -107,6 +107,17 @@ def test_batched_flags_a_nonfinite_matrix_only():
         check(mats[k], s[k], U[k], Vt[k])
 
 
+def test_batched_wide_rows_match_lapack():
+    # rows wider than 512 columns take the segmented sweeps
+    rng = np.random.default_rng(17)
+    shapes = [(600, 513), (700, 650), (1100, 600), (2048, 64), (530, 530), (64, 60)]
+    mats = [rng.standard_normal(s).astype(np.float32) for s in shapes]
+    s, U, Vt, st = P.svd_batched(mats)
+    assert st == [0] * len(mats)
+    for k, A in enumerate(mats):
+        check(A, s[k], U[k], Vt[k])
+
+
 def test_batched_matches_single_matrix_path_within_tolerance():
     mats = mixed_batch(13, 5)
     s, U, Vt, _ = P.svd_batched(mats)
