@@ -42,6 +42,9 @@ WORKLOADS = {
     "cfg3": dict(M=8192, N=4096, gen="clustered"),
     # batched form: 10,000 matrices, M uniform on [32, 512], N uniform on [16, M], iid N(0,1)
     "cfg4": dict(kind="batched", count=10000, Mlo=32, Mhi=512, Nlo=16, gen="normal"),
+    # serving form: Poisson requests at 2,000/s for 60 s, 90% M log-uniform on [16, 256], 10% on
+    # [256, 2048], N uniform on [M/4, M], 20% graded spectra, 64 GB device working-set cap
+    "cfg5": dict(kind="serving", rate=2000.0, seconds=60.0, cap_gb=64),
 }
 CPU_SAMPLE_N = 768  # oracle sample size (about 5 s of single-thread work)
 
@@ -204,6 +207,10 @@ def run_reference(args, wl, rank):
     if rank != 0:
         return
     batched = wl.get("kind") == "batched"
+    if wl.get("kind") == "serving":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving mode; its CPU "
+                          "algorithm is timed per matrix by the batched and single-matrix workloads"}))
+        return
     cb = cpu_baseline_batched(wl) if batched else cpu_baseline(wl, steps=args.steps)
     line = {"metric": "SVDs/sec", "value": cb["value"], "unit": "SVDs/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -226,6 +233,7 @@ def main():
     ap.add_argument("--workload", default="cfg2a", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end measurement")
+    ap.add_argument("--serve-seconds", type=float, default=None, help="length of the serving trace")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
 
@@ -248,6 +256,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     if wl.get("kind") == "batched":
         run_batched(args, wl, rank, world, local, dist)
+        return
+    if wl.get("kind") == "serving":
+        run_serving(args, wl, rank, world, local, dist)
         return
     M, N = wl["M"], wl["N"]
     A_host, sig_exact = make_matrix(wl, seed=1234 + rank, with_sigma=True)
@@ -505,6 +516,85 @@ def run_batched(args, wl, rank, world, local, dist):
             "batched_over_plain": (value / world / plain["value"]) if plain else None}
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline_batched(wl)
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_serving(args, wl, rank, world, local, dist):
+    """cfg5: a Poisson trace through the continuous-batching loop of serve.py.
+    Inputs are generated on the device before the clock starts (a request's A
+    is resident when it arrives); latency = completion - arrival."""
+    import torch
+    import pacosvd as P
+    import serve as S
+
+    seconds = args.serve_seconds or wl["seconds"]
+    arr = S.poisson_arrivals(wl["rate"], seconds, 2024 + rank)
+    M, N, graded = S.serving_shapes(len(arr), 2025 + rank)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(7 + rank)
+    t = time.perf_counter()
+    reqs = [S.Request(k, S.make_input(int(m), int(n), bool(g), gen)) for k, (m, n, g) in enumerate(zip(M, N, graded))]
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t
+    # warm the loop (library plans, allocator pools) on a short slice of the same mix
+    warm = [S.Request(-1 - k, r.A.clone()) for k, r in enumerate(reqs[:200])]
+    S.run_trace(S.SvdServer(cap_bytes=wl["cap_gb"] << 30), warm, np.zeros(len(warm)))
+    srv = S.SvdServer(cap_bytes=wl["cap_gb"] << 30)
+    lib = P.lib()
+    lib.paco_launch_count.restype = ctypes.c_ulonglong
+    launches0 = lib.paco_launch_count()
+    clocks = ClockSampler(local)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    wall = S.run_trace(srv, reqs, arr)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = lib.paco_launch_count() - launches0
+    done = srv.completed
+    span = max(r.done for r in done) - min(r.arrival for r in done)
+    span = max_over_ranks(span * 1000.0, dist) / 1000.0
+    stats = S.latency_stats(done)
+    errors = len(srv.status_errors())
+    small = [r for r in done if r.M <= srv.small_max]
+    large = [r for r in done if r.M > srv.small_max]
+
+    # the plain single-matrix path (one paco_svd call per request, direct launches) on a sample
+    plain = None
+    if rank == 0:
+        rng = np.random.default_rng(3)
+        idx = rng.choice(len(M), size=min(200, len(M)), replace=False)
+        ws = [P.Workspace(int(M[k]), int(N[k])) for k in idx]
+        for w in ws:
+            w.A.normal_(generator=gen)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for w in ws:
+            w.run()
+        torch.cuda.synchronize()
+        plain = {"value": len(ws) / (time.perf_counter() - t), "unit": "SVDs/s",
+                 "sample": f"{len(ws)} requests of the same mix, one paco_svd call each, direct launches"}
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    value = world * len(done) / span
+    line = {"metric": "SVDs/sec", "value": value, "unit": "SVDs/s", "n_gpus": world, "steps": 1, "warmup": 1,
+            "ms_per_step": span * 1000.0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"cfg5: Poisson requests at {wl['rate']:.0f}/s for {seconds:.0f} s, 90% M "
+                                   f"log-uniform on [16, 256], 10% on [256, 2048], N uniform on [M/4, M], 20% "
+                                   f"graded spectra, {wl['cap_gb']} GB working-set cap; continuous batching",
+                       "requests": len(done), "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+            "latency": dict(stats, small=S.latency_stats(small) if small else None,
+                            large=S.latency_stats(large) if large else None),
+            "offered_rate": wl["rate"], "wall_s": wall, "batches": srv.batches, "status_errors": errors,
+            "peak_working_set_gb": srv.peak_inflight / 1e9, "input_setup_s": setup_s,
+            "clocks": clk, "e2e": None, "gpu_launches": int(launches),
+            "plain_single_matrix": plain, "served_over_plain": (value / world / plain["value"]) if plain else None}
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()

@@ -27,6 +27,7 @@
 // back-transform scratch lives in one slot per CTA.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "batched.cuh"
@@ -281,8 +282,8 @@ static __device__ void bt_sweep(const BtSweepSh &sh, const float *A, float *W, l
     if (lane == 0) sh.ssig[warp] = ssig;
 }
 
-// bt_sweep for rows wider than 16 chunks: each warp takes one row at a time
-// in segments of 512 columns, in two passes (left update and the dot with
+// bt_sweep for rows wider than 16 chunks: each warp takes RW rows at a time,
+// in segments of 512 columns and two passes (left update and the dot with
 // the right reflector, then the right update and the sums for the next
 // column reflector, which go straight into the warp's row of part).
 template <int MODE>
@@ -290,7 +291,7 @@ static __device__ void bt_sweep_wide(const BtSweepSh &sh, const float *A, float 
                                      int ci, float inv_v0, float tq, float tp, int *bad)
 {
     using namespace bt;
-    constexpr int SEG = 16, NW = W_SWEEP;
+    constexpr int SEG = 16, NW = W_SWEEP, RW = 2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int cn = ci + 1;
     const int q0 = ci < 0 ? 0 : ci >> 5;
@@ -298,81 +299,122 @@ static __device__ void bt_sweep_wide(const BtSweepSh &sh, const float *A, float 
     float *mypart = sh.part + warp * sh.maxc;
     for (int c = cbeg + lane; c < N; c += 32) mypart[c] = 0.f;
     float ssig = 0.f;
-    for (int r = r0 + warp; r < M; r += NW) {
-        float *row = W + (long)r * ldw;
-        float xn = 0.f;
-        if (MODE == 0) {
-            const float *src = A + (long)r * N;
-            for (int s0 = cbeg; s0 < N; s0 += 32 * SEG) {
-                float a[SEG];
+    for (int base = r0 + warp * RW; base < M; base += NW * RW) {
+        const int nr = min(RW, M - base);
+        float xn[RW];
 #pragma unroll
-                for (int j = 0; j < SEG; j++) {
-                    const int c = s0 + 32 * j + lane;
-                    float x = (c < N) ? src[c] : 0.f;
-                    if (!isfinite(x)) { x = 0.f; *bad = 1; }
-                    a[j] = x;
-                    if (c < N) row[c] = x;
-                }
-                if (s0 == cbeg) xn = __shfl_sync(0xffffffffu, a[0], 0);
-                if (r > cn) {
+        for (int w = 0; w < RW; w++) xn[w] = 0.f;
+        if (MODE == 0) {
+            for (int s0 = cbeg; s0 < N; s0 += 32 * SEG) {
+                float a[RW][SEG];
+#pragma unroll
+                for (int w = 0; w < RW; w++) {
+                    const float *src = A + (long)(base + w) * N;
 #pragma unroll
                     for (int j = 0; j < SEG; j++) {
                         const int c = s0 + 32 * j + lane;
-                        if (c > cn && c < N) mypart[c] += xn * a[j];
+                        a[w][j] = (w < nr && c < N) ? src[c] : 0.f;
+                    }
+                }
+#pragma unroll
+                for (int w = 0; w < RW; w++) {
+                    if (w >= nr) break;
+                    const int r = base + w;
+                    float *row = W + (long)r * ldw;
+#pragma unroll
+                    for (int j = 0; j < SEG; j++) {
+                        const int c = s0 + 32 * j + lane;
+                        if (!isfinite(a[w][j])) { a[w][j] = 0.f; *bad = 1; }
+                        if (c < N) row[c] = a[w][j];
+                    }
+                    if (s0 == cbeg) xn[w] = __shfl_sync(0xffffffffu, a[w][0], 0);
+                    if (r > cn) {
+#pragma unroll
+                        for (int j = 0; j < SEG; j++) {
+                            const int c = s0 + 32 * j + lane;
+                            if (c > cn && c < N) mypart[c] += xn[w] * a[w][j];
+                        }
                     }
                 }
             }
         } else {
-            float vr = 0.f, dot = 0.f;
+            float vr[RW], dot[RW];
+#pragma unroll
+            for (int w = 0; w < RW; w++) { vr[w] = 0.f; dot[w] = 0.f; }
             for (int s0 = cbeg; s0 < N; s0 += 32 * SEG) {
-                float a[SEG];
+                float a[RW][SEG];
 #pragma unroll
-                for (int j = 0; j < SEG; j++) {
-                    const int c = s0 + 32 * j + lane;
-                    a[j] = (c >= ci && c < N) ? row[c] : 0.f;
-                }
-                if (s0 == cbeg) {
-                    vr = __shfl_sync(0xffffffffu, a[0], ci & 31) * inv_v0;
-                    if (lane == (ci & 31)) row[ci] = vr;
-                }
-                const float lf = tq * vr;
-#pragma unroll
-                for (int j = 0; j < SEG; j++) {
-                    const int c = s0 + 32 * j + lane;
-                    if (c > ci && c < N) {
-                        a[j] -= lf * sh.wv[c];
-                        dot += a[j] * sh.uv[c];
-                        row[c] = a[j];
-                    }
-                }
-            }
-            dot = warp_sum(dot) * tp;
-            for (int s0 = cbeg; s0 < N; s0 += 32 * SEG) {
-                float a[SEG];
-#pragma unroll
-                for (int j = 0; j < SEG; j++) {
-                    const int c = s0 + 32 * j + lane;
-                    if (c > ci && c < N) {
-                        a[j] = row[c] - dot * sh.uv[c];
-                        row[c] = a[j];
-                    } else {
-                        a[j] = 0.f;
-                    }
-                }
-                if (s0 == cbeg) {
-                    const float xs = ((cn >> 5) > q0) ? a[1] : a[0];
-                    xn = __shfl_sync(0xffffffffu, xs, cn & 31);
-                }
-                if (cn < N && r > cn) {
+                for (int w = 0; w < RW; w++) {
+                    const float *row = W + (long)(base + w) * ldw;
 #pragma unroll
                     for (int j = 0; j < SEG; j++) {
                         const int c = s0 + 32 * j + lane;
-                        if (c > cn && c < N) mypart[c] += xn * a[j];
+                        a[w][j] = (w < nr && c >= ci && c < N) ? row[c] : 0.f;
+                    }
+                }
+#pragma unroll
+                for (int w = 0; w < RW; w++) {
+                    if (w >= nr) break;
+                    float *row = W + (long)(base + w) * ldw;
+                    if (s0 == cbeg) {
+                        vr[w] = __shfl_sync(0xffffffffu, a[w][0], ci & 31) * inv_v0;
+                        if (lane == (ci & 31)) row[ci] = vr[w];
+                    }
+                    const float lf = tq * vr[w];
+#pragma unroll
+                    for (int j = 0; j < SEG; j++) {
+                        const int c = s0 + 32 * j + lane;
+                        if (c > ci && c < N) {
+                            a[w][j] -= lf * sh.wv[c];
+                            dot[w] += a[w][j] * sh.uv[c];
+                            row[c] = a[w][j];
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int w = 0; w < RW; w++) dot[w] = warp_sum(dot[w]) * tp;
+            for (int s0 = cbeg; s0 < N; s0 += 32 * SEG) {
+                float a[RW][SEG];
+#pragma unroll
+                for (int w = 0; w < RW; w++) {
+                    const float *row = W + (long)(base + w) * ldw;
+#pragma unroll
+                    for (int j = 0; j < SEG; j++) {
+                        const int c = s0 + 32 * j + lane;
+                        a[w][j] = (w < nr && c > ci && c < N) ? row[c] : 0.f;
+                    }
+                }
+#pragma unroll
+                for (int w = 0; w < RW; w++) {
+                    if (w >= nr) break;
+                    const int r = base + w;
+                    float *row = W + (long)r * ldw;
+#pragma unroll
+                    for (int j = 0; j < SEG; j++) {
+                        const int c = s0 + 32 * j + lane;
+                        if (c > ci && c < N) {
+                            a[w][j] -= dot[w] * sh.uv[c];
+                            row[c] = a[w][j];
+                        }
+                    }
+                    if (s0 == cbeg) {
+                        const float xs = ((cn >> 5) > q0) ? a[w][1] : a[w][0];
+                        xn[w] = __shfl_sync(0xffffffffu, xs, cn & 31);
+                    }
+                    if (cn < N && r > cn) {
+#pragma unroll
+                        for (int j = 0; j < SEG; j++) {
+                            const int c = s0 + 32 * j + lane;
+                            if (c > cn && c < N) mypart[c] += xn[w] * a[w][j];
+                        }
                     }
                 }
             }
         }
-        if (cn < N && r > cn) ssig += xn * xn;
+#pragma unroll
+        for (int w = 0; w < RW; w++)
+            if (w < nr && cn < N && base + w > cn) ssig += xn[w] * xn[w];
     }
     if (lane == 0) sh.ssig[warp] = ssig;
 }
@@ -765,82 +807,27 @@ static __device__ void bt_apply_back_n(const BtSweepSh &sh, float *Y, long ldy, 
     __syncthreads();
 }
 
-// bt_apply_back_n for rows wider than 16 chunks: one row at a time per warp,
-// the sums for the next reflector accumulated in the warp's row of part.
-template <typename Vec>
-static __device__ void bt_apply_back_wide(const BtSweepSh &sh, float *Y, long ldy, int R, int C, int k1, int sh_off,
-                                          const float *tau, Vec vec)
-{
-    using namespace bt;
-    constexpr int NT = T_SWEEP, NW = W_SWEEP;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    float *mypart = sh.part + warp * sh.maxc;
-    {
-        const int p = k1 + sh_off;
-        for (int c = lane; c < C; c += 32) mypart[c] = 0.f;
-        for (int r = p + warp; r < R; r += NW) {
-            const float vr = (r == p) ? 1.f : vec(k1, r);
-            const float *row = Y + (long)r * ldy;
-            for (int c = lane; c < C; c += 32) mypart[c] += vr * row[c];
-        }
-        __syncthreads();
-        for (int c = tid; c < C; c += NT) {
-            float w = 0.f;
-#pragma unroll
-            for (int x = 0; x < NW; x++) w += sh.part[x * sh.maxc + c];
-            sh.wv[c] = w;
-        }
-        __syncthreads();
-    }
-    for (int k = k1; k >= 0; k--) {
-        const int p = k + sh_off;
-        const float tk = tau[k];
-        const bool nxt = k > 0;
-        for (int c = lane; c < C; c += 32) mypart[c] = 0.f;
-        for (int r = p + warp; r < R; r += NW) {
-            const float vr = (r == p) ? 1.f : vec(k, r);
-            const float vn = nxt ? vec(k - 1, r) : 0.f;
-            const float f = tk * vr;
-            float *row = Y + (long)r * ldy;
-#pragma unroll 4
-            for (int c = lane; c < C; c += 32) {
-                const float v = row[c] - f * sh.wv[c];
-                row[c] = v;
-                mypart[c] += vn * v;
-            }
-        }
-        if (!nxt) break;
-        __syncthreads();
-        for (int c = tid; c < C; c += NT) {
-            float w = Y[(long)(p - 1) * ldy + c];
-#pragma unroll
-            for (int x = 0; x < NW; x++) w += sh.part[x * sh.maxc + c];
-            sh.wv[c] = w;
-        }
-        __syncthreads();
-    }
-    __syncthreads();
-}
-
 template <typename Vec>
 static __device__ void bt_apply_back(const BtSweepSh &sh, float *Y, long ldy, int R, int C, int k1, int sh_off,
                                      const float *tau, Vec vec)
 {
     if (k1 < 0) return;
-    if (C > 512) {
-        bt_apply_back_wide(sh, Y, ldy, R, C, k1, sh_off, tau, vec);
-        return;
-    }
+    // the update of a column depends on that column only: strips of at most
+    // 512 columns each take the whole reflector sequence on their own
+    for (int c0 = 0; c0 < C; c0 += 512) {
+        const int Cs = min(512, C - c0);
+        float *Ys = Y + c0;
 #define BT_APPLY_CASE(K) \
-    case K: bt_apply_back_n<K>(sh, Y, ldy, R, C, k1, sh_off, tau, vec); break;
-    switch ((C + 31) >> 5) {
-        BT_APPLY_CASE(1) BT_APPLY_CASE(2) BT_APPLY_CASE(3) BT_APPLY_CASE(4)
-        BT_APPLY_CASE(5) BT_APPLY_CASE(6) BT_APPLY_CASE(7) BT_APPLY_CASE(8)
-        BT_APPLY_CASE(9) BT_APPLY_CASE(10) BT_APPLY_CASE(11) BT_APPLY_CASE(12)
-        BT_APPLY_CASE(13) BT_APPLY_CASE(14) BT_APPLY_CASE(15) BT_APPLY_CASE(16)
-        default: break;
-    }
+    case K: bt_apply_back_n<K>(sh, Ys, ldy, R, Cs, k1, sh_off, tau, vec); break;
+        switch ((Cs + 31) >> 5) {
+            BT_APPLY_CASE(1) BT_APPLY_CASE(2) BT_APPLY_CASE(3) BT_APPLY_CASE(4)
+            BT_APPLY_CASE(5) BT_APPLY_CASE(6) BT_APPLY_CASE(7) BT_APPLY_CASE(8)
+            BT_APPLY_CASE(9) BT_APPLY_CASE(10) BT_APPLY_CASE(11) BT_APPLY_CASE(12)
+            BT_APPLY_CASE(13) BT_APPLY_CASE(14) BT_APPLY_CASE(15) BT_APPLY_CASE(16)
+            default: break;
+        }
 #undef BT_APPLY_CASE
+    }
 }
 
 // entry r of column reflector k (below the diagonal of W) / row reflector k
@@ -1018,6 +1005,42 @@ extern "C" int paco_debug_batched_times(float out[3])
     return PACO_OK;
 }
 
+// Pinned host staging for the work-queue descriptors: a copy from pageable
+// memory would first wait for the stream's earlier work, which serializes a
+// serving loop that enqueues batch after batch.  A buffer is reused once the
+// event recorded after its copy has completed; the pool grows with the number
+// of calls in flight.
+namespace {
+struct BtStaging {
+    void *p;
+    size_t cap;
+    cudaEvent_t done;
+};
+std::mutex g_bt_staging_mu;
+std::vector<BtStaging> g_bt_staging;
+}  // namespace
+
+static cudaError_t bt_copy_items(void *dst, const void *src, size_t bytes, cudaStream_t s)
+{
+    std::lock_guard<std::mutex> lock(g_bt_staging_mu);
+    BtStaging *slot = nullptr;
+    for (auto &b : g_bt_staging)
+        if (b.cap >= bytes && cudaEventQuery(b.done) == cudaSuccess) { slot = &b; break; }
+    cudaGetLastError();  // a not-ready query is not an error of this call
+    if (!slot) {
+        BtStaging b;
+        b.cap = std::max(bytes, (size_t)1 << 20);
+        if (cudaMallocHost(&b.p, b.cap) != cudaSuccess) return cudaErrorMemoryAllocation;
+        if (cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming) != cudaSuccess) return cudaErrorUnknown;
+        g_bt_staging.push_back(b);
+        slot = &g_bt_staging.back();
+    }
+    memcpy(slot->p, src, bytes);
+    cudaError_t err = cudaMemcpyAsync(dst, slot->p, bytes, cudaMemcpyHostToDevice, s);
+    if (err == cudaSuccess) err = cudaEventRecord(slot->done, s);
+    return err;
+}
+
 size_t paco_batched_workspace_size(int count, const int *M, const int *N)
 {
     BtPlan p;
@@ -1056,8 +1079,7 @@ int paco_svd_batched(int count, const int *M, const int *N, const float *const *
     unsigned long long *prof = (unsigned long long *)(ws + 64);
     const BtItem *dit = (const BtItem *)(ws + p.items_off);
     if (cudaMemsetAsync(ws, 0, 256, s) != cudaSuccess) return PACO_ERR_CUDA;
-    if (cudaMemcpyAsync(ws + p.items_off, items.data(), sizeof(BtItem) * count, cudaMemcpyHostToDevice, s) !=
-        cudaSuccess)
+    if (bt_copy_items(ws + p.items_off, items.data(), sizeof(BtItem) * count, s) != cudaSuccess)
         return PACO_ERR_CUDA;
     char *arena = ws + p.arena_off;
     if (g_bt_timing) cudaEventRecord(g_bt_ev[0], s);

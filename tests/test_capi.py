@@ -123,3 +123,13 @@ def test_batched_entry_validates_before_touching_the_device():
     assert L.paco_svd_batched(1, Ms, Ns, nul, nul, nul, nul, None, None, 0, None) == P.PACO_ERR_UNSUPPORTED
     Ms[0] = 3
     assert L.paco_svd_batched(1, Ms, Ns, nul, nul, nul, nul, None, None, 0, None) == P.PACO_ERR_INVALID_ARG
+
+
+def test_serving_trace_generators():
+    import serve as S
+    arr = S.poisson_arrivals(2000.0, 1.0, 3)
+    assert 1800 < len(arr) < 2200 and np.all(np.diff(arr) > 0) and arr[-1] < 1.0
+    M, N, g = S.serving_shapes(20000, 4)
+    assert M.min() >= 16 and M.max() <= 2048 and np.all(N <= M) and np.all(N >= np.maximum(1, M // 4))
+    assert 0.08 < np.mean(M > 256) < 0.12 and 0.18 < g.mean() < 0.22
+    assert S.footprint(64, 32) > 4 * (64 * 32 + 64 * 64)
