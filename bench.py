@@ -234,6 +234,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end measurement")
     ap.add_argument("--serve-seconds", type=float, default=None, help="length of the serving trace")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default configuration (no paco_autotune)")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
 
@@ -261,6 +262,8 @@ def main():
         run_serving(args, wl, rank, world, local, dist)
         return
     M, N = wl["M"], wl["N"]
+    # the tiling autotuner picks this shape's configuration before the clock starts
+    tune = None if args.no_autotune else P.autotune(M, N)
     A_host, sig_exact = make_matrix(wl, seed=1234 + rank, with_sigma=True)
     A0 = torch.from_numpy(A_host).cuda()
     W = P.Workspace(M, N)
@@ -384,6 +387,8 @@ def main():
                        "M": M, "N": N, "l2": "512 MiB buffer written between timed steps",
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
             "sigma_max": float(s[0]), "sigma_min": float(s[-1]), "accuracy": acc,
+            "autotune": ({"choice": tune["name"], "ms": tune["ms"], "default_ms": tune["default_ms"]}
+                         if tune else None),
             "roofline": roof, "clocks": clk,
             "e2e": ({"value": 1000.0 / e2e_t * world, "unit": "SVDs/s",
                      "h2d_bytes_per_step": 4 * M * N, "d2h_bytes_per_step": 4 * (M * M + N * N + N)}

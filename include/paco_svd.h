@@ -46,6 +46,23 @@ int getTilingSize(int N, int svdBlockNum);
  * Replaces svd_tiling.cpp:83 GenerateTiling(int N, int blockDim, uint8_t*). */
 void GenerateTiling(int N, int blockDim, uint8_t *TilingHost);
 
+/* Tiling autotuner (replaces the fixed host tiling of svd_tiling.cpp:11-66,
+ * SVDTiling / initTCubeTiling, which sets one 1024^3 matmul tile for every
+ * shape).  paco_autotune times the candidate configurations of the
+ * single-matrix path on a synthetic M x N matrix (the persistent panel kernel
+ * or the two-kernel row/column passes, rows per CTA of a panel, the tcgen05
+ * or SIMT engine for the large products), keeps the fastest for (M, N) in a
+ * process-wide table that every later call of that shape uses, and returns
+ * out[0] = chosen candidate, out[1] = its ms per SVD, out[2] = ms of the
+ * defaults, out[3] = candidates tried.  It allocates its own device buffers
+ * and synchronizes `stream`.  cfg[4] = {persistent (0/1), rows per CTA
+ * (4..256), tcgen05 products (0/1), 0}: paco_tune_get returns the entry in
+ * use for (M, N) (the defaults {1, 16, 1, 0} if none), paco_tune_set stores
+ * one (for example a choice saved by an earlier process). */
+int paco_autotune(int M, int N, void *stream, double out[4]);
+int paco_tune_get(int M, int N, int cfg[4]);
+int paco_tune_set(int M, int N, const int cfg[4]);
+
 /* Buffer sizes in bytes of main.cpp:33-43, in this order:
  * [0] U M*M, [1] A M*N, [2] Vt N*N, [3] d N, [4] e N-1, [5] tauq N,
  * [6] taup N-1, [7] qt 2*N*N, [8] wt 2*N*N, [9] tiling, [10] idx 16*N*u32,

@@ -178,6 +178,7 @@ int bdc_run(int M, int N, float *a, float *u, float *vt, float *d, float *e, flo
     BdcWs w;
     bdc_carve(workspace, M, N, &w);
     bdc_init_attrs();
+    if (!paco_tune_for(M, N).tc) w.tcs = nullptr;
     std::vector<HostLevel> lv;
     const int nleaf = host_schedule(N, lv);
     LevelArgs A;

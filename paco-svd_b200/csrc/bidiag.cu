@@ -734,6 +734,8 @@ int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, f
     BdWs w;
     bd_carve(workspace, M, N, &w);
     bd_init_attrs();
+    const PacoTune tune = paco_tune_for(M, N);
+    if (!tune.tc) w.tcs = nullptr;  // the large products stay on the SIMT engine
     prof_begin(s);
     BdArgs a;
     a.M = M; a.N = N; a.ldw = w.ldw; a.st = w.st;
@@ -752,7 +754,8 @@ int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, f
     a.trace_p0 = trace_env;
 
     const int gmax = std::max(1, std::min(RB_CAP, num_sms));
-    auto grid_rows = [&](int rows) { return std::max(1, std::min(gmax, ceil_div(rows, RMIN_PER_BLOCK))); };
+    const int rpc = std::max(1, tune.rows_per_cta);
+    auto grid_rows = [&](int rows) { return std::max(1, std::min(gmax, ceil_div(rows, rpc))); };
     cudaMemsetAsync(w.st->counters, 0, sizeof(w.st->counters), s);
     cudaMemsetAsync(w.ctl, 0, sizeof(PkCtl), s);
     bd_pk_init_attrs();
@@ -762,14 +765,14 @@ int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, f
         const char *v = getenv("PACO_PERSISTENT");
         use_pk_env = !(v && v[0] == '0');
     }
-    const bool use_pk = use_pk_env != 0;
+    const bool use_pk = use_pk_env != 0 && tune.persistent;
     cudaMemsetAsync(w.Yt, 0, sizeof(float) * NB * w.ldw, s);
     cudaMemsetAsync(w.X, 0, sizeof(float) * (size_t)M * NB, s);
     paco_count_launch(), bd_copy_in<<<std::min(4096, ceil_div((long)M * w.ldw, 256)), 256, 0, s>>>(a_in, w.W, M, N, w.ldw, w.st);
 
     for (int p0 = 0; p0 < N; p0 += NB) {
         const int p1 = std::min(N, p0 + NB), nbp = p1 - p0;
-        const int Gp = std::max(1, std::min(gmax, ceil_div(M - p0, 16)));
+        const int Gp = grid_rows(M - p0);
         bool pk = false;
         if (use_pk) {
             cudaEvent_t e0 = nullptr, e1 = nullptr;

@@ -12,7 +12,7 @@ constexpr int RMAX = 8;            // max rows staged per TMA batch
 constexpr int RB_CAP = 256;        // max row-pass CTAs (partial records)
 constexpr int CB_CAP = 512;        // max column-pass CTAs (N/32)
 constexpr int PR = 2 * NB + 8;     // floats per partial record
-constexpr int RMIN_PER_BLOCK = 16; // fewest rows a row-pass CTA is given
+constexpr int RMIN_PER_BLOCK = 16; // rows per CTA of a panel unless the autotuner chose otherwise
 constexpr int SPLITS = 8;          // split-K factor cap for the skinny V^T Q products
 constexpr int PCAP = 512;          // CTA slots of a partial record (>= RB_CAP, CB_CAP)
 constexpr int NBF = 128;           // reflectors per block update when U and V are formed

@@ -52,6 +52,61 @@ static unsigned long long g_launches = 0;
 static int g_prof_on = 0;
 void paco_count_launch() { g_launches++; }
 
+// ------------------------------------------------ tiling autotuner state
+// The reference fixes its tiling on the host (svd_tiling.cpp:11-66: one
+// 1024^3 matmul tile and the leaf partition).  Here the shape-dependent
+// choices of the single-matrix path are measured per (M, N) by
+// paco_autotune and kept in a process-wide table; every later call of that
+// shape reads its entry (other shapes use the defaults).  A change bumps a
+// generation number so recorded CUDA graphs of older choices are re-recorded.
+namespace {
+struct TuneEntry {
+    int M, N;
+    PacoTune cfg;
+};
+std::mutex g_tune_mu;
+std::vector<TuneEntry> g_tune;
+unsigned g_tune_gen = 0;
+const PacoTune kTuneDefault = {1, bd::RMIN_PER_BLOCK, 1, 0};
+
+bool tune_valid(const PacoTune &t)
+{
+    return (t.persistent == 0 || t.persistent == 1) && (t.tc == 0 || t.tc == 1) && t.rows_per_cta >= 4 &&
+           t.rows_per_cta <= 256;
+}
+
+void tune_store(int M, int N, const PacoTune &cfg)
+{
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    for (TuneEntry &e : g_tune)
+        if (e.M == M && e.N == N) {
+            e.cfg = cfg;
+            g_tune_gen++;
+            return;
+        }
+    g_tune.push_back({M, N, cfg});
+    g_tune_gen++;
+}
+}  // namespace
+
+PacoTune paco_tune_for(int M, int N)
+{
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    for (const TuneEntry &e : g_tune)
+        if (e.M == M && e.N == N) return e.cfg;
+    return kTuneDefault;
+}
+
+// fills A with reproducible values uniform on [-1, 1) (a hash of the index)
+__global__ void tune_fill(float *A, long n, unsigned seed)
+{
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+        unsigned x = (unsigned)t * 2654435761u ^ seed;
+        x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
+        A[t] = (float)(x >> 8) * (2.f / 16777216.f) - 1.f;
+    }
+}
+
 __global__ void dev_status_begin(DevStatus *st, int stage)
 {
     const int t = threadIdx.x;
@@ -247,6 +302,7 @@ static int svd_direct(int M, int N, float *A, float *U, float *Vt, float *sigma,
 namespace {
 struct GraphEntry {
     int M, N, prof;
+    unsigned tune_gen;  // autotuner generation the graph was recorded under
     void *A, *U, *Vt, *sigma, *ws;
     cudaStream_t s;
     cudaGraphExec_t exec;
@@ -279,7 +335,7 @@ int paco_svd(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws
         return svd_direct(M, N, A, U, Vt, sigma, b, L, stream);
     for (GraphEntry &g : g_graphs) {
         if (g.M == M && g.N == N && g.A == A && g.U == U && g.Vt == Vt && g.sigma == sigma && g.ws == ws &&
-            g.s == s && g.prof == g_prof_on) {
+            g.s == s && g.prof == g_prof_on && g.tune_gen == g_tune_gen) {
             if (cudaGraphLaunch(g.exec, s) != cudaSuccess) return PACO_ERR_CUDA;
             bd_profile_replayed(g.prof_run);
             g_launches += g.kernels;
@@ -305,6 +361,7 @@ int paco_svd(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws
     }
     GraphEntry g;
     g.M = M; g.N = N; g.prof = g_prof_on; g.A = A; g.U = U; g.Vt = Vt; g.sigma = sigma; g.ws = ws; g.s = s;
+    g.tune_gen = g_tune_gen;
     g.prof_run = g_prof_on ? bd_profile_last_graph_run() : -1;
     g.kernels = kernels;
     err = cudaGraphInstantiate(&g.exec, graph, 0);
@@ -322,6 +379,80 @@ int paco_svd(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws
     bd_profile_replayed(g.prof_run);
     g_launches += g.kernels;
     return PACO_OK;
+}
+
+// ------------------------------------------------ tiling autotuner
+
+int paco_tune_get(int M, int N, int cfg[4])
+{
+    if (!cfg) return PACO_ERR_INVALID_ARG;
+    const PacoTune t = paco_tune_for(M, N);
+    cfg[0] = t.persistent; cfg[1] = t.rows_per_cta; cfg[2] = t.tc; cfg[3] = 0;
+    return PACO_OK;
+}
+
+int paco_tune_set(int M, int N, const int cfg[4])
+{
+    if (!cfg || !shape_ok(M, N)) return PACO_ERR_INVALID_ARG;
+    const PacoTune t = {cfg[0], cfg[1], cfg[2], 0};
+    if (!tune_valid(t)) return PACO_ERR_INVALID_ARG;
+    tune_store(M, N, t);
+    return PACO_OK;
+}
+
+int paco_autotune(int M, int N, void *stream, double out[4])
+{
+    if (!shape_ok(M, N)) return (N >= 1 && M >= N) ? PACO_ERR_UNSUPPORTED : PACO_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const SvdLayout L = svd_layout(M, N);
+    float *A0 = nullptr, *A = nullptr, *U = nullptr, *Vt = nullptr, *sg = nullptr;
+    char *ws = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t err = cudaSuccess;
+    err = err ? err : cudaMalloc(&A0, sizeof(float) * (size_t)M * N);
+    err = err ? err : cudaMalloc(&A, sizeof(float) * (size_t)M * N);
+    err = err ? err : cudaMalloc(&U, sizeof(float) * (size_t)M * M);
+    err = err ? err : cudaMalloc(&Vt, sizeof(float) * (size_t)N * N);
+    err = err ? err : cudaMalloc(&sg, sizeof(float) * N);
+    err = err ? err : cudaMalloc(&ws, L.total);
+    err = err ? err : cudaEventCreate(&e0);
+    err = err ? err : cudaEventCreate(&e1);
+    int rc = err ? PACO_ERR_CUDA : PACO_OK;
+    // candidates: the defaults first, then fewer / more rows per CTA, the
+    // SIMT engine for the large products, the two-kernel row/column passes
+    const PacoTune cands[] = {{1, bd::RMIN_PER_BLOCK, 1, 0}, {1, 8, 1, 0}, {1, 32, 1, 0}, {1, bd::RMIN_PER_BLOCK, 0, 0},
+                              {0, bd::RMIN_PER_BLOCK, 1, 0}};
+    const int nc = (int)(sizeof(cands) / sizeof(cands[0]));
+    float best = 1e30f, tdef = 0.f;
+    int bi = 0;
+    if (!rc) {
+        paco_count_launch(), tune_fill<<<std::min(4096, ceil_div((long)M * N, 256)), 256, 0, s>>>(A0, (long)M * N,
+                                                                                                   12345u);
+        for (int k = 0; k < nc && !rc; k++) {
+            tune_store(M, N, cands[k]);
+            float tk = 1e30f;
+            for (int rep = 0; rep < 3; rep++) {
+                cudaMemcpyAsync(A, A0, sizeof(float) * (size_t)M * N, cudaMemcpyDeviceToDevice, s);
+                cudaEventRecord(e0, s);
+                int r = svd_direct(M, N, A, U, Vt, sg, ws, L, stream);
+                cudaEventRecord(e1, s);
+                if (r || cudaEventSynchronize(e1) != cudaSuccess) { rc = r ? r : PACO_ERR_CUDA; break; }
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (rep > 0) tk = std::min(tk, ms);  // the first run warms up
+            }
+            int info = 0;
+            if (!rc && paco_sync_status(ws + L.ws, stream, &info) != PACO_OK) tk = 1e30f;  // not a usable choice
+            if (k == 0) tdef = tk;
+            if (tk < best) { best = tk; bi = k; }
+        }
+        tune_store(M, N, cands[bi]);
+    }
+    if (out) { out[0] = bi; out[1] = best; out[2] = tdef; out[3] = nc; }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(A0); cudaFree(A); cudaFree(U); cudaFree(Vt); cudaFree(sg); cudaFree(ws);
+    return rc;
 }
 
 // ------------------------------------------------ allocation-free entry point

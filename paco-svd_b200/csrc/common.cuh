@@ -73,5 +73,15 @@ __device__ __forceinline__ bool last_block_ticket(int *counter, int nblocks, int
 // Host-side count of kernel launches issued by the library (paco_launch_count).
 void paco_count_launch();
 
+// Shape-dependent choices of the single-matrix path (the tiling autotuner's
+// output, paco_autotune): the persistent panel kernel or the two-kernel row /
+// column passes, rows per CTA of a panel (sets the grid: fewer CTAs meet at
+// each barrier, more CTAs stream more bandwidth), and whether the large
+// products use the tcgen05 GEMM.
+struct PacoTune {
+    int persistent, rows_per_cta, tc, pad;
+};
+PacoTune paco_tune_for(int M, int N);
+
 static inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
 static inline long round_up(long a, long b) { return (a + b - 1) / b * b; }

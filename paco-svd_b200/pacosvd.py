@@ -76,6 +76,9 @@ def lib():
         L.paco_ctx_destroy.argtypes = [vp]; L.paco_ctx_destroy.restype = None
         L.paco_version.argtypes = []; L.paco_version.restype = ctypes.c_char_p
         ip = ctypes.POINTER(ctypes.c_int)
+        L.paco_autotune.argtypes = [i, i, vp, ctypes.POINTER(ctypes.c_double)]; L.paco_autotune.restype = i
+        L.paco_tune_get.argtypes = [i, i, ip]; L.paco_tune_get.restype = i
+        L.paco_tune_set.argtypes = [i, i, ip]; L.paco_tune_set.restype = i
         L.paco_batched_workspace_size.argtypes = [i, ip, ip]
         L.paco_batched_workspace_size.restype = ctypes.c_size_t
         L.paco_svd_batched.argtypes = [i, ip, ip, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
@@ -229,6 +232,32 @@ def svd(A, check=True):
         rc, info = sync_status(w.ws)
         _check(rc, f"paco_svd (device, info={info})")
     return s.clone(), U.clone(), Vt.clone()
+
+
+TUNE_CANDIDATES = ["persistent, 16 rows/CTA, tcgen05", "persistent, 8 rows/CTA, tcgen05",
+                   "persistent, 32 rows/CTA, tcgen05", "persistent, 16 rows/CTA, SIMT products",
+                   "row/column passes, 16 rows/CTA, tcgen05"]
+
+
+def autotune(M: int, N: int, stream=None) -> dict:
+    """Times the single-matrix configurations for (M, N) and keeps the fastest
+    for later calls of that shape (svd_tiling.cpp's fixed tiling, measured)."""
+    out = (ctypes.c_double * 4)()
+    _check(lib().paco_autotune(M, N, _stream(stream), out), "paco_autotune")
+    k = int(out[0])
+    return {"choice": k, "name": TUNE_CANDIDATES[k] if k < len(TUNE_CANDIDATES) else str(k),
+            "ms": out[1], "default_ms": out[2], "candidates": int(out[3]), "config": tune_get(M, N)}
+
+
+def tune_get(M: int, N: int):
+    cfg = (ctypes.c_int * 4)()
+    _check(lib().paco_tune_get(M, N, cfg), "paco_tune_get")
+    return list(cfg)
+
+
+def tune_set(M: int, N: int, cfg) -> None:
+    c = (ctypes.c_int * 4)(*[int(x) for x in cfg])
+    _check(lib().paco_tune_set(M, N, c), "paco_tune_set")
 
 
 PACO_BATCH_MAX_M = 2048

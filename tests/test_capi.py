@@ -133,3 +133,15 @@ def test_serving_trace_generators():
     assert M.min() >= 16 and M.max() <= 2048 and np.all(N <= M) and np.all(N >= np.maximum(1, M // 4))
     assert 0.08 < np.mean(M > 256) < 0.12 and 0.18 < g.mean() < 0.22
     assert S.footprint(64, 32) > 4 * (64 * 32 + 64 * 64)
+
+
+def test_tune_table_defaults_and_round_trip():
+    assert P.tune_get(300, 200) == [1, 16, 1, 0]
+    P.tune_set(301, 201, [1, 32, 0, 0])
+    assert P.tune_get(301, 201) == [1, 32, 0, 0]
+    assert P.tune_get(300, 200) == [1, 16, 1, 0]     # other shapes keep the defaults
+    for bad in ([2, 16, 1, 0], [1, 2, 1, 0], [1, 16, 3, 0], [1, 1000, 1, 0]):
+        with pytest.raises(P.PacoError):
+            P.tune_set(301, 201, bad)
+    with pytest.raises(P.PacoError):
+        P.tune_set(4, 8, [1, 16, 1, 0])               # M < N
