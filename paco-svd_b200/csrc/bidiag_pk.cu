@@ -103,17 +103,24 @@ __device__ __forceinline__ void reduce_records_fast(const float *rec, int G, int
 
 }  // namespace
 
-template <int CPT>
+// Rows a row-pass batch takes (one warp per row): resident rows go 16 at a
+// time, streamed rows at most RMAX per TMA stage.
+constexpr int PK_RMAX = RP_THREADS / 32;
+// Owned rows whose X entries a CTA keeps in shared memory (else: global).
+constexpr int PK_XOWN = 64;
+
+// RB: rows per row-pass batch the unrolled loops cover (R <= RB).
+template <int CPT, int RB>
 __global__ void __launch_bounds__(RP_THREADS, 1)
     bd_panel_pk(BdArgs a, PkCtl *ctl, int p0, int p1, int resident, int R, unsigned cnt_base)
 {
     extern __shared__ __align__(128) float tiles[];
     __shared__ __align__(8) uint64_t bars[2];
-    __shared__ float red[RP_THREADS / 32][RMAX];
-    __shared__ float xs[RMAX];
+    __shared__ float red[RP_THREADS / 32][PK_RMAX];
+    __shared__ float xs[PK_RMAX];
     __shared__ float s_t3[NB + 1], s_t4[NB], s_ycol[NB], s_wcol[NB]; // row reflector of step i-1
     __shared__ float s_t1[NB], s_t2[NB], s_ai[NB], s_xi[NB];         // column reflector of step i
-    __shared__ float s_part[RMAX][PR];
+    __shared__ float s_part[PK_RMAX][PR];
     __shared__ float s_red[PR], s_bc[PR];
     __shared__ float cy[RP_THREADS / 32][32], cA[RP_THREADS / 32][32], cB[RP_THREADS / 32][32];
     __shared__ float s_cpart[PR];
@@ -129,6 +136,10 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
     const int nown = (M - p0 - b + G - 1) / G > 0 ? (M - p0 - b + G - 1) / G : 0;
     auto own_row = [&](int k) { return p0 + b + k * G; };
     unsigned nbar = 0;
+    // X entries of this CTA's rows (it computes them itself) after the row
+    // tiles, when at most PK_XOWN rows are owned
+    const int own_max = (M - p0 + G - 1) / G;
+    float *xsm = (own_max <= PK_XOWN) ? tiles + (resident ? (long)own_max * L : 2L * R * L) : nullptr;
 
     if (tid == 0) {
         mbar_init(&bars[0], 1);
@@ -224,7 +235,7 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
         }
 #pragma unroll
         for (int k = 0; k < CPT; k++) acc4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int t = tid; t < RMAX * PR; t += RP_THREADS) (&s_part[0][0])[t] = 0.f;
+        for (int t = tid; t < PK_RMAX * PR; t += RP_THREADS) (&s_part[0][0])[t] = 0.f;
         const float taup_prev = doX ? s_rtaup : 0.f;
         const float invc = (ii >= 1) ? s_cinv_prev : 1.f;
 
@@ -257,8 +268,9 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
             const int stage = bb & 1;
             // X entries of the staged rows, loaded before the dot products so
             // their latency overlaps them
-            const float xq_pre =
-                (warp < nr && doX && lane < iip) ? a.X[(long)own_row(k0 + warp) * NB + lane] : 0.f;
+            const float xq_pre = (warp < nr && doX && lane < iip)
+                                     ? (xsm ? xsm[(k0 + warp) * NB + lane] : a.X[(long)own_row(k0 + warp) * NB + lane])
+                                     : 0.f;
             if (resident) {
                 T = tiles + (long)k0 * L;
             } else {
@@ -268,11 +280,11 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
                 T = tiles + (long)stage * R * L;
             }
             if (doX) {
-                float pd[RMAX];
+                float pd[RB];
 #pragma unroll
-                for (int rr = 0; rr < RMAX; rr++) pd[rr] = 0.f;
+                for (int rr = 0; rr < RB; rr++) pd[rr] = 0.f;
 #pragma unroll
-                for (int rr = 0; rr < RMAX; rr++) {
+                for (int rr = 0; rr < RB; rr++) {
                     if (rr < nr) {
 #pragma unroll
                         for (int k = 0; k < CPT; k++) {
@@ -285,7 +297,7 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
                     }
                 }
 #pragma unroll
-                for (int rr = 0; rr < RMAX; rr++) {
+                for (int rr = 0; rr < RB; rr++) {
                     if (rr < nr) {
                         float v = warp_sum(pd[rr]);
                         if (lane == 0) red[warp][rr] = v;
@@ -310,7 +322,10 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
                     for (int w2 = 0; w2 < RP_THREADS / 32; w2++) dot += red[w2][rr];
                     float sx = ((lane <= iip) ? aq * s_t3[lane] : 0.f) + ((lane < iip) ? xq * s_t4[lane] : 0.f);
                     Xn = taup_prev * (dot - warp_sum(sx));
-                    if (lane == 0) a.X[(long)r * NB + iip] = Xn;
+                    if (lane == 0) {
+                        a.X[(long)r * NB + iip] = Xn;
+                        if (xsm) xsm[(k0 + rr) * NB + iip] = Xn;
+                    }
                 }
                 if (doCol) {
                     float xrq = (lane < ii - 1) ? xq : ((lane == ii - 1) ? Xn : 0.f);
@@ -338,7 +353,7 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
             __syncthreads();
             if (doCol) {
 #pragma unroll
-                for (int rr = 0; rr < RMAX; rr++) {
+                for (int rr = 0; rr < RB; rr++) {
                     if (rr < nr && own_row(k0 + rr) > i) {
                         float xr = xs[rr];
 #pragma unroll
@@ -369,7 +384,7 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
             int c4 = tid + k * RP_THREADS;
             if (4 * c4 < L) *reinterpret_cast<float4 *>(a.ypart + (long)b * ldw + p0 + 4 * c4) = acc4[k];
         }
-        if (warp < RMAX) {
+        if (warp < PK_RMAX) {
             if (lane == 0) s_part[warp][0] = w_ss;
             if (lane < ii) {
                 s_part[warp][1 + lane] = w_g1;
@@ -379,7 +394,7 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
         __syncthreads();
         for (int t = tid; t < PR; t += RP_THREADS) {
             float v = 0.f;
-            for (int w = 0; w < RMAX; w++) v += s_part[w][t];
+            for (int w = 0; w < PK_RMAX; w++) v += s_part[w][t];
             a.tpart[(long)t * PCAP + b] = v;
         }
         // operands of this CTA's first column-pass chunk do not depend on the
@@ -539,12 +554,14 @@ bool bd_panel_pk_launch(const BdArgs &a, PkCtl *ctl, int p0, int p1, int G, unsi
     int resident = ((long)own * L * 4 <= budget) ? 1 : 0;
     int R = std::max(1, std::min(RMAX, (int)(budget / (2L * L * 4))));
     size_t smem = resident ? (size_t)own * L * 4 : (size_t)2 * R * L * 4;
-    if (resident) R = RMAX;
+    if (resident) R = PK_RMAX;
+    if (own <= PK_XOWN) smem += (size_t)own * NB * 4;  // X entries of the owned rows
     const int chunks = ceil_div(L, 4 * RP_THREADS);
     void *fn;
-    if (chunks <= 1) fn = (void *)bd_panel_pk<1>;
-    else if (chunks == 2) fn = (void *)bd_panel_pk<2>;
-    else fn = (void *)bd_panel_pk<4>;
+    if (resident) fn = chunks <= 1 ? (void *)bd_panel_pk<1, PK_RMAX> : chunks == 2 ? (void *)bd_panel_pk<2, PK_RMAX>
+                                                                                 : (void *)bd_panel_pk<4, PK_RMAX>;
+    else fn = chunks <= 1 ? (void *)bd_panel_pk<1, RMAX> : chunks == 2 ? (void *)bd_panel_pk<2, RMAX>
+                                                                       : (void *)bd_panel_pk<4, RMAX>;
     BdArgs aa = a;
     unsigned base = *cnt;
     void *args[] = {&aa, &ctl, &p0, &p1, &resident, &R, &base};
@@ -561,9 +578,12 @@ void bd_pk_init_attrs()
 {
     static bool done = false;
     if (done) return;
-    int maxs = 200 * 1024 + 1024;
-    cudaFuncSetAttribute(bd_panel_pk<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
-    cudaFuncSetAttribute(bd_panel_pk<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
-    cudaFuncSetAttribute(bd_panel_pk<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
+    int maxs = 200 * 1024 + PK_XOWN * NB * 4 + 1024;
+    cudaFuncSetAttribute(bd_panel_pk<1, PK_RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
+    cudaFuncSetAttribute(bd_panel_pk<2, PK_RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
+    cudaFuncSetAttribute(bd_panel_pk<4, PK_RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
+    cudaFuncSetAttribute(bd_panel_pk<1, RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
+    cudaFuncSetAttribute(bd_panel_pk<2, RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
+    cudaFuncSetAttribute(bd_panel_pk<4, RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
     done = true;
 }
