@@ -29,6 +29,9 @@
 
 #include "bdc_dev.cuh"
 
+// merges at least this large take their back-transform on the tensor cores
+#define BDC_TC_MIN_N 256
+
 // --------------------------------------------------------------- kernels
 
 __global__ void bdc_schedule(int N, const uint8_t *tiling, BdcWs w)
@@ -36,8 +39,13 @@ __global__ void bdc_schedule(int N, const uint8_t *tiling, BdcWs w)
     if (threadIdx.x == 0 && blockIdx.x == 0) bdc_schedule_dev(N, tiling, w, nullptr, nullptr);
 }
 
+struct HostMerge {
+    int s, n, nc;
+};
+
 struct HostLevel {
     int off, nm, max_n, max_nc;
+    std::vector<HostMerge> merges;
 };
 
 static int host_schedule(int N, std::vector<HostLevel> &lv)
@@ -47,13 +55,14 @@ static int host_schedule(int N, std::vector<HostLevel> &lv)
     leaf_partition(N, s.data(), e.data());
     int cnt = nleaf, out = 0;
     while (cnt > 1) {
-        HostLevel L{out, 0, 0, 0};
+        HostLevel L{out, 0, 0, 0, {}};
         int wpos = 0, r = 0;
         while (r < cnt - 1) {
             int ms = s[r], me = e[r + 1];
             int sq = (me == N);
             int n = me - ms - 1 + sq, nc = me - ms;
             L.nm++; L.max_n = std::max(L.max_n, n); L.max_nc = std::max(L.max_nc, nc);
+            L.merges.push_back({ms, n, nc});
             out++;
             s[wpos] = ms; e[wpos] = me; wpos++;
             r += 2;
@@ -111,8 +120,10 @@ __global__ void __launch_bounds__(256) bdc_vectors(LevelArgs A, int nm)
     bdc_vectors_dev<32>(A, nm, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, threadIdx.x & 31, 0, 0x7fffffff);
 }
 
-__global__ void __launch_bounds__(256) bdc_btgemm(LevelArgs A, int tiles_n)
+// merges with n >= skip_n are multiplied on the tensor cores instead
+__global__ void __launch_bounds__(256) bdc_btgemm(LevelArgs A, int tiles_n, int skip_n)
 {
+    if (A.w.meta[A.w.mg_s[A.off + blockIdx.z]].n >= skip_n) return;
     bdc_btgemm_dev(A, blockIdx.z, blockIdx.y, blockIdx.x / tiles_n, blockIdx.x % tiles_n);
 }
 
@@ -206,7 +217,28 @@ int bdc_run(int M, int N, float *a, float *u, float *vt, float *d, float *e, flo
         paco_count_launch(), bdc_vectors<<<ceil_div((long)N * 32, 256), 256, 0, s>>>(A, L.nm);
         paco_count_launch(), bdc_copyback<<<g2, 128, 0, s>>>(A);
         int tiles_n = ceil_div(L.max_nc, 128);
-        paco_count_launch(), bdc_btgemm<<<dim3(tiles_n * ceil_div(L.max_n, 128), 2, L.nm), 256, 0, s>>>(A, tiles_n);
+        // back-transforms of large merges on the tensor cores, limited on the
+        // device to the merge's k (rows beyond k hold deflated vectors)
+        int skip_n = 0x7fffffff;
+        if (w.tcs && L.max_n >= BDC_TC_MIN_N) {
+            bool fits = true;
+            for (const HostMerge &g : L.merges)
+                if (g.n >= BDC_TC_MIN_N && gemm_tc_scratch_floats(g.n, g.nc, g.n) > w.tcs_floats) fits = false;
+            if (fits) skip_n = BDC_TC_MIN_N;
+        }
+        paco_count_launch(), bdc_btgemm<<<dim3(tiles_n * ceil_div(L.max_n, 128), 2, L.nm), 256, 0, s>>>(A, tiles_n,
+                                                                                                      skip_n);
+        if (skip_n != 0x7fffffff) {
+            for (const HostMerge &g : L.merges) {
+                if (g.n < skip_n) continue;
+                const long off = (long)g.s * N + g.s;
+                const int *kd = &w.meta[g.s].k;
+                gemm_tc_run(g.n, g.n, g.n, 1.f, gop(w.Us + off, N, 1), gop(A.ST + off, N, 1), 0.f, A.QT + off, N,
+                            w.tcs, w.st, s, kd);
+                gemm_tc_run(g.n, g.nc, g.n, 1.f, gop(w.Vs + off, N, 1), gop(A.GT + off, N, 1), 0.f, A.WT + off, N,
+                            w.tcs, w.st, s, kd);
+            }
+        }
         paco_count_launch(), bdc_finalize<<<L.nm, 256, 0, s>>>(A);
     }
     paco_count_launch(), bdc_sort_desc<<<ceil_div(N, 256), 256, 0, s>>>(N, d, w.perm, w.sig);

@@ -111,13 +111,19 @@ TcGeom tc_geom(int M, int N, int K)
 // Operand X with R rows and K columns, element (r, k) = opA(r, k) (or opB(k, r)
 // when `transposed`); writes hi and lo images, image (rt, kt) at
 // (rt * KT + kt) * IMG floats.  One CTA of 256 threads per image.
+// With lim, k >= *lim (and, for A, rows >= *lim) read as 0.
 __global__ void __launch_bounds__(256) tc_pack(GemmOp X, int transposed, int R, int K, int KT, float *hi,
-                                               float *lo)
+                                               float *lo, const int *lim)
 {
     __shared__ float tile[TM][TK + 1];
     const int img = blockIdx.x;
     const int rt = img / KT, kt = img % KT;
     const int t = threadIdx.x;
+    if (lim) {
+        const int l = *lim;
+        K = min(K, l);
+        if (!transposed) R = min(R, l);
+    }
     const bool kfast = transposed ? (X.rs == 1) : (X.cs == 1);
 #pragma unroll 4
     for (int i = 0; i < 16; i++) {
@@ -151,8 +157,9 @@ __global__ void __launch_bounds__(256) tc_pack(GemmOp X, int transposed, int R, 
 
 __global__ void __launch_bounds__(128, 1)
     tc_gemm(int M, int N, int KT, int kper, float alpha, const float *Ahi, const float *Alo, const float *Bhi,
-            const float *Blo, float beta, float *C, long ldc, float *part, int ctma, DevStatus *st)
+            const float *Blo, float beta, float *C, long ldc, float *part, int ctma, const int *lim, DevStatus *st)
 {
+    if (lim) M = min(M, *lim);  // rows at or beyond the limit are left as they are
     extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
     __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done, cbar;
     __shared__ uint32_t s_tmem;
@@ -177,7 +184,7 @@ __global__ void __launch_bounds__(128, 1)
         al = 1.f;
         be = 0.f;
     }
-    const bool cload = ctma && be != 0.f;
+    const bool cload = ctma && be != 0.f && nrows > 0;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
@@ -352,24 +359,28 @@ void gemm_tc_init_attrs()
 }
 
 cudaError_t gemm_tc_run(int M, int N, int K, float alpha, GemmOp A, GemmOp B, float beta, float *C, long ldc,
-                        float *scratch, DevStatus *st, cudaStream_t s)
+                        float *scratch, DevStatus *st, cudaStream_t s, const int *lim)
 {
     if (M <= 0 || N <= 0) return cudaSuccess;
     K = std::max(K, 1);
-    const TcGeom g = tc_geom(M, N, K);
+    TcGeom g = tc_geom(M, N, K);
+    if (lim) g.splits = 1;
     float *Ahi = scratch, *Alo = Ahi + (size_t)g.MT * g.KT * IMG;
     float *Bhi = Alo + (size_t)g.MT * g.KT * IMG, *Blo = Bhi + (size_t)g.NT * g.KT * IMG;
     float *part = g.splits > 1 ? Blo + (size_t)g.NT * g.KT * IMG : nullptr;
     const int kper = ceil_div(g.KT, g.splits);
-    paco_count_launch(), tc_pack<<<g.MT * g.KT, 256, 0, s>>>(A, 0, M, K, g.KT, Ahi, Alo);
-    paco_count_launch(), tc_pack<<<g.NT * g.KT, 256, 0, s>>>(B, 1, N, K, g.KT, Bhi, Blo);
+    paco_count_launch(), tc_pack<<<g.MT * g.KT, 256, 0, s>>>(A, 0, M, K, g.KT, Ahi, Alo, lim);
+    paco_count_launch(), tc_pack<<<g.NT * g.KT, 256, 0, s>>>(B, 1, N, K, g.KT, Bhi, Blo, lim);
     // bulk-copy epilogue when every row segment of the destination is 16-byte aligned
     const float *dst = part ? part : C;
     const long dld = part ? (long)N : ldc;
     const int ctma = ((((uintptr_t)dst) & 15) == 0 && (dld % 4) == 0 && (N % 4) == 0) ? 1 : 0;
     paco_count_launch(), tc_gemm<<<dim3(g.NT, g.MT, g.splits), 128, tc_smem_bytes(), s>>>(
-                             M, N, g.KT, kper, alpha, Ahi, Alo, Bhi, Blo, beta, C, ldc, part, ctma, st);
-    if (part) return gemm_splitk_reduce_run(M, N, g.splits, alpha, part, beta, C, ldc, s);
+                             M, N, g.KT, kper, alpha, Ahi, Alo, Bhi, Blo, beta, C, ldc, part, ctma, lim, st);
+    if (part) {
+        if (lim) return cudaErrorInvalidValue;  // a limited product is never split (see gemm_tc_scratch_floats)
+        return gemm_splitk_reduce_run(M, N, g.splits, alpha, part, beta, C, ldc, s);
+    }
     return cudaGetLastError();
 }
 

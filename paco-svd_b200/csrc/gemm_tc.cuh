@@ -20,8 +20,11 @@ void gemm_tc_init_attrs();
 // C = alpha * opA * opB + beta * C on the tensor cores; scratch holds
 // gemm_tc_scratch_floats(M, N, K) floats.  A bounded wait that gives up
 // records PACO_ERR_TIMEOUT in st.
+// With lim (a device int), the product is limited to M' = min(M, *lim) rows
+// and K' = min(K, *lim): opA rows and k beyond it read as 0 and C's rows
+// beyond it are left as they are.  A limited product must not be split-K.
 cudaError_t gemm_tc_run(int M, int N, int K, float alpha, GemmOp A, GemmOp B, float beta, float *C, long ldc,
-                        float *scratch, DevStatus *st, cudaStream_t s);
+                        float *scratch, DevStatus *st, cudaStream_t s, const int *lim = nullptr);
 
 // Tensor-core product when it is enabled, tc_scratch holds enough floats and
 // the product is large enough to pay for the operand packing; otherwise the
