@@ -18,10 +18,9 @@
 //      merges, per warp for large ones), back-transform products through
 //      64x64 shared-memory tiles.
 //   3. bt_apply_k (512 threads per matrix)  U = H_0 ... H_{N-1} blockdiag(Q, I)
-//      and V = G_0 ... G_{N-2} W applied backward to the divide-and-conquer
-//      vectors with one fused sweep per reflector (apply H_i, accumulate the w
-//      of H_{i-1}); this replaces the formation of U, V and the two final
-//      products of svd.cpp:1911-1981.
+//      and V = G_0 ... G_{N-2} W applied to the divide-and-conquer vectors in
+//      compact-WY blocks of 32 reflectors, last block first; this replaces
+//      the formation of U, V and the two final products of svd.cpp:1911-1981.
 // Each matrix keeps its Householder vectors, d/e/tau and Q^T/W^T in its own
 // area of the workspace between the launches; the divide-and-conquer and
 // back-transform scratch lives in one slot per CTA.
@@ -709,154 +708,201 @@ __global__ void __launch_bounds__(bt::T_BDC, 2) bt_bdc_k(const BtItem *items, in
 
 // ---------------------------------------------------------------- kernel 3
 
-// Backward application of reflectors k = k1, k1-1, ..., 0 to the rows of Y
-// (R rows, C <= 32 NA columns, ld ldy): reflector k acts on rows >= k + sh_off
-// with v_{k+sh_off} = 1 and v_r = vec(k, r) for r > k + sh_off.  Each sweep
-// applies reflector k and accumulates the w of reflector k-1.
-template <int NA, typename Vec>
-static __device__ void bt_apply_back_n(const BtSweepSh &sh, float *Y, long ldy, int R, int C, int k1, int sh_off,
-                                       const float *tau, Vec vec)
-{
-    using namespace bt;
-    constexpr int RBn = BtRows<NA>::RB;
-    constexpr int NT = T_SWEEP, NW = W_SWEEP;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    // w of reflector k1
-    {
-        const int p = k1 + sh_off;
-        float acc[NA];
-#pragma unroll
-        for (int j = 0; j < NA; j++) acc[j] = 0.f;
-        for (int r = p + warp; r < R; r += NW) {
-            const float vr = (r == p) ? 1.f : vec(k1, r);
-            const float *row = Y + (long)r * ldy;
-#pragma unroll
-            for (int j = 0; j < NA; j++) {
-                const int c = lane + 32 * j;
-                if (c < C) acc[j] += vr * row[c];
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < NA; j++) {
-            const int c = lane + 32 * j;
-            if (c < C) sh.part[warp * sh.maxc + c] = acc[j];
-        }
-        __syncthreads();
-        for (int c = tid; c < C; c += NT) {
-            float w = 0.f;
-#pragma unroll
-            for (int x = 0; x < NW; x++) w += sh.part[x * sh.maxc + c];
-            sh.wv[c] = w;
-        }
-        __syncthreads();
-    }
-    for (int k = k1; k >= 0; k--) {
-        const int p = k + sh_off;
-        const float tk = tau[k];
-        const bool nxt = k > 0;
-        float acc[NA];
-#pragma unroll
-        for (int j = 0; j < NA; j++) acc[j] = 0.f;
-        for (int base = p; base < R; base += NW * RBn) {
-            float y[RBn][NA];
-#pragma unroll
-            for (int rb = 0; rb < RBn; rb++) {
-                const int r = base + rb * NW + warp;
-                const float *row = Y + (long)r * ldy;
-#pragma unroll
-                for (int j = 0; j < NA; j++) {
-                    const int c = lane + 32 * j;
-                    y[rb][j] = (r < R && c < C) ? row[c] : 0.f;
-                }
-            }
-#pragma unroll
-            for (int rb = 0; rb < RBn; rb++) {
-                const int r = base + rb * NW + warp;
-                if (r >= R) break;
-                const float vr = (r == p) ? 1.f : vec(k, r);
-                const float vn = nxt ? vec(k - 1, r) : 0.f;  // r > p - 1: entry of reflector k-1
-                const float f = tk * vr;
-                float *row = Y + (long)r * ldy;
-#pragma unroll
-                for (int j = 0; j < NA; j++) {
-                    const int c = lane + 32 * j;
-                    if (c < C) {
-                        const float v = y[rb][j] - f * sh.wv[c];
-                        row[c] = v;
-                        acc[j] += vn * v;
-                    }
-                }
-            }
-        }
-        if (!nxt) break;
-#pragma unroll
-        for (int j = 0; j < NA; j++) {
-            const int c = lane + 32 * j;
-            if (c < C) sh.part[warp * sh.maxc + c] = acc[j];
-        }
-        __syncthreads();
-        // row p - 1 is untouched by reflector k: w' = Y[p-1] + sum of the partials
-        for (int c = tid; c < C; c += NT) {
-            float w = Y[(long)(p - 1) * ldy + c];
-#pragma unroll
-            for (int x = 0; x < NW; x++) w += sh.part[x * sh.maxc + c];
-            sh.wv[c] = w;
-        }
-        __syncthreads();
-    }
-    __syncthreads();
-}
-
-template <typename Vec>
-static __device__ void bt_apply_back(const BtSweepSh &sh, float *Y, long ldy, int R, int C, int k1, int sh_off,
-                                     const float *tau, Vec vec)
-{
-    if (k1 < 0) return;
-    // the update of a column depends on that column only: strips of at most
-    // 512 columns each take the whole reflector sequence on their own
-    for (int c0 = 0; c0 < C; c0 += 512) {
-        const int Cs = min(512, C - c0);
-        float *Ys = Y + c0;
-#define BT_APPLY_CASE(K) \
-    case K: bt_apply_back_n<K>(sh, Ys, ldy, R, Cs, k1, sh_off, tau, vec); break;
-        switch ((Cs + 31) >> 5) {
-            BT_APPLY_CASE(1) BT_APPLY_CASE(2) BT_APPLY_CASE(3) BT_APPLY_CASE(4)
-            BT_APPLY_CASE(5) BT_APPLY_CASE(6) BT_APPLY_CASE(7) BT_APPLY_CASE(8)
-            BT_APPLY_CASE(9) BT_APPLY_CASE(10) BT_APPLY_CASE(11) BT_APPLY_CASE(12)
-            BT_APPLY_CASE(13) BT_APPLY_CASE(14) BT_APPLY_CASE(15) BT_APPLY_CASE(16)
-            default: break;
-        }
-#undef BT_APPLY_CASE
-    }
-}
-
 // entry r of column reflector k (below the diagonal of W) / row reflector k
-// (right of the superdiagonal)
+// (right of the superdiagonal); kRowMajorK: the entries of consecutive
+// reflectors for one r are adjacent in memory
 struct BtColVec {
+    static constexpr bool kRowMajorK = true;
     const float *W;
     long ldw;
     __device__ float operator()(int k, int r) const { return W[(long)r * ldw + k]; }
 };
 struct BtRowVec {
+    static constexpr bool kRowMajorK = false;
     const float *W;
     long ldw;
     __device__ float operator()(int k, int r) const { return W[(long)k * ldw + r]; }
 };
 
+namespace bt {
+constexpr int ANB = 32;   // reflectors per block of the blocked application
+constexpr int ARCH = 128; // rows of V staged at a time
+}  // namespace bt
+
+__host__ __device__ static size_t bt_apply_smem()
+{
+    using namespace bt;
+    return sizeof(float) * ((size_t)ARCH * (ANB + 1) + 2 * ANB * (ANB + 1) + (size_t)T_SWEEP * ANB) + 16;
+}
+
+// Y (R x C, ld ldy) <- H_0 H_1 ... H_k1 Y, reflector k acting on rows >= p_k =
+// k + sh_off with v_k(p_k) = 1 and v_k(r) = vec(k, r) below.  Blocks of ANB
+// consecutive reflectors are applied as I - V T V^T (compact WY, T upper
+// triangular from the Gram matrix V^T V by the larft recurrence), last block
+// first: Z = V^T Y, Z' = T Z, Y -= V Z'.  Every thread owns one column of a
+// strip of at most 512 columns; narrow strips split the rows over groups of
+// threads.  V is staged through shared memory ARCH rows at a time.
+template <typename Vec>
+static __device__ void bt_apply_blocked(float *sm, float *Y, long ldy, int R, int C, int k1, int sh_off,
+                                        const float *tau, Vec vec)
+{
+    using namespace bt;
+    constexpr int NT = T_SWEEP, NB = ANB, LD = ANB + 1;
+    if (k1 < 0) return;
+    float *Vs = sm;                  // ARCH x LD
+    float *Ts = Vs + ARCH * LD;      // NB x LD
+    float *Gs = Ts + NB * LD;        // NB x LD
+    float *Zs = Gs + NB * LD;        // NT x NB partial sums
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int kb = (k1 / NB) * NB; kb >= 0; kb -= NB) {
+        const int nb = min(k1 + 1, kb + NB) - kb;
+        const int pb = kb + sh_off;  // first row of the block's reflectors
+        auto stage = [&](int r0, int nr) {
+            __syncthreads();
+            for (int x = tid; x < nr * NB; x += NT) {
+                int rr, jj;
+                if (Vec::kRowMajorK) { rr = x / NB; jj = x % NB; }
+                else { jj = x / nr; rr = x % nr; }
+                const int r = r0 + rr, k = kb + jj, p = k + sh_off;
+                float v = 0.f;
+                if (jj < nb && r >= p) v = (r == p) ? 1.f : vec(k, r);
+                Vs[rr * LD + jj] = v;
+            }
+            __syncthreads();
+        };
+        // Gram matrix of the block's vectors: entries (e / NB, e % NB), e = tid, tid + NT
+        float g0 = 0.f, g1 = 0.f;
+        for (int r0 = pb; r0 < R; r0 += ARCH) {
+            const int nr = min(ARCH, R - r0);
+            stage(r0, nr);
+            const int i0 = tid / NB, i1 = (tid + NT) / NB, j = tid % NB;
+            for (int rr = 0; rr < nr; rr++) {
+                const float vj = Vs[rr * LD + j];
+                g0 = fmaf(Vs[rr * LD + i0], vj, g0);
+                g1 = fmaf(Vs[rr * LD + i1], vj, g1);
+            }
+        }
+        Gs[(tid / NB) * LD + tid % NB] = g0;
+        Gs[((tid + NT) / NB) * LD + tid % NB] = g1;
+        __syncthreads();
+        // T: one warp per row i, lane l holds T[i][l]:  T[i][i] = tau,
+        // T[i][j] = -tau_j sum_{b=i}^{j-1} T[i][b] G[b][j]
+        for (int i = warp; i < NB; i += NT / 32) {
+            float t = (lane == i && i < nb) ? tau[kb + i] : 0.f;
+            if (i < nb) {
+                for (int j = i + 1; j < nb; j++) {
+                    float p = (lane >= i && lane < j) ? t * Gs[lane * LD + j] : 0.f;
+                    p = warp_sum(p);
+                    if (lane == j) t = -tau[kb + j] * p;
+                }
+            }
+            Ts[i * LD + lane] = t;
+        }
+        __syncthreads();
+        for (int c0 = 0; c0 < C; c0 += NT) {
+            const int Cs = min(NT, C - c0);
+            const int S = max(1, NT / Cs);
+            const int c = tid % Cs, g = tid / Cs;
+            const bool act = g < S;
+            float z[NB];
+#pragma unroll
+            for (int jj = 0; jj < NB; jj++) z[jj] = 0.f;
+            // Z = V^T Y (each group of threads over its share of the rows)
+            for (int r0 = pb; r0 < R; r0 += ARCH) {
+                const int nr = min(ARCH, R - r0);
+                stage(r0, nr);
+                if (act) {
+                    // four rows' loads in flight before their products
+                    int rr = g;
+                    for (; rr + 3 * S < nr; rr += 4 * S) {
+                        float y[4];
+#pragma unroll
+                        for (int u = 0; u < 4; u++) y[u] = Y[(long)(r0 + rr + u * S) * ldy + c0 + c];
+#pragma unroll
+                        for (int u = 0; u < 4; u++)
+#pragma unroll
+                            for (int jj = 0; jj < NB; jj++) z[jj] = fmaf(Vs[(rr + u * S) * LD + jj], y[u], z[jj]);
+                    }
+                    for (; rr < nr; rr += S) {
+                        const float y = Y[(long)(r0 + rr) * ldy + c0 + c];
+#pragma unroll
+                        for (int jj = 0; jj < NB; jj++) z[jj] = fmaf(Vs[rr * LD + jj], y, z[jj]);
+                    }
+                }
+            }
+            if (act) {
+#pragma unroll
+                for (int jj = 0; jj < NB; jj++) Zs[(g * NB + jj) * Cs + c] = z[jj];
+            }
+            __syncthreads();
+            if (act && g == 0) {
+                // sum the groups, then Z' = T Z for this column
+#pragma unroll
+                for (int jj = 0; jj < NB; jj++) {
+                    float v = z[jj];
+                    for (int h = 1; h < S; h++) v += Zs[(h * NB + jj) * Cs + c];
+                    z[jj] = v;
+                }
+#pragma unroll
+                for (int i = 0; i < NB; i++) {
+                    float v = 0.f;
+#pragma unroll
+                    for (int jj = 0; jj < NB; jj++)
+                        if (jj >= i) v = fmaf(Ts[i * LD + jj], z[jj], v);
+                    Zs[i * Cs + c] = v;  // group 0's slots: read back by every group below
+                }
+            }
+            __syncthreads();
+            if (act) {
+#pragma unroll
+                for (int jj = 0; jj < NB; jj++) z[jj] = Zs[jj * Cs + c];
+            }
+            // Y -= V Z'
+            for (int r0 = pb; r0 < R; r0 += ARCH) {
+                const int nr = min(ARCH, R - r0);
+                stage(r0, nr);
+                if (act) {
+                    int rr = g;
+                    for (; rr + 3 * S < nr; rr += 4 * S) {
+                        float v[4];
+#pragma unroll
+                        for (int u = 0; u < 4; u++) v[u] = Y[(long)(r0 + rr + u * S) * ldy + c0 + c];
+#pragma unroll
+                        for (int u = 0; u < 4; u++) {
+#pragma unroll
+                            for (int jj = 0; jj < NB; jj++) v[u] = fmaf(-Vs[(rr + u * S) * LD + jj], z[jj], v[u]);
+                            Y[(long)(r0 + rr + u * S) * ldy + c0 + c] = v[u];
+                        }
+                    }
+                    for (; rr < nr; rr += S) {
+                        float *y = Y + (long)(r0 + rr) * ldy + c0 + c;
+                        float v = *y;
+#pragma unroll
+                        for (int jj = 0; jj < NB; jj++) v = fmaf(-Vs[rr * LD + jj], z[jj], v);
+                        *y = v;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+}
+
 // prof[2..5]: SM cycles of the U/X set-up, the U sweeps, the V sweeps and
 // the outputs; matrices finished
 __global__ void __launch_bounds__(bt::T_SWEEP, 1) bt_apply_k(const BtItem *items, int count, unsigned *queue,
                                                              char *arena, float *xslots, size_t xslot_floats,
-                                                             int maxc, int *status, unsigned long long *prof)
+                                                             int *status, unsigned long long *prof)
 {
     using namespace bt;
     constexpr int NT = T_SWEEP;
-    extern __shared__ __align__(16) unsigned char bt_sm3[];
-    const BtSweepSh sh = bt_sweep_sh(bt_sm3, maxc);
+    extern __shared__ __align__(16) float bt_sm3[];
+    int *s_item = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(bt_sm3) + bt_apply_smem() - 16);
     const int tid = threadIdx.x;
     float *X = xslots + (size_t)blockIdx.x * xslot_floats;
     for (;;) {
-        const int b = bt_next(queue, count, sh.item);
+        const int b = bt_next(queue, count, s_item);
         if (b < 0) break;
         const BtItem it = items[b];
         const int M = it.M, N = it.N;
@@ -878,9 +924,9 @@ __global__ void __launch_bounds__(bt::T_SWEEP, 1) bt_apply_k(const BtItem *items
         }
         __syncthreads();
         const long long t1 = clock64();
-        bt_apply_back(sh, it.U, M, M, M, N - 1, 0, m.tauq, BtColVec{m.W, m.ldw});
+        bt_apply_blocked(bt_sm3, it.U, M, M, M, N - 1, 0, m.tauq, BtColVec{m.W, m.ldw});
         const long long t2 = clock64();
-        bt_apply_back(sh, X, N, N, N, N - 2, 1, m.taup, BtRowVec{m.W, m.ldw});
+        bt_apply_blocked(bt_sm3, X, N, N, N, N - 2, 1, m.taup, BtRowVec{m.W, m.ldw});
         for (long t = tid; t < (long)N * N; t += NT) {
             const int r = (int)(t / N), j = (int)(t % N);
             it.Vt[t] = X[(long)j * N + r];
@@ -938,7 +984,7 @@ static bool bt_plan(int count, const int *M, const int *N, BtPlan *p)
         cudaFuncSetAttribute(bt_bdc_k, cudaFuncAttributeMaxDynamicSharedMemorySize, 48 * 1024);
         const int big = (int)bt_sweep_smem(PACO_BATCH_MAX_M);
         cudaFuncSetAttribute(bt_bidiag_k, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-        cudaFuncSetAttribute(bt_apply_k, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+        cudaFuncSetAttribute(bt_apply_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bt_apply_smem());
         cudaGetLastError();
         attr = true;
     }
@@ -963,7 +1009,7 @@ static bool bt_plan(int count, const int *M, const int *N, BtPlan *p)
     p->slots2 = std::min(count, sms * bt_occupancy((const void *)bt_bdc_k, bt::T_BDC, bt_dyn_smem(Nx)));
     // divide-and-conquer scratch is N^2-sized per CTA: at most about 4 GiB of it
     p->slots2 = std::max(1, std::min(p->slots2, (int)std::max<size_t>(sms / 4, ((size_t)4 << 30) / p->bdc_slot)));
-    p->slots3 = std::min(count, sms * bt_occupancy((const void *)bt_apply_k, bt::T_SWEEP, bt_sweep_smem(p->maxc3)));
+    p->slots3 = std::min(count, sms * bt_occupancy((const void *)bt_apply_k, bt::T_SWEEP, bt_apply_smem()));
     p->bdc_off = p->arena_off + a;
     p->x_off = p->bdc_off + p->bdc_slot * p->slots2;
     p->total = p->x_off + ((sizeof(float) * p->x_slot * p->slots3 + 255) & ~(size_t)255);
@@ -1089,8 +1135,8 @@ int paco_svd_batched(int count, const int *M, const int *N, const float *const *
     paco_count_launch(), bt_bdc_k<<<p.slots2, bt::T_BDC, bt_dyn_smem(p.Nx), s>>>(
                              dit, count, queues + 1, arena, ws + p.bdc_off, p.bdc_slot, prof);
     if (g_bt_timing) cudaEventRecord(g_bt_ev[2], s);
-    paco_count_launch(), bt_apply_k<<<p.slots3, bt::T_SWEEP, bt_sweep_smem(p.maxc3), s>>>(
-                             dit, count, queues + 2, arena, (float *)(ws + p.x_off), p.x_slot, p.maxc3, status, prof);
+    paco_count_launch(), bt_apply_k<<<p.slots3, bt::T_SWEEP, bt_apply_smem(), s>>>(
+                             dit, count, queues + 2, arena, (float *)(ws + p.x_off), p.x_slot, status, prof);
     if (g_bt_timing) cudaEventRecord(g_bt_ev[3], s);
     return cudaGetLastError() == cudaSuccess ? PACO_OK : PACO_ERR_CUDA;
 }
