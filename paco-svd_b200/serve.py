@@ -164,6 +164,12 @@ class SvdServer:
             self.inflight -= r.nbytes
             r.A = None
             self.completed.append(r)
+        # the copies above run on the current stream: keep the batch's buffers
+        # out of the allocator's reach until they have, or the next batch on
+        # this batch's stream could reuse and overwrite them first
+        cur = self.torch.cuda.current_stream()
+        for t in (b.U, b.Vt, b.s, b.status):
+            t.record_stream(cur)
         self.inflight -= b.nbytes
 
     def step(self, now_fn):
