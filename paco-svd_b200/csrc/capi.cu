@@ -140,7 +140,8 @@ size_t paco_debug_trace_offset(int M, int N)
 
 // Test hook (not part of the public header): one strided product
 // C = alpha * opA * opB + beta * C on the SIMT engine (mode 0) or the tensor
-// cores (mode 1), opA(m, k) = A[m * a_rs + k * a_cs], opB(k, n) = B[k * b_rs + n * b_cs].
+// cores (mode 1; mode 2 keeps products without split-K off the persistent
+// kernel), opA(m, k) = A[m * a_rs + k * a_cs], opB(k, n) = B[k * b_rs + n * b_cs].
 // `ws` starts with the status block; the rest is GEMM scratch.  Synchronous.
 size_t paco_debug_gemm_ws_bytes(int M, int N, int K)
 {
@@ -157,10 +158,15 @@ int paco_debug_gemm(int M, int N, int K, float alpha, const float *A, long a_rs,
     float *scr = (float *)((char *)ws + 512);
     bd_init_attrs();
     cudaMemsetAsync(st, 0, sizeof(DevStatus), s);
-    cudaError_t err = mode == 1 ? gemm_tc_run(M, N, K, alpha, gop(A, a_rs, a_cs), gop(B, b_rs, b_cs), beta, C, ldc,
-                                              scr, st, s)
-                                : gemm_run(M, N, K, alpha, gop(A, a_rs, a_cs), gop(B, b_rs, b_cs), beta, C, ldc,
-                                           std::min(8, std::max(1, K / 512)), scr, s);
+    cudaError_t err;
+    if (mode == 1 || mode == 2) {  // 2: the one-tile-per-CTA kernel only
+        const int prev = gemm_tc_set_persistent(mode == 1);
+        err = gemm_tc_run(M, N, K, alpha, gop(A, a_rs, a_cs), gop(B, b_rs, b_cs), beta, C, ldc, scr, st, s);
+        gemm_tc_set_persistent(prev);
+    } else {
+        err = gemm_run(M, N, K, alpha, gop(A, a_rs, a_cs), gop(B, b_rs, b_cs), beta, C, ldc,
+                       std::min(8, std::max(1, K / 512)), scr, s);
+    }
     if (err != cudaSuccess) return PACO_ERR_CUDA;
     return paco_sync_status(ws, stream, nullptr);
 }

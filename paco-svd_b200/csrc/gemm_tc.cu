@@ -329,10 +329,235 @@ __global__ void __launch_bounds__(128, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN) : "memory");
 }
 
+// ------------------------------------------------------------------ persistent GEMM
+
+// Persistent, warp-specialized form of tc_gemm for products without split-K:
+// CTA b takes tiles b, b + gridDim.x, ... (6 warps).  Warp 0 issues the bulk
+// copies (operand stages, and the C tile when beta != 0), warp 1 issues the
+// MMAs into one of two TMEM accumulators (tile parity), warps 2-5 run the
+// epilogue of tile t while the MMAs of tile t+1 proceed.  Barriers:
+//   full/empty[s]   operand stage s loaded / consumed by the MMAs
+//   accf/acce[a]    accumulator a complete / read out by the epilogue
+//   cfull/cempty    C tile loaded / written back (its buffer free)
+// Every wait is bounded; a role that gives up raises s_abort, the others stop
+// at their next check or time out, copies in flight and issued MMAs are
+// waited for (bounded) and the tensor memory is freed.
+constexpr int PT_THREADS = 192;
+
+__global__ void __launch_bounds__(PT_THREADS, 1)
+    tc_gemm_p(int M, int N, int KT, int NTt, int ntiles, float alpha, const float *Ahi, const float *Alo,
+              const float *Bhi, const float *Blo, float beta, float *C, long ldc, int ctma, const int *lim,
+              DevStatus *st)
+{
+    if (lim) M = min(M, *lim);
+    extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], accf[2], acce[2], cfull, cempty, done;
+    __shared__ uint32_t s_tmem;
+    __shared__ volatile int s_abort;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    float *stage = (float *)(tc_smem_raw + ((1024u - (smem_u32(tc_smem_raw) & 1023u)) & 1023u));
+    float *Cbuf = stage + (long)STAGES * 4 * IMG;  // TM x TN
+    float *sbuf = Cbuf + TM * TN;                  // 4 x 32 x 33 epilogue staging
+    const bool cload = ctma && beta != 0.f;
+    const int ntl = (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;  // tiles of this CTA
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(2 * TN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int k = 0; k < STAGES; k++) {
+            mbar_init(&full[k], 1);
+            mbar_init(&empty[k], 1);
+        }
+        for (int k = 0; k < 2; k++) {
+            mbar_init(&accf[k], 1);
+            mbar_init(&acce[k], 1);
+        }
+        mbar_init(&cfull, 1);
+        mbar_init(&cempty, 1);
+        mbar_init(&done, 1);
+        mbar_init_fence();
+        s_abort = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+
+    if (warp == 0 && lane == 0) {
+        // ------------------------------------------------ producer
+        int it = 0, cl = 0;  // stage uses issued, C tiles issued
+        for (int lt = 0; lt < ntl && !s_abort; lt++) {
+            const int t = blockIdx.x + lt * gridDim.x, mt = t / NTt, nt = t % NTt;
+            const long abase = (long)mt * KT * IMG, bbase = (long)nt * KT * IMG;
+            bool ok = true;
+            for (int kb = 0; kb < KT; kb++, it++) {
+                const int sidx = it % STAGES;
+                if (it >= STAGES && !mbar_wait_bounded(&empty[sidx], ((it / STAGES) - 1) & 1, st, 611)) {
+                    ok = false;
+                    break;
+                }
+                float *dst = stage + (long)sidx * 4 * IMG;
+                const long ko = (long)kb * IMG;
+                mbar_expect_tx(&full[sidx], 4u * IMG * 4u);
+                tma_load_1d(dst + 0 * IMG, Ahi + abase + ko, IMG * 4u, &full[sidx]);
+                tma_load_1d(dst + 1 * IMG, Alo + abase + ko, IMG * 4u, &full[sidx]);
+                tma_load_1d(dst + 2 * IMG, Bhi + bbase + ko, IMG * 4u, &full[sidx]);
+                tma_load_1d(dst + 3 * IMG, Blo + bbase + ko, IMG * 4u, &full[sidx]);
+            }
+            if (!ok) { s_abort = 1; break; }
+            // the C tile of this tile, once the epilogue of the previous one has
+            // written its tile back (the operands of the next tile are already
+            // on their way)
+            if (cload) {
+                if (lt > 0 && !mbar_wait_bounded(&cempty, (lt - 1) & 1, st, 610)) { s_abort = 1; break; }
+                const int m0 = mt * TM, n0 = nt * TN;
+                const int nrows = max(0, min(TM, M - m0)), ncols = min(TN, N - n0);
+                mbar_expect_tx(&cfull, (uint32_t)(nrows * ncols * 4));
+                for (int r = 0; r < nrows; r++)
+                    tma_load_1d(Cbuf + r * TN, C + (long)(m0 + r) * ldc + n0, (uint32_t)(ncols * 4), &cfull);
+                cl++;
+            }
+        }
+        // copies in flight land before the CTA exits: the last use of each stage
+        for (int j = max(0, it - STAGES); j < it; j++)
+            mbar_wait_bounded(&full[j % STAGES], (j / STAGES) & 1, st, 612, 1000000000LL);
+        if (cl > 0) mbar_wait_bounded(&cfull, (cl - 1) & 1, st, 613, 1000000000LL);
+    } else if (warp == 1 && lane == 0) {
+        // ------------------------------------------------ MMA issuer
+        int it = 0;
+        for (int lt = 0; lt < ntl && !s_abort; lt++) {
+            const int ab = lt & 1;
+            if (lt >= 2 && !mbar_wait_bounded(&acce[ab], ((lt >> 1) - 1) & 1, st, 620)) { s_abort = 1; break; }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t acc = tmem + (uint32_t)(ab * TN);
+            bool ok = true;
+            for (int kb = 0; kb < KT; kb++, it++) {
+                const int sidx = it % STAGES;
+                if (!mbar_wait_bounded(&full[sidx], (it / STAGES) & 1, st, 621)) { ok = false; break; }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t base = smem_u32(stage + (long)sidx * 4 * IMG);
+                const uint64_t ahi = smem_desc(base), alo = smem_desc(base + IMG * 4);
+                const uint64_t bhi = smem_desc(base + 2 * IMG * 4), blo = smem_desc(base + 3 * IMG * 4);
+#pragma unroll
+                for (int j = 0; j < TK / 8; j++) {
+                    const uint64_t dk = (uint64_t)(j * 32 >> 4);
+                    mma_tf32(acc, alo + dk, bhi + dk, (kb | j) ? 1u : 0u);
+                    mma_tf32(acc, ahi + dk, blo + dk, 1u);
+                    mma_tf32(acc, ahi + dk, bhi + dk, 1u);
+                }
+                mma_commit(&empty[sidx]);
+            }
+            if (!ok) { s_abort = 1; break; }
+            mma_commit(&accf[ab]);
+        }
+        mma_commit(&done);  // every MMA issued above has completed when this arrives
+        mbar_wait_bounded(&done, 0, st, 622);
+    } else if (warp >= 2) {
+        // ------------------------------------------------ epilogue (warps 2-5)
+        const int q = warp & 3;          // TMEM lane quarter of this warp: rows 32q..32q+31
+        const int ew = warp - 2;
+        float(*sb)[33] = reinterpret_cast<float(*)[33]>(sbuf + ew * 32 * 33);
+        for (int lt = 0; lt < ntl; lt++) {
+            const int ab = lt & 1;
+            bool ok = mbar_wait_bounded(&accf[ab], (lt >> 1) & 1, st, 630);
+            if (ok && cload) ok = mbar_wait_bounded(&cfull, lt & 1, st, 631);
+            if (bar_or(1, 128, !ok || s_abort)) { s_abort = 1; break; }  // the same decision in every warp
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int t = blockIdx.x + lt * gridDim.x, mt = t / NTt, nt = t % NTt;
+            const int m0 = mt * TM, n0 = nt * TN;
+            const int nrows = min(TM, M - m0), ncols = min(TN, N - n0);
+            const uint32_t taddr = tmem + (uint32_t)(ab * TN) + ((uint32_t)(q * 32) << 16);
+#pragma unroll 1
+            for (int c0 = 0; c0 < TN; c0 += 32) {
+                uint32_t v[32];
+                tmem_ld32(taddr + (uint32_t)c0, v);
+#pragma unroll
+                for (int k = 0; k < 32; k++) sb[lane][k] = __uint_as_float(v[k]);
+                __syncwarp();
+                const int cl = c0 + lane;
+                if (cl < ncols) {
+#pragma unroll 4
+                    for (int rr = 0; rr < 32; rr++) {
+                        const int rl = q * 32 + rr;
+                        if (rl >= nrows) break;
+                        float x = alpha * sb[rr][lane];
+                        if (ctma) {
+                            if (cload) x = fmaf(beta, Cbuf[rl * TN + cl], x);
+                            Cbuf[rl * TN + cl] = x;
+                        } else {
+                            float *c = C + (long)(m0 + rl) * ldc + n0 + cl;
+                            if (beta != 0.f) x = fmaf(beta, *c, x);
+                            *c = x;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            if (ctma) proxy_async_fence();  // Cbuf writes visible to the bulk stores
+            bar_or(1, 128, false);          // every warp has read the accumulator and written Cbuf
+            if (ew == 0 && lane == 0) mbar_arrive(&acce[ab]);
+            if (ctma) {
+                if (ew == 0) {
+                    for (int r = lane; r < nrows; r += 32)
+                        tma_store_1d(C + (long)(m0 + r) * ldc + n0, Cbuf + r * TN, (uint32_t)(ncols * 4));
+                    tma_store_commit_and_drain();
+                }
+                bar_or(1, 128, false);  // the stores have read Cbuf
+                if (cload && ew == 0 && lane == 0) mbar_arrive(&cempty);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        __syncwarp();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TN) : "memory");
+    }
+}
+
 // ------------------------------------------------------------------ host
 
 // stages, the C tile, and slack for the 1024-byte alignment
 static size_t tc_smem_bytes() { return (size_t)(STAGES * 4 * IMG + TM * TN) * sizeof(float) + 1024; }
+// the persistent kernel adds the epilogue staging of its four epilogue warps
+static size_t tc_p_smem_bytes() { return tc_smem_bytes() + 4 * 32 * 33 * sizeof(float); }
+
+static int tc_sms()
+{
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) !=
+                                                      cudaSuccess || n < 1)
+            n = 148;
+    }
+    return n;
+}
+
+// PACO_TC_PERSISTENT=0 keeps every product on the one-tile-per-CTA kernel
+static int g_tc_persistent = -1;
+
+static bool tc_persistent()
+{
+    if (g_tc_persistent < 0) {
+        const char *e = getenv("PACO_TC_PERSISTENT");
+        g_tc_persistent = (e && e[0] == '0') ? 0 : 1;
+    }
+    return g_tc_persistent == 1;
+}
+
+int gemm_tc_set_persistent(int on)
+{
+    const int prev = tc_persistent() ? 1 : 0;
+    g_tc_persistent = on ? 1 : 0;
+    return prev;
+}
 
 size_t gemm_tc_scratch_floats(int M, int N, int K)
 {
@@ -356,6 +581,7 @@ bool gemm_tc_enabled()
 void gemm_tc_init_attrs()
 {
     cudaFuncSetAttribute(tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes());
+    cudaFuncSetAttribute(tc_gemm_p, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_p_smem_bytes());
 }
 
 cudaError_t gemm_tc_run(int M, int N, int K, float alpha, GemmOp A, GemmOp B, float beta, float *C, long ldc,
@@ -375,6 +601,13 @@ cudaError_t gemm_tc_run(int M, int N, int K, float alpha, GemmOp A, GemmOp B, fl
     const float *dst = part ? part : C;
     const long dld = part ? (long)N : ldc;
     const int ctma = ((((uintptr_t)dst) & 15) == 0 && (dld % 4) == 0 && (N % 4) == 0) ? 1 : 0;
+    if (!part && tc_persistent()) {
+        const int ntiles = g.MT * g.NT;
+        const int grid = std::min(ntiles, tc_sms());
+        paco_count_launch(), tc_gemm_p<<<grid, PT_THREADS, tc_p_smem_bytes(), s>>>(
+                                 M, N, g.KT, g.NT, ntiles, alpha, Ahi, Alo, Bhi, Blo, beta, C, ldc, ctma, lim, st);
+        return cudaGetLastError();
+    }
     paco_count_launch(), tc_gemm<<<dim3(g.NT, g.MT, g.splits), 128, tc_smem_bytes(), s>>>(
                              M, N, g.KT, kper, alpha, Ahi, Alo, Bhi, Blo, beta, C, ldc, part, ctma, lim, st);
     if (part) {

@@ -26,6 +26,11 @@ void gemm_tc_init_attrs();
 cudaError_t gemm_tc_run(int M, int N, int K, float alpha, GemmOp A, GemmOp B, float beta, float *C, long ldc,
                         float *scratch, DevStatus *st, cudaStream_t s, const int *lim = nullptr);
 
+// Products without split-K run on the persistent kernel (one CTA per SM
+// walking the tiles) unless this is set to 0 (or PACO_TC_PERSISTENT=0);
+// returns the previous setting.
+int gemm_tc_set_persistent(int on);
+
 // Tensor-core product when it is enabled, tc_scratch holds enough floats and
 // the product is large enough to pay for the operand packing; otherwise the
 // SIMT engine (with its own split-K scratch).

@@ -54,6 +54,26 @@ __device__ __forceinline__ void tma_store_commit_and_drain()
     asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
+// Plain arrival (count 1) on an mbarrier.
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Named barrier `id` over `nthreads` threads (a multiple of 32, whole warps)
+// that also ORs a predicate: every participant gets the same result.  The
+// non-aligned form, so lanes need not arrive converged.
+__device__ __forceinline__ bool bar_or(int id, int nthreads, bool v)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n barrier.red.or.pred q, %2, %3, p;\n selp.u32 %0, 1, 0, q;\n}"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id), "r"(nthreads)
+        : "memory");
+    return r != 0;
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
 {
     uint32_t ok;

@@ -1,7 +1,8 @@
 """The tensor-core (tcgen05, 3xTF32) product against a float64 product and the
 SIMT engine, on the operand layouts the SVD pipeline uses: row-major and
-transposed operands, partial 128-tiles, split-K, beta = 0 and beta = 1.
-Called through the library's test hook paco_debug_gemm."""
+transposed operands, partial 128-tiles, split-K, beta = 0 and beta = 1, on
+both the persistent kernel (several tiles per CTA) and the one-tile-per-CTA
+kernel.  Called through the library's test hook paco_debug_gemm."""
 import ctypes
 
 import numpy as np
@@ -49,6 +50,9 @@ SHAPES = [
     (1000, 1100, 64, False, False),    # trailing update shape
     (517, 517, 517, False, True),      # W^T-like transposed B
     (96, 64, 1300, True, True),
+    (2048, 2048, 64, False, False),    # 256 tiles: the persistent kernel walks 2 per CTA
+    (4100, 1030, 96, False, False),    # 297 tiles, partial in m and n, N % 4 != 0 (plain stores)
+    (4096, 4096, 64, False, True),     # 1024 tiles, 7 per CTA
 ]
 
 
@@ -65,7 +69,7 @@ def test_tensor_core_product_matches_float64(M, N, K, at, bt, beta):
     opB = (B64.float().double().T if bt else B64.float().double())
     ref = -1.0 * (opA @ opB) + beta * C64.float().double()
     scale = (opA.abs() @ opB.abs()).max().item() + beta * C64.abs().max().item()
-    for mode in (1, 0):
+    for mode in (1, 2, 0):
         C = C64.float().cuda()
         run_gemm(A, B, C, -1.0, beta, mode, at, bt)
         err = (C.double().cpu() - ref).abs().max().item()
@@ -82,5 +86,21 @@ def test_tensor_core_product_is_deterministic():
     for _ in range(2):
         C = torch.zeros(128, 640, device="cuda")
         run_gemm(A, B, C, 1.0, 0.0, 1)
+        outs.append(C.cpu())
+    assert torch.equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("M,N,K", [(2048, 2048, 64), (1000, 1100, 64), (517, 517, 517)])
+def test_persistent_and_per_tile_kernels_agree_bitwise(M, N, K):
+    # same products, same accumulation order within a tile: identical bits
+    import torch
+    g = torch.Generator().manual_seed(M + N + K)
+    A = torch.randn(M, K, generator=g).cuda()
+    B = torch.randn(K, N, generator=g).cuda()
+    C0 = torch.randn(M, N, generator=g).cuda()
+    outs = []
+    for mode in (1, 2):
+        C = C0.clone()
+        run_gemm(A, B, C, -1.0, 1.0, mode)
         outs.append(C.cpu())
     assert torch.equal(outs[0], outs[1])
