@@ -521,8 +521,11 @@ static cudaError_t apply_block_reflector(const BdWs &w, float *Q, long ldq, long
                                          const float *tau, cudaStream_t s)
 {
     const int splits = std::max(1, std::min(SPLITS, ceil_div(Lp, 512)));
-    // G = Vp^T Vp (split along the long k = Lp dimension), then T
-    cudaError_t err = gemm_run(nbp, nbp, Lp, 1.f, gop(w.Vp, 1, NBF), gop(w.Vp, NBF, 1), 0.f, w.gram, NBF, splits,
+    // G = Vp^T Vp: one 128 x 128 tile, so the long k = Lp dimension is split
+    // finely (64 rows per CTA, as many splits as the partial buffer holds)
+    // (the partial buffer holds SPLITS * NBF * max(M, N) >= SPLITS * NBF * ldq floats)
+    const int gsplits = (int)std::max(1L, std::min({(long)ceil_div(Lp, 64), 64L, (long)SPLITS * ldq / NBF}));
+    cudaError_t err = gemm_run(nbp, nbp, Lp, 1.f, gop(w.Vp, 1, NBF), gop(w.Vp, NBF, 1), 0.f, w.gram, NBF, gsplits,
                                w.gscr, s);
     if (err) return err;
     paco_count_launch(), bd_build_t<<<NBF / 8, 256, (size_t)NBF * NBF * sizeof(float), s>>>(w.gram, nbp, tau, w.T);
@@ -531,9 +534,13 @@ static cudaError_t apply_block_reflector(const BdWs &w, float *Q, long ldq, long
     err = gemm_any(nbp, Lp, Lp, 1.f, gop(w.Vp, 1, NBF), gop(Qs, ldq, 1), 0.f, w.G1, Lp, splits, w.gscr, w.tcs,
                    w.tcs_floats, w.st, s);
     if (err) return err;
-    // G2 = T G1
-    err = gemm_any(nbp, Lp, nbp, 1.f, gop(w.T, NBF, 1), gop(w.G1, Lp, 1), 0.f, w.G2, Lp, 1, nullptr, w.tcs,
-                   w.tcs_floats, w.st, s);
+    // G2 = T G1 (128 x Lp x 128: small, but on the SIMT engine it runs on
+    // only Lp / 128 CTAs, so it goes to the tensor cores from Lp = 256 on)
+    if (w.tcs && gemm_tc_enabled() && Lp >= 256 && gemm_tc_scratch_floats(nbp, Lp, nbp) <= w.tcs_floats)
+        err = gemm_tc_run(nbp, Lp, nbp, 1.f, gop(w.T, NBF, 1), gop(w.G1, Lp, 1), 0.f, w.G2, Lp, w.tcs, w.st, s);
+    else
+        err = gemm_any(nbp, Lp, nbp, 1.f, gop(w.T, NBF, 1), gop(w.G1, Lp, 1), 0.f, w.G2, Lp, 1, nullptr, w.tcs,
+                       w.tcs_floats, w.st, s);
     if (err) return err;
     // Q_sub -= Vp G2
     return gemm_any(Lp, Lp, nbp, -1.f, gop(w.Vp, NBF, 1), gop(w.G2, Lp, 1), 1.f, Qs, ldq, 1, nullptr, w.tcs,

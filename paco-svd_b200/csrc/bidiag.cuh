@@ -60,7 +60,7 @@ struct BdWs {
     float *inv_v0c, *inv_v0r; // N each: 1/v0 of every reflector
     StepScal *sc;
     PkCtl *ctl;
-    unsigned long long *trace; // NB+1 steps x 8 phases x 2 CTAs
+    unsigned long long *trace; // NB+1 steps x 16 slots x 2 CTAs
     float *bcA, *bcB;          // PR each: pivot and panel entries of a reflector
     float *Vp;     // max(M,N) x NBF explicit reflector block (formation of U, V)
     float *T;      // NBF x NBF
@@ -99,7 +99,7 @@ static inline size_t bd_carve(void *base, int M, int N, BdWs *w)
     w->inv_v0r = (float *)take(sizeof(float) * N);
     w->sc = (StepScal *)take(sizeof(StepScal));
     w->ctl = (PkCtl *)take(sizeof(PkCtl));
-    w->trace = (unsigned long long *)take(sizeof(unsigned long long) * (NB + 1) * 8 * 2);
+    w->trace = (unsigned long long *)take(sizeof(unsigned long long) * (NB + 1) * 16 * 2);
     w->bcA = (float *)take(sizeof(float) * PR);
     w->bcB = (float *)take(sizeof(float) * PR);
     w->Vp = (float *)take(sizeof(float) * (size_t)mx * NBF);

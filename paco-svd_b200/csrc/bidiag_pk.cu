@@ -45,13 +45,19 @@ __device__ __forceinline__ unsigned long long gtimer()
     return t;
 }
 
-// Arrive at a grid barrier and wait (bounded) until `target` arrivals.
+__device__ __forceinline__ void red_release_add(unsigned *p, unsigned v)
+{
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Arrive at a grid barrier and wait (bounded) until `target` arrivals.  The
+// arrival is a release (it publishes every write the CTA made before the
+// __syncthreads) and the poll an acquire, so no further fences are needed.
 __device__ bool pk_barrier(PkCtl *c, unsigned target, DevStatus *st, int where, int *s_ok)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
-        __threadfence();
-        atomicAdd(&c->cnt, 1u);
+        red_release_add(&c->cnt, 1u);
         int ok = 1;
         long long t0 = clock64();
         while (ld_acquire(&c->cnt) < target) {
@@ -67,7 +73,6 @@ __device__ bool pk_barrier(PkCtl *c, unsigned target, DevStatus *st, int where, 
         *s_ok = ok;
     }
     __syncthreads();
-    __threadfence();
     return *s_ok != 0;
 }
 
@@ -150,6 +155,22 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
     __syncthreads();
     uint32_t phase0 = 0, phase1 = 0;
     bool failed = false;
+    // streamed rows: batches of the coming row pass already on their way
+    // (issued at the end of the previous row pass, so their latency hides
+    // behind the barriers and the column pass)
+    int pf_n = 0;
+    auto first_active = [&](int step) {
+        int k = 0;
+        while (k < nown && own_row(k) < step) k++;
+        return k;
+    };
+    auto issue_rows = [&](int kf, int bb, int stage) {
+        int k0 = kf + bb * R, nr = min(R, nown - k0);
+        mbar_expect_tx(&bars[stage], (uint32_t)nr * L * 4u);
+        for (int rr = 0; rr < nr; rr++)
+            tma_load_1d(tiles + ((long)stage * R + rr) * L, a.W + (long)own_row(k0 + rr) * ldw + p0, (uint32_t)L * 4u,
+                        &bars[stage]);
+    };
 
     if (resident && nown > 0) {
         if (tid == 0) {
@@ -166,8 +187,11 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
     const int last_step = (p1 < N) ? p1 : p1 - 1;
     const bool tracing = a.trace && a.trace_p0 == p0 && tid == 0 && (b == 0 || b == G - 1);
     auto stamp = [&](int i, int ph) {
-        if (tracing) a.trace[(((i - p0) * 8 + ph) * 2) + (b == 0 ? 0 : 1)] = gtimer();
+        if (tracing) a.trace[(((i - p0) * 16 + ph) * 2) + (b == 0 ? 0 : 1)] = gtimer();
     };
+    // slots 7-8 of a step: nanoseconds its row pass waited for streamed
+    // rows, and its number of row batches
+    unsigned long long waited = 0;
     for (int i = p0; i <= last_step && !failed; i++) {
         stamp(i, 0);
         const bool xonly = (i == p1);
@@ -240,27 +264,17 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
         const float invc = (ii >= 1) ? s_cinv_prev : 1.f;
 
         // ------------------------------------------------------ row pass
-        int kfirst = 0;
-        while (kfirst < nown && own_row(kfirst) < i) kfirst++;
+        const int kfirst = first_active(i);
         const int nact = nown - kfirst;
         const int nbatch = (nact + R - 1) / R;
         __syncthreads();
         stamp(i, 1);
-        if (!resident && tid == 0) {
+        if (!resident && tid == 0 && pf_n < min(2, nbatch)) {
             proxy_async_fence();
             asm volatile("fence.proxy.async.global;" ::: "memory");
+            for (int bb = pf_n; bb < min(2, nbatch); bb++) issue_rows(kfirst, bb, bb);
         }
-        auto issue = [&](int bb, int stage) {
-            int k0 = kfirst + bb * R, nr = min(R, nown - k0);
-            mbar_expect_tx(&bars[stage], (uint32_t)nr * L * 4u);
-            for (int rr = 0; rr < nr; rr++)
-                tma_load_1d(tiles + ((long)stage * R + rr) * L, a.W + (long)own_row(k0 + rr) * ldw + p0,
-                            (uint32_t)L * 4u, &bars[stage]);
-        };
-        if (!resident && tid == 0) {
-            if (nbatch > 0) issue(0, 0);
-            if (nbatch > 1) issue(1, 1);
-        }
+        pf_n = 0;
         float w_ss = 0.f, w_g1 = 0.f, w_g2 = 0.f;
         for (int bb = 0; bb < nbatch; bb++) {
             const int k0 = kfirst + bb * R, nr = min(R, nown - k0);
@@ -274,7 +288,9 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
             if (resident) {
                 T = tiles + (long)k0 * L;
             } else {
+                const unsigned long long tw = tracing ? gtimer() : 0ull;
                 bool ok = mbar_wait_bounded(&bars[stage], stage ? phase1 : phase0, st, 200 + i);
+                if (tracing) waited += gtimer() - tw;
                 if (stage) phase1 ^= 1; else phase0 ^= 1;
                 if (__syncthreads_or(!ok)) { failed = true; break; }
                 T = tiles + (long)stage * R * L;
@@ -371,10 +387,27 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
             __syncthreads();
             if (!resident && tid == 0 && bb + 2 < nbatch) {
                 proxy_async_fence();
-                issue(bb + 2, stage);
+                issue_rows(kfirst, bb + 2, stage);
             }
         }
         if (__syncthreads_or(failed)) { failed = true; break; }
+        if (tracing) {
+            unsigned long long *tr = a.trace + (long)(i - p0) * 32 + (b == 0 ? 0 : 1);
+            tr[7 * 2] = waited;
+            tr[8 * 2] = (unsigned long long)nbatch;
+            waited = 0;
+        }
+        if (!resident && i < last_step) {
+            // the first two batches of the next step's row pass: its rows (>= i+1)
+            // changed only in this row pass, by this CTA
+            const int kf1 = first_active(i + 1);
+            const int nb1 = (nown - kf1 + R - 1) / R;
+            pf_n = min(2, nb1);
+            if (tid == 0 && pf_n > 0) {
+                asm volatile("fence.proxy.async.global;" ::: "memory");
+                for (int bb = 0; bb < pf_n; bb++) issue_rows(kf1, bb, bb);
+            }
+        }
         stamp(i, 2);
         if (xonly) break; // the X-only pass ends the panel
 
@@ -418,6 +451,20 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
         stamp(i, 3);
         if (!pk_barrier(ctl, cnt_base + (++nbar) * G, st, 300 + i, &s_ok)) { failed = true; break; }
 
+        // the partial A^T x records of this CTA's first column chunk travel
+        // with the records of the column reflector: one L2 round trip
+        constexpr int YV = RB_CAP / (RP_THREADS / 32);
+        float yv0[YV];
+        {
+            const int j = i + 1 + b * 32 + lane;
+            const bool v = (b < nchunk) && j < N;
+#pragma unroll
+            for (int k = 0; k < YV; k++) {
+                const int q = warp + (RP_THREADS / 32) * k;
+                yv0[k] = (v && q < G) ? __ldcg(&a.ypart[(long)q * ldw + j]) : 0.f;
+            }
+        }
+
         // ------------- column reflector of step i (every CTA)
         {
             const int nbc = 1 + 2 * ii;
@@ -459,19 +506,19 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
         for (int ch = b; ch < nchunk; ch += G) {
             const int j = i + 1 + ch * 32 + lane;
             const bool valid = j < N;
-            float yv[RB_CAP / (RP_THREADS / 32)];
+            const bool first = (ch == b);
+            float yv[YV];
 #pragma unroll
-            for (int k = 0; k < RB_CAP / (RP_THREADS / 32); k++) {
+            for (int k = 0; k < YV; k++) {
                 int q = warp + (RP_THREADS / 32) * k;
-                yv[k] = (valid && q < G) ? __ldcg(&a.ypart[(long)q * ldw + j]) : 0.f;
+                yv[k] = first ? yv0[k] : ((valid && q < G) ? __ldcg(&a.ypart[(long)q * ldw + j]) : 0.f);
             }
             float ys = 0.f;
 #pragma unroll
-            for (int k = 0; k < RB_CAP / (RP_THREADS / 32); k++) ys += yv[k];
+            for (int k = 0; k < YV; k++) ys += yv[k];
             cy[warp][lane] = ys;
             // warp w owns panel indices q in [2w, 2w+2)
             float Yq[2], Wq[2], pa = 0.f, pb = 0.f;
-            const bool first = (ch == b);
 #pragma unroll
             for (int e = 0; e < 2; e++) {
                 int q = 2 * warp + e;
@@ -532,6 +579,11 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
         if (!pk_barrier(ctl, cnt_base + (++nbar) * G, st, 400 + i, &s_ok)) { failed = true; break; }
         stamp(i, 6);
     }
+    // a step that ended early leaves prefetched rows in flight: they land
+    // before the CTA exits
+    if (!resident && tid == 0)
+        for (int bb = 0; bb < pf_n; bb++)
+            mbar_wait_bounded(&bars[bb], bb ? phase1 : phase0, st, 91, 1000000000LL);
 }
 
 // Grid barriers one launch for panel [p0, p1) passes (host and kernel agree):
