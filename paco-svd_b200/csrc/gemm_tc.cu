@@ -20,8 +20,12 @@
 // Every wait is bounded; a wait that gives up records PACO_ERR_TIMEOUT, the
 // copies still in flight are waited for (again bounded), the CTA frees its
 // tensor memory and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cstdlib>
+#include <cstring>
 
 #include "gemm_tc.cuh"
 #include "tma.cuh"
@@ -332,33 +336,56 @@ __global__ void __launch_bounds__(128, 1)
 // ------------------------------------------------------------------ persistent GEMM
 
 // Persistent, warp-specialized form of tc_gemm for products without split-K:
-// CTA b takes tiles b, b + gridDim.x, ... (6 warps).  Warp 0 issues the bulk
-// copies (operand stages, and the C tile when beta != 0), warp 1 issues the
-// MMAs into one of two TMEM accumulators (tile parity), warps 2-5 run the
-// epilogue of tile t while the MMAs of tile t+1 proceed.  Barriers:
-//   full/empty[s]   operand stage s loaded / consumed by the MMAs
-//   accf/acce[a]    accumulator a complete / read out by the epilogue
-//   cfull/cempty    C tile loaded / written back (its buffer free)
+// CTA b takes tiles b, b + gridDim.x, ... (6 warps).  Warp 0 issues the copies
+// (operand stages; the C tile when beta != 0), warp 1 issues the MMAs into one
+// of two TMEM accumulators (tile parity), warps 2-5 run the epilogue of tile t
+// while the MMAs of tile t+1 proceed.
+// With a tensor map for C (C rows 16-byte aligned, no row limit) the C tile
+// moves in two halves of 64 columns, each with one 2-D TMA load and one TMA
+// store: the load of a half of the next tile starts as soon as the store of
+// that half of this tile has read the buffer, so C streams continuously.
+// Otherwise (plain mode) the epilogue reads and writes C in global memory.
+// Barriers:
+//   full/empty[s]    operand stage s loaded / consumed by the MMAs
+//   accf/acce[a]     accumulator a complete / read out by the epilogue
+//   cfull/cempty[h]  C half h loaded / written back (its buffer free)
 // Every wait is bounded; a role that gives up raises s_abort, the others stop
 // at their next check or time out, copies in flight and issued MMAs are
 // waited for (bounded) and the tensor memory is freed.
 constexpr int PT_THREADS = 192;
+constexpr int CH = TN / 2;  // columns of a C half
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *tm, int x, int y, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(tm), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap *tm, int x, int y, const void *src)
+{
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(tm), "r"(x),
+                 "r"(y), "r"(smem_u32(src))
+                 : "memory");
+}
 
 __global__ void __launch_bounds__(PT_THREADS, 1)
     tc_gemm_p(int M, int N, int KT, int NTt, int ntiles, float alpha, const float *Ahi, const float *Alo,
-              const float *Bhi, const float *Blo, float beta, float *C, long ldc, int ctma, const int *lim,
-              DevStatus *st)
+              const float *Bhi, const float *Blo, float beta, float *C, long ldc, int use_tm,
+              const __grid_constant__ CUtensorMap tmC, const int *lim, DevStatus *st)
 {
     if (lim) M = min(M, *lim);
     extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
-    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], accf[2], acce[2], cfull, cempty, done;
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], accf[2], acce[2], cfull[2], cempty[2], done;
     __shared__ uint32_t s_tmem;
     __shared__ volatile int s_abort;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     float *stage = (float *)(tc_smem_raw + ((1024u - (smem_u32(tc_smem_raw) & 1023u)) & 1023u));
-    float *Cbuf = stage + (long)STAGES * 4 * IMG;  // TM x TN
+    float *Cbuf = stage + (long)STAGES * 4 * IMG;  // [2][TM][CH]: the two C halves
     float *sbuf = Cbuf + TM * TN;                  // 4 x 32 x 33 epilogue staging
-    const bool cload = ctma && beta != 0.f;
+    const bool cload = use_tm && beta != 0.f;
     const int ntl = (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;  // tiles of this CTA
 
     if (warp == 0) {
@@ -375,9 +402,9 @@ __global__ void __launch_bounds__(PT_THREADS, 1)
         for (int k = 0; k < 2; k++) {
             mbar_init(&accf[k], 1);
             mbar_init(&acce[k], 1);
+            mbar_init(&cfull[k], 1);
+            mbar_init(&cempty[k], 1);
         }
-        mbar_init(&cfull, 1);
-        mbar_init(&cempty, 1);
         mbar_init(&done, 1);
         mbar_init_fence();
         s_abort = 0;
@@ -409,23 +436,24 @@ __global__ void __launch_bounds__(PT_THREADS, 1)
                 tma_load_1d(dst + 3 * IMG, Blo + bbase + ko, IMG * 4u, &full[sidx]);
             }
             if (!ok) { s_abort = 1; break; }
-            // the C tile of this tile, once the epilogue of the previous one has
-            // written its tile back (the operands of the next tile are already
-            // on their way)
+            // the C halves of this tile, each once the epilogue has written the
+            // same half of the previous tile back (the box always moves its
+            // full size: rows and columns outside C read as zero)
             if (cload) {
-                if (lt > 0 && !mbar_wait_bounded(&cempty, (lt - 1) & 1, st, 610)) { s_abort = 1; break; }
-                const int m0 = mt * TM, n0 = nt * TN;
-                const int nrows = max(0, min(TM, M - m0)), ncols = min(TN, N - n0);
-                mbar_expect_tx(&cfull, (uint32_t)(nrows * ncols * 4));
-                for (int r = 0; r < nrows; r++)
-                    tma_load_1d(Cbuf + r * TN, C + (long)(m0 + r) * ldc + n0, (uint32_t)(ncols * 4), &cfull);
+                for (int h = 0; h < 2 && ok; h++) {
+                    if (lt > 0 && !mbar_wait_bounded(&cempty[h], (lt - 1) & 1, st, 610)) { ok = false; break; }
+                    mbar_expect_tx(&cfull[h], (uint32_t)(TM * CH * 4));
+                    tma_load_2d(Cbuf + h * TM * CH, &tmC, nt * TN + h * CH, mt * TM, &cfull[h]);
+                }
+                if (!ok) { s_abort = 1; break; }
                 cl++;
             }
         }
         // copies in flight land before the CTA exits: the last use of each stage
         for (int j = max(0, it - STAGES); j < it; j++)
             mbar_wait_bounded(&full[j % STAGES], (j / STAGES) & 1, st, 612, 1000000000LL);
-        if (cl > 0) mbar_wait_bounded(&cfull, (cl - 1) & 1, st, 613, 1000000000LL);
+        if (cl > 0)
+            for (int h = 0; h < 2; h++) mbar_wait_bounded(&cfull[h], (cl - 1) & 1, st, 613, 1000000000LL);
     } else if (warp == 1 && lane == 0) {
         // ------------------------------------------------ MMA issuer
         int it = 0;
@@ -458,59 +486,78 @@ __global__ void __launch_bounds__(PT_THREADS, 1)
         mbar_wait_bounded(&done, 0, st, 622);
     } else if (warp >= 2) {
         // ------------------------------------------------ epilogue (warps 2-5)
-        const int q = warp & 3;          // TMEM lane quarter of this warp: rows 32q..32q+31
+        const int q = warp & 3;  // TMEM lane quarter of this warp: rows 32q..32q+31
         const int ew = warp - 2;
         float(*sb)[33] = reinterpret_cast<float(*)[33]>(sbuf + ew * 32 * 33);
         for (int lt = 0; lt < ntl; lt++) {
             const int ab = lt & 1;
-            bool ok = mbar_wait_bounded(&accf[ab], (lt >> 1) & 1, st, 630);
-            if (ok && cload) ok = mbar_wait_bounded(&cfull, lt & 1, st, 631);
+            const bool ok = mbar_wait_bounded(&accf[ab], (lt >> 1) & 1, st, 630);
             if (bar_or(1, 128, !ok || s_abort)) { s_abort = 1; break; }  // the same decision in every warp
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int t = blockIdx.x + lt * gridDim.x, mt = t / NTt, nt = t % NTt;
             const int m0 = mt * TM, n0 = nt * TN;
             const int nrows = min(TM, M - m0), ncols = min(TN, N - n0);
             const uint32_t taddr = tmem + (uint32_t)(ab * TN) + ((uint32_t)(q * 32) << 16);
+            bool abort = false;
+            for (int h = 0; h < 2; h++) {
+                float *Ch = Cbuf + h * TM * CH;
+                if (use_tm) {
+                    bool okc = true;
+                    if (cload) okc = mbar_wait_bounded(&cfull[h], lt & 1, st, 631);
+                    if (bar_or(1, 128, !okc || s_abort)) { abort = true; break; }
+                }
 #pragma unroll 1
-            for (int c0 = 0; c0 < TN; c0 += 32) {
-                uint32_t v[32];
-                tmem_ld32(taddr + (uint32_t)c0, v);
+                for (int c0 = h * CH; c0 < (h + 1) * CH; c0 += 32) {
+                    uint32_t v[32];
+                    tmem_ld32(taddr + (uint32_t)c0, v);
 #pragma unroll
-                for (int k = 0; k < 32; k++) sb[lane][k] = __uint_as_float(v[k]);
-                __syncwarp();
-                const int cl = c0 + lane;
-                if (cl < ncols) {
+                    for (int k = 0; k < 32; k++) sb[lane][k] = __uint_as_float(v[k]);
+                    __syncwarp();
+                    const int cl = c0 + lane;
+                    if (use_tm) {
+                        // the whole box goes back; TMA drops what lies outside C
+                        const int cc = cl - h * CH;
 #pragma unroll 4
-                    for (int rr = 0; rr < 32; rr++) {
-                        const int rl = q * 32 + rr;
-                        if (rl >= nrows) break;
-                        float x = alpha * sb[rr][lane];
-                        if (ctma) {
-                            if (cload) x = fmaf(beta, Cbuf[rl * TN + cl], x);
-                            Cbuf[rl * TN + cl] = x;
-                        } else {
+                        for (int rr = 0; rr < 32; rr++) {
+                            const int rl = q * 32 + rr;
+                            float x = alpha * sb[rr][lane];
+                            if (cload) x = fmaf(beta, Ch[rl * CH + cc], x);
+                            Ch[rl * CH + cc] = x;
+                        }
+                    } else if (cl < ncols) {
+#pragma unroll 4
+                        for (int rr = 0; rr < 32; rr++) {
+                            const int rl = q * 32 + rr;
+                            if (rl >= nrows) break;
                             float *c = C + (long)(m0 + rl) * ldc + n0 + cl;
+                            float x = alpha * sb[rr][lane];
                             if (beta != 0.f) x = fmaf(beta, *c, x);
                             *c = x;
                         }
                     }
+                    __syncwarp();
                 }
-                __syncwarp();
-            }
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            if (ctma) proxy_async_fence();  // Cbuf writes visible to the bulk stores
-            bar_or(1, 128, false);          // every warp has read the accumulator and written Cbuf
-            if (ew == 0 && lane == 0) mbar_arrive(&acce[ab]);
-            if (ctma) {
-                if (ew == 0) {
-                    for (int r = lane; r < nrows; r += 32)
-                        tma_store_1d(C + (long)(m0 + r) * ldc + n0, Cbuf + r * TN, (uint32_t)(ncols * 4));
-                    tma_store_commit_and_drain();
+                if (h == 1) {
+                    // the accumulator is read out: the MMAs of tile lt+2 may use it
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    bar_or(1, 128, false);
+                    if (ew == 0 && lane == 0) mbar_arrive(&acce[ab]);
                 }
-                bar_or(1, 128, false);  // the stores have read Cbuf
-                if (cload && ew == 0 && lane == 0) mbar_arrive(&cempty);
+                if (use_tm) {
+                    proxy_async_fence();  // the half's writes visible to the TMA store
+                    bar_or(1, 128, false);
+                    if (ew == 0 && lane == 0) {
+                        tma_store_2d(&tmC, n0 + h * CH, m0, Ch);
+                        tma_store_commit_and_drain();  // the store has read the buffer
+                    }
+                    bar_or(1, 128, false);
+                    if (cload && ew == 0 && lane == 0) mbar_arrive(&cempty[h]);
+                }
             }
+            if (abort) { s_abort = 1; break; }
         }
+        // the last stores complete before the CTA exits
+        if (use_tm && ew == 0 && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -538,6 +585,32 @@ static int tc_sms()
             n = 148;
     }
     return n;
+}
+
+// Tensor map of C (FP32, M rows of N columns, row stride ldc floats) with a
+// box of one C half (TM rows x CH columns); false when the driver entry point
+// is not available or the encoding is refused.
+static bool encode_c_map(CUtensorMap *tm, float *C, int M, int N, long ldc)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
+    static int tried = 0;
+    if (!tried) {
+        tried = 1;
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            enc = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+        cudaGetLastError();
+    }
+    if (!enc) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)M};
+    const cuuint64_t strides[1] = {(cuuint64_t)ldc * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)CH, (cuuint32_t)TM};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)C, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // PACO_TC_PERSISTENT=0 keeps every product on the one-tile-per-CTA kernel
@@ -604,8 +677,11 @@ cudaError_t gemm_tc_run(int M, int N, int K, float alpha, GemmOp A, GemmOp B, fl
     if (!part && tc_persistent()) {
         const int ntiles = g.MT * g.NT;
         const int grid = std::min(ntiles, tc_sms());
+        CUtensorMap tm;
+        const int use_tm = (ctma && !lim && encode_c_map(&tm, C, M, N, ldc)) ? 1 : 0;
+        if (!use_tm) memset(&tm, 0, sizeof(tm));
         paco_count_launch(), tc_gemm_p<<<grid, PT_THREADS, tc_p_smem_bytes(), s>>>(
-                                 M, N, g.KT, g.NT, ntiles, alpha, Ahi, Alo, Bhi, Blo, beta, C, ldc, ctma, lim, st);
+                                 M, N, g.KT, g.NT, ntiles, alpha, Ahi, Alo, Bhi, Blo, beta, C, ldc, use_tm, tm, lim, st);
         return cudaGetLastError();
     }
     paco_count_launch(), tc_gemm<<<dim3(g.NT, g.MT, g.splits), 128, tc_smem_bytes(), s>>>(
