@@ -358,7 +358,8 @@ def main():
         return
     peaks, peak_kind = measured_peaks()
     rp_ms, rp_launches, rp_bytes = prof[0], prof[1], prof[2]
-    kname = ("bd_panel_pk (persistent stage-1 panel kernel: all column steps of a 32-column panel)"
+    kname = ("bd_panel_pk (persistent stage-1 panel kernel: all column steps of a 32-column panel) "
+             "and bd_tail_k (the last columns on one thread-block cluster, one launch per SVD)"
              if prof[3] == 1 else "bd_row_pass (stage-1 fused GEMV row pass)")
     # algorithmic bytes of the GEMV phase: two FP32 reads of the trailing matrix
     # per column step, 8 * sum_i (M-i)(N-i) bytes per SVD; the fused panel

@@ -732,6 +732,7 @@ void bd_init_attrs()
     cudaFuncSetAttribute(bd_row_pass<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
     cudaFuncSetAttribute(bd_build_t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(NBF * NBF * sizeof(float)));
     gemm_tc_init_attrs();
+    bd_tail_init();
     rp_attrs_set = true;
 }
 
@@ -777,7 +778,22 @@ int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, f
     cudaMemsetAsync(w.X, 0, sizeof(float) * (size_t)M * NB, s);
     paco_count_launch(), bd_copy_in<<<std::min(4096, ceil_div((long)M * w.ldw, 256)), 256, 0, s>>>(a_in, w.W, M, N, w.ldw, w.st);
 
+    // the last columns, once their block fits in a cluster's shared memory,
+    // go to the cluster kernel in one launch
+    const int tail_p = use_pk ? bd_tail_start(M, N) : N;
     for (int p0 = 0; p0 < N; p0 += NB) {
+        if (p0 == tail_p) {
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            if (g_prof.on) prof_record(e0 = prof_event(), s);
+            const bool done = bd_tail_launch(a, p0, s);
+            if (g_prof.on) {
+                prof_record(e1 = prof_event(), s);
+                g_prof.cur.ev.push_back(e0);
+                g_prof.cur.ev.push_back(e1);
+                g_prof.cur.bytes.push_back(done ? 4.0 * (double)(M - p0) * (double)(N - p0) : 0.0);
+            }
+            if (done) break;
+        }
         const int p1 = std::min(N, p0 + NB), nbp = p1 - p0;
         const int Gp = grid_rows(M - p0);
         bool pk = false;

@@ -156,6 +156,13 @@ static __device__ __forceinline__ void reduce_records(const float *rec, int ncta
 }
 
 bool bd_panel_pk_launch(const BdArgs &a, PkCtl *ctl, int p0, int p1, int G, unsigned *cnt, cudaStream_t s);
+// Cluster kernel for the last columns: its set-up (once, outside stream
+// capture), the first panel boundary p from which the block A[p:, p:] goes to
+// it (N when it never does), and that launch (false: not possible, the panels
+// continue).
+void bd_tail_init();
+int bd_tail_start(int M, int N);
+bool bd_tail_launch(const BdArgs &a, int p, cudaStream_t s);
 void bd_pk_init_attrs();
 
 size_t bd_workspace_bytes(int M, int N);
