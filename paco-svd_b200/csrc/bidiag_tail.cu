@@ -62,10 +62,12 @@ __device__ __forceinline__ uint32_t dsmem_addr(const void *local, int rank)
     return r;
 }
 
+// Ordered after the cluster barrier by that barrier's own memory clobber;
+// independent loads stay free to overlap.
 __device__ __forceinline__ float ld_dsmem(uint32_t addr)
 {
     float v;
-    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(addr) : "memory");
+    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(addr));
     return v;
 }
 
@@ -238,9 +240,14 @@ __global__ void __launch_bounds__(TT, 1) bd_tail_k(TailArgs t, int CS)
         tail_reflector(x0, sig, m - i, &beta, &tq, &v0);
         const float inv_v0 = 1.f / v0;
         for (int c = i + 1 + tid; c < w; c += TT) {
-            float S = 0.f;
-            for (int q = 0; q < CS; q++) S += ld_dsmem(dsmem_addr(sh.part + par * t.w4 + c, q));
+            // all remote loads in flight before the first add
+            float v[16];
+#pragma unroll
+            for (int q = 0; q < 16; q++) v[q] = (q < CS) ? ld_dsmem(dsmem_addr(sh.part + par * t.w4 + c, q)) : 0.f;
             const float aic = ld_dsmem(dsmem_addr(prow + c, owner));
+            float S = 0.f;
+#pragma unroll
+            for (int q = 0; q < 16; q++) S += v[q];
             const float wj = aic + inv_v0 * S;
             sh.wv[c] = wj;
             sh.rv[c] = aic - tq * wj;
