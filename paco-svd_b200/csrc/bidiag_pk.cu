@@ -79,8 +79,11 @@ __device__ bool pk_barrier(PkCtl *c, unsigned target, DevStatus *st, int where, 
 // Sums the per-CTA partial records rec[t * PCAP + cta] (cta < G <= 160) into
 // out[t] for t < nval <= 80.  Every warp issues all of its loads before the
 // first add, so the reduction costs one L2 round trip; the sum order is fixed
-// (bitwise reproducible).  Called by every thread of the CTA.
-__device__ __forceinline__ void reduce_records_fast(const float *rec, int G, int nval, float *out)
+// (bitwise reproducible).  Threads t < nbc also store bc_val into bc_dst[t]
+// before the closing barrier (a value they loaded before the call).  Called
+// by every thread of the CTA.
+__device__ __forceinline__ void reduce_records_fast(const float *rec, int G, int nval, float *out, float *bc_dst,
+                                                    float bc_val, int nbc)
 {
     constexpr int NW = RP_THREADS / 32, VPW = 5, LPV = 5;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -103,6 +106,7 @@ __device__ __forceinline__ void reduce_records_fast(const float *rec, int G, int
         sum = warp_sum(sum);
         if (lane == 0 && t < nval) out[t] = sum;
     }
+    if ((int)threadIdx.x < nbc) bc_dst[threadIdx.x] = bc_val;
     __syncthreads();
 }
 
@@ -130,7 +134,7 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
     __shared__ float cy[RP_THREADS / 32][32], cA[RP_THREADS / 32][32], cB[RP_THREADS / 32][32];
     __shared__ float s_cpart[PR];
     __shared__ int s_ok;
-    __shared__ float s_rtaup, s_rinv, s_ctau, s_cinv, s_cinv_prev;
+
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int M = a.M, N = a.N, G = gridDim.x, b = blockIdx.x;
@@ -150,11 +154,13 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
         mbar_init_fence();
-        s_cinv_prev = 1.f;
     }
     __syncthreads();
     uint32_t phase0 = 0, phase1 = 0;
     bool failed = false;
+    // 1/v0 of the previous column reflector: scales that column's entries in
+    // the next row pass (every thread holds the same value)
+    float cinv_prev = 1.f;
     // streamed rows: batches of the coming row pass already on their way
     // (issued at the end of the previous row pass, so their latency hides
     // behind the barriers and the column pass)
@@ -201,6 +207,7 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
 
         // ------------- finish the row reflector of step i-1 (every CTA)
         float4 u4[CPT], acc4[CPT];
+        float r_taup = 0.f;  // the row reflector of step i-1 (the same in every thread)
         if (doX) {
             // all loads of this phase in flight together
             const int nbc = 2 + 2 * iip;
@@ -212,18 +219,12 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
                 rb[k] = (c < ldw) ? __ldcg(reinterpret_cast<const float4 *>(a.rowbuf + c))
                                   : make_float4(0.f, 0.f, 0.f, 0.f);
             }
-            reduce_records_fast(a.cpart, G, nbc, s_red);
-            if (tid < nbc) s_bc[tid] = bcv;
-            __syncthreads();
-            if (tid == 0) {
-                float beta, tau, v0;
-                make_reflector(s_bc[0], s_red[0], N - (i - 1) - 1, &beta, &tau, &v0);
-                s_rtaup = tau;
-                s_rinv = 1.f / v0;
-                if (b == 0) { a.e[i - 1] = beta; a.taup[i - 1] = tau; a.inv_v0r[i - 1] = 1.f / v0; }
-            }
-            __syncthreads();
-            const float inv = s_rinv;
+            reduce_records_fast(a.cpart, G, nbc, s_red, s_bc, bcv, nbc);
+            // every thread forms the same reflector from the same sums
+            float beta, v0;
+            make_reflector(s_bc[0], s_red[0], N - (i - 1) - 1, &beta, &r_taup, &v0);
+            const float inv = 1.f / v0;
+            if (b == 0 && tid == 0) { a.e[i - 1] = beta; a.taup[i - 1] = r_taup; a.inv_v0r[i - 1] = inv; }
             // t3 = Y^T u (ii values), t4 = U u (iip values); next column's panel entries
             if (tid <= iip) {
                 s_t3[tid] = s_bc[1 + tid] + s_red[1 + tid] * inv;
@@ -260,8 +261,8 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
 #pragma unroll
         for (int k = 0; k < CPT; k++) acc4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
         for (int t = tid; t < PK_RMAX * PR; t += RP_THREADS) (&s_part[0][0])[t] = 0.f;
-        const float taup_prev = doX ? s_rtaup : 0.f;
-        const float invc = (ii >= 1) ? s_cinv_prev : 1.f;
+        const float taup_prev = doX ? r_taup : 0.f;
+        const float invc = (ii >= 1) ? cinv_prev : 1.f;
 
         // ------------------------------------------------------ row pass
         const int kfirst = first_active(i);
@@ -465,24 +466,19 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
             }
         }
 
-        // ------------- column reflector of step i (every CTA)
+        // ------------- column reflector of step i (every CTA, every thread)
+        float c_tau, c_inv;
         {
             const int nbc = 1 + 2 * ii;
             const float bcv = (tid < nbc) ? __ldcg(&a.bcA[tid]) : 0.f;
-            reduce_records_fast(a.tpart, G, 1 + 2 * ii, s_red);
-            if (tid < nbc) s_bc[tid] = bcv;
-            __syncthreads();
-            if (tid == 0) {
-                float beta, tau, v0;
-                make_reflector(s_bc[0], s_red[0], M - i, &beta, &tau, &v0);
-                s_ctau = tau;
-                s_cinv = 1.f / v0;
-                s_cinv_prev = 1.f / v0; // scales column i's entries in the next step
-                if (b == 0) { a.d[i] = beta; a.tauq[i] = tau; a.inv_v0c[i] = 1.f / v0; }
-            }
-            __syncthreads();
+            reduce_records_fast(a.tpart, G, 1 + 2 * ii, s_red, s_bc, bcv, nbc);
+            float beta, v0;
+            make_reflector(s_bc[0], s_red[0], M - i, &beta, &c_tau, &v0);
+            c_inv = 1.f / v0;
+            cinv_prev = c_inv;  // scales column i's entries in the next step
+            if (b == 0 && tid == 0) { a.d[i] = beta; a.tauq[i] = c_tau; a.inv_v0c[i] = c_inv; }
             if (tid < ii) {
-                const float inv = s_cinv;
+                const float inv = c_inv;
                 s_ai[tid] = s_bc[1 + tid];                                  // V[i, q] (row i panel entries)
                 s_xi[tid] = s_bc[1 + ii + tid];                             // X[i, q]
                 s_t1[tid] = s_bc[1 + tid] + s_red[1 + tid] * inv;           // V^T v
@@ -502,7 +498,7 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
         if (i >= N - 1) break; // no row reflector after the last column
 
         // --------------------------------------------------- column pass
-        const float tq = s_ctau, invc_i = s_cinv;
+        const float tq = c_tau, invc_i = c_inv;
         for (int ch = b; ch < nchunk; ch += G) {
             const int j = i + 1 + ch * 32 + lane;
             const bool valid = j < N;
