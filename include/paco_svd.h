@@ -51,12 +51,14 @@ void GenerateTiling(int N, int blockDim, uint8_t *TilingHost);
  * shape).  paco_autotune times the candidate configurations of the
  * single-matrix path on a synthetic M x N matrix (the persistent panel kernel
  * or the two-kernel row/column passes, rows per CTA of a panel, the tcgen05
- * or SIMT engine for the large products), keeps the fastest for (M, N) in a
+ * or SIMT engine for the large products, the last columns on one
+ * thread-block cluster or on the panel kernel), keeps the fastest for (M, N) in a
  * process-wide table that every later call of that shape uses, and returns
  * out[0] = chosen candidate, out[1] = its ms per SVD, out[2] = ms of the
  * defaults, out[3] = candidates tried.  It allocates its own device buffers
  * and synchronizes `stream`.  cfg[4] = {persistent (0/1), rows per CTA
- * (4..256), tcgen05 products (0/1), 0}: paco_tune_get returns the entry in
+ * (4..256), tcgen05 products (0/1), last columns kept off the cluster kernel
+ * (0/1)}: paco_tune_get returns the entry in
  * use for (M, N) (the defaults {1, 16, 1, 0} if none), paco_tune_set stores
  * one (for example a choice saved by an earlier process). */
 int paco_autotune(int M, int N, void *stream, double out[4]);

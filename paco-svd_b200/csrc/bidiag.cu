@@ -780,7 +780,7 @@ int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, f
 
     // the last columns, once their block fits in a cluster's shared memory,
     // go to the cluster kernel in one launch
-    const int tail_p = use_pk ? bd_tail_start(M, N) : N;
+    const int tail_p = (use_pk && !tune.no_tail) ? bd_tail_start(M, N) : N;
     for (int p0 = 0; p0 < N; p0 += NB) {
         if (p0 == tail_p) {
             cudaEvent_t e0 = nullptr, e1 = nullptr;

@@ -72,7 +72,7 @@ const PacoTune kTuneDefault = {1, bd::RMIN_PER_BLOCK, 1, 0};
 bool tune_valid(const PacoTune &t)
 {
     return (t.persistent == 0 || t.persistent == 1) && (t.tc == 0 || t.tc == 1) && t.rows_per_cta >= 4 &&
-           t.rows_per_cta <= 256;
+           t.rows_per_cta <= 256 && (t.no_tail == 0 || t.no_tail == 1);
 }
 
 void tune_store(int M, int N, const PacoTune &cfg)
@@ -393,14 +393,14 @@ int paco_tune_get(int M, int N, int cfg[4])
 {
     if (!cfg) return PACO_ERR_INVALID_ARG;
     const PacoTune t = paco_tune_for(M, N);
-    cfg[0] = t.persistent; cfg[1] = t.rows_per_cta; cfg[2] = t.tc; cfg[3] = 0;
+    cfg[0] = t.persistent; cfg[1] = t.rows_per_cta; cfg[2] = t.tc; cfg[3] = t.no_tail;
     return PACO_OK;
 }
 
 int paco_tune_set(int M, int N, const int cfg[4])
 {
     if (!cfg || !shape_ok(M, N)) return PACO_ERR_INVALID_ARG;
-    const PacoTune t = {cfg[0], cfg[1], cfg[2], 0};
+    const PacoTune t = {cfg[0], cfg[1], cfg[2], cfg[3]};
     if (!tune_valid(t)) return PACO_ERR_INVALID_ARG;
     tune_store(M, N, t);
     return PACO_OK;
@@ -425,9 +425,10 @@ int paco_autotune(int M, int N, void *stream, double out[4])
     err = err ? err : cudaEventCreate(&e1);
     int rc = err ? PACO_ERR_CUDA : PACO_OK;
     // candidates: the defaults first, then fewer / more rows per CTA, the
-    // SIMT engine for the large products, the two-kernel row/column passes
+    // SIMT engine for the large products, the two-kernel row/column passes,
+    // the last columns on the panel kernel
     const PacoTune cands[] = {{1, bd::RMIN_PER_BLOCK, 1, 0}, {1, 8, 1, 0}, {1, 32, 1, 0}, {1, bd::RMIN_PER_BLOCK, 0, 0},
-                              {0, bd::RMIN_PER_BLOCK, 1, 0}};
+                              {0, bd::RMIN_PER_BLOCK, 1, 0}, {1, bd::RMIN_PER_BLOCK, 1, 1}};
     const int nc = (int)(sizeof(cands) / sizeof(cands[0]));
     float best = 1e30f, tdef = 0.f;
     int bi = 0;

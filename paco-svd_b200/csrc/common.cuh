@@ -77,9 +77,10 @@ void paco_count_launch();
 // output, paco_autotune): the persistent panel kernel or the two-kernel row /
 // column passes, rows per CTA of a panel (sets the grid: fewer CTAs meet at
 // each barrier, more CTAs stream more bandwidth), and whether the large
-// products use the tcgen05 GEMM.
+// products use the tcgen05 GEMM, and whether the last columns stay on the
+// panel kernel instead of the cluster kernel (no_tail = 1).
 struct PacoTune {
-    int persistent, rows_per_cta, tc, pad;
+    int persistent, rows_per_cta, tc, no_tail;
 };
 PacoTune paco_tune_for(int M, int N);
 

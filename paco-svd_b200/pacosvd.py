@@ -236,7 +236,7 @@ def svd(A, check=True):
 
 TUNE_CANDIDATES = ["persistent, 16 rows/CTA, tcgen05", "persistent, 8 rows/CTA, tcgen05",
                    "persistent, 32 rows/CTA, tcgen05", "persistent, 16 rows/CTA, SIMT products",
-                   "row/column passes, 16 rows/CTA, tcgen05"]
+                   "row/column passes, 16 rows/CTA, tcgen05", "persistent, 16 rows/CTA, tcgen05, no cluster tail"]
 
 
 def autotune(M: int, N: int, stream=None) -> dict:

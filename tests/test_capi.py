@@ -139,8 +139,10 @@ def test_tune_table_defaults_and_round_trip():
     assert P.tune_get(300, 200) == [1, 16, 1, 0]
     P.tune_set(301, 201, [1, 32, 0, 0])
     assert P.tune_get(301, 201) == [1, 32, 0, 0]
+    P.tune_set(301, 201, [1, 16, 1, 1])                # last columns kept on the panel kernel
+    assert P.tune_get(301, 201) == [1, 16, 1, 1]
     assert P.tune_get(300, 200) == [1, 16, 1, 0]     # other shapes keep the defaults
-    for bad in ([2, 16, 1, 0], [1, 2, 1, 0], [1, 16, 3, 0], [1, 1000, 1, 0]):
+    for bad in ([2, 16, 1, 0], [1, 2, 1, 0], [1, 16, 3, 0], [1, 1000, 1, 0], [1, 16, 1, 2]):
         with pytest.raises(P.PacoError):
             P.tune_set(301, 201, bad)
     with pytest.raises(P.PacoError):

@@ -26,7 +26,8 @@ def test_autotune_picks_a_candidate_and_keeps_it():
     assert r["config"] == P.tune_get(1100, 1030)
 
 
-@pytest.mark.parametrize("cfg", [[1, 16, 1, 0], [1, 8, 1, 0], [1, 32, 1, 0], [1, 16, 0, 0], [0, 16, 1, 0]])
+@pytest.mark.parametrize("cfg", [[1, 16, 1, 0], [1, 8, 1, 0], [1, 32, 1, 0], [1, 16, 0, 0], [0, 16, 1, 0],
+                                 [1, 16, 1, 1]])
 def test_every_candidate_is_correct(cfg):
     M, N = 1100, 1030
     P.tune_set(M, N, cfg)

@@ -131,6 +131,24 @@ def test_svd_streamed_panels_match_lapack_and_repeat_bitwise():
     check_svd(A_np, s, U, Vt, O.lapack_dgesdd_sigma(A_np))
 
 
+@pytest.mark.parametrize("shape", [(65, 33), (300, 200), (900, 777), (1300, 800)])
+def test_cluster_tail_and_panel_kernel_both_match_lapack(shape):
+    # the last columns of stage 1 run on one thread-block cluster when their
+    # block fits in its shared memory (all of these shapes, from column 0 or
+    # later), or on the grid-wide panel kernel (tuning entry no_tail = 1)
+    M, N = shape
+    rng = np.random.default_rng(M + 3 * N)
+    A = rng.standard_normal((M, N)).astype(np.float32)
+    ref = O.lapack_dgesdd_sigma(A)
+    try:
+        for no_tail in (0, 1):
+            P.tune_set(M, N, [1, 16, 1, no_tail])
+            s, U, Vt = run_svd(A)
+            check_svd(A, s, U, Vt, ref)
+    finally:
+        P.tune_set(M, N, [1, 16, 1, 0])
+
+
 def test_results_are_bitwise_deterministic():
     rng = np.random.default_rng(5)
     A = torch.from_numpy(rng.standard_normal((300, 200)).astype(np.float32)).cuda()
