@@ -170,6 +170,28 @@ def batched_shapes(wl, seed):
     return out
 
 
+def batched_accuracy(As, Us, Vts, sigmas):
+    """Worst sigma error (against FP64 LAPACK dgesdd of the FP32 input),
+    residual ||A - U S Vt||_F / ||A||_F and orthogonality ||Q^T Q - I||_F over
+    a sample of batched results (numpy arrays, FP64 on the host)."""
+    import scipy.linalg
+    worst = {"sigma_err": 0.0, "residual": 0.0, "orth_U": 0.0, "orth_V": 0.0, "max_N": 0}
+    for A, U, Vt, s in zip(As, Us, Vts, sigmas):
+        A, U, Vt, s = (np.asarray(x, np.float64) for x in (A, U, Vt, s))
+        n = A.shape[1]
+        ref = scipy.linalg.svd(A, compute_uv=False, lapack_driver="gesdd")
+        r = {"sigma_err": float(np.max(np.abs(s - ref)) / max(ref[0], np.finfo(float).tiny)),
+             "residual": float(np.linalg.norm(A - (U[:, :n] * s[None, :]) @ Vt) / max(np.linalg.norm(A), 1e-300)),
+             "orth_U": float(np.linalg.norm(U.T @ U - np.eye(U.shape[1]))),
+             "orth_V": float(np.linalg.norm(Vt @ Vt.T - np.eye(n)))}
+        for k, v in r.items():
+            worst[k] = max(worst[k], v)
+        worst["max_N"] = max(worst["max_N"], n)
+    worst["matrices"] = len(As)
+    worst["tolerance"] = {"sigma_err": 1e-5, "residual_and_orth": "1e-5 * N of each matrix"}
+    return worst
+
+
 def cpu_baseline_batched(wl, nsample=30):
     """Oracle port (FP64 C restatement, 1 thread) on `nsample` matrices drawn
     from the batch's size distribution: SVDs/s of that sample."""
@@ -452,6 +474,12 @@ def run_batched(args, wl, rank, world, local, dist):
     lib.paco_debug_batched_timing(0)
     clk = clocks.stop()
     total_ms = max_over_ranks(sum(a.elapsed_time(c) for a, c in ev), dist)
+    # accuracy of the last timed call on 40 matrices spread over the batch (outside the timing)
+    acc = None
+    if rank == 0:
+        pick = list(range(0, count, max(1, count // 40)))[:40]
+        acc = batched_accuracy([b.A[k].cpu().numpy() for k in pick], [b.U[k].cpu().numpy() for k in pick],
+                               [b.Vt[k].cpu().numpy() for k in pick], [b.sigma[k].cpu().numpy() for k in pick])
 
     # end to end: host (pinned) inputs in, host outputs back, every step
     e2e = None
@@ -517,7 +545,7 @@ def run_batched(args, wl, rank, world, local, dist):
                          "alg_bytes_definition": "sum over matrices of 8*sum_i (M-i)(N-i)",
                          "kernel_ms": {"bt_bidiag_k": k1, "bt_bdc_k": ksum[1] / steps, "bt_apply_k": ksum[2] / steps},
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)"},
-            "clocks": clk, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clk, "e2e": e2e, "gpu_launches": int(launches), "accuracy": acc,
             "plain_single_matrix": plain,
             "batched_over_plain": (value / world / plain["value"]) if plain else None}
     if not args.no_cpu_baseline and world == 1:
