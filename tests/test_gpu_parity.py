@@ -1,7 +1,7 @@
 """GPU parity tests: the CUDA library (through its C ABI) against the oracle
 and the LAPACK goldens.
 
-Tolerances (BASELINE north star, FP32 outputs, Frobenius norms):
+Tolerances (FP32 outputs, Frobenius norms):
   sigma:          max_i |s_i - s_ref_i| / s_ref_1            <= 1e-5
   residual:       ||A - U[:, :N] S Vt||_F / ||A||_F          <= 1e-5 * N
   orthogonality:  ||U^T U - I||_F, ||V^T V - I||_F           <= 1e-5 * N
