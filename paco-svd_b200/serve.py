@@ -67,10 +67,14 @@ class SvdServer:
         self.small_max = small_max
         self.device = device
         # a pool of streams per class, so small batches never wait for a free
-        # stream behind long-running large ones
+        # stream behind long-running large ones; the small class's streams
+        # have the higher priority, so its CTAs take the SMs that large
+        # matrices free first
         if isinstance(max_inflight, int):
             max_inflight = (max_inflight, max_inflight)
-        self.streams = [[torch.cuda.Stream() for _ in range(n)] for n in max_inflight]
+        # (a lower number is a higher priority; torch maps it into the device's range)
+        self.streams = [[torch.cuda.Stream(priority=(-8 if cls == 0 else 0)) for _ in range(n)]
+                        for cls, n in enumerate(max_inflight)]
         self.busy = [[None] * n for n in max_inflight]
         self.waiting = collections.deque()      # arrived, not yet admitted
         self.pending = [collections.deque(), collections.deque()]  # admitted, by class (small, large)
