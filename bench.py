@@ -225,6 +225,32 @@ def cpu_baseline(wl, steps=1):
                       f"({t:.2f} s), scaled by the M*N^2 work ratio {scale:.1f}"}
 
 
+def cpu_lapack(wl, n=1024, steps=2):
+    """LAPACK sgesdd (numpy's OpenBLAS, every host thread it uses) on an n-column
+    sample with the workload's aspect ratio, full U as the C ABI returns it,
+    scaled to the workload's SVDs/s by the M*N^2 work ratio: the golden the
+    reference's own checker compares with, timed beside the GPU."""
+    n = min(n, wl["N"])
+    A = make_matrix(dict(M=n * wl["M"] // wl["N"], N=n, gen=wl["gen"]), seed=98)
+    threads = os.cpu_count() or 1
+    try:
+        import threadpoolctl
+        threads = max([i.get("num_threads", 0) for i in threadpoolctl.threadpool_info()
+                       if i.get("internal_api") == "openblas"] or [threads])
+    except Exception:
+        pass
+    times = []
+    for _ in range(max(1, steps)):
+        t = time.perf_counter()
+        np.linalg.svd(A, full_matrices=True)
+        times.append(time.perf_counter() - t)
+    t = min(times)
+    scale = (wl["M"] * wl["N"] ** 2) / (A.shape[0] * A.shape[1] ** 2)
+    return {"value": 1.0 / (t * scale), "unit": "SVDs/s", "cores": int(threads), "kind": "lapack sgesdd",
+            "sample": f"numpy.linalg.svd (OpenBLAS sgesdd, FP32) on a {A.shape[0]}x{A.shape[1]} {wl['gen']} "
+                      f"matrix, best of {len(times)} ({t:.2f} s), scaled by the M*N^2 work ratio {scale:.1f}"}
+
+
 def run_reference(args, wl, rank):
     if rank != 0:
         return
@@ -419,6 +445,7 @@ def main():
             "gpu_launches": int(launches)}
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(wl)
+        line["cpu_lapack"] = cpu_lapack(wl)
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
