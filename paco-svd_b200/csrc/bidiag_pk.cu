@@ -249,9 +249,16 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
             }
             // the scaled row reflector goes into row i-1 of W (later column passes
             // and the panel's trailing update read it)
+            // (from the row values this thread already holds: no second read)
             if (b == 0) {
-                for (int j = i + 1 + tid; j < N; j += RP_THREADS)
-                    a.W[(long)(i - 1) * ldw + j] = __ldcg(&a.rowbuf[j]) * inv;
+#pragma unroll
+                for (int k = 0; k < CPT; k++) {
+                    const int c = p0 + 4 * (tid + k * RP_THREADS);
+                    const float r[4] = {rb[k].x, rb[k].y, rb[k].z, rb[k].w};
+#pragma unroll
+                    for (int e = 0; e < 4; e++)
+                        if (c + e > i && c + e < N) a.W[(long)(i - 1) * ldw + c + e] = r[e] * inv;
+                }
                 if (xonly && tid == 0) a.W[(long)(i - 1) * ldw + i] = 1.f;
             }
         } else {
