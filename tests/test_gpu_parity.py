@@ -212,3 +212,11 @@ def test_svd_main_cli_writes_reference_files(tmp_path):
     U = np.fromfile(tmp_path / "output" / "U.bin", np.float32).reshape(M, M).astype(np.float64)
     Vt = np.fromfile(tmp_path / "output" / "Vt.bin", np.float32).reshape(N, N).astype(np.float64)
     check_svd(A, s, U, Vt, GOLD["cfg1"]["sigma_d"])
+    # and the reference's own checker on those files (scripts/verify_svd.py:35-65,102-104):
+    # orthogonality and sigma with rtol 1e-3 / atol 1e-5, reconstruction max-abs <= 1e-3
+    assert np.allclose(U @ U.T, np.eye(M), rtol=1e-3, atol=1e-5)
+    assert np.allclose(Vt @ Vt.T, np.eye(N), rtol=1e-3, atol=1e-5)
+    assert np.allclose(s, GOLD["cfg1"]["sigma_s"], rtol=1e-3, atol=1e-5)
+    S = np.zeros((M, N))
+    S[np.arange(N), np.arange(N)] = s
+    assert np.max(np.abs(U @ S @ Vt - A)) <= 1e-3
