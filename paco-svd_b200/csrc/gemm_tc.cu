@@ -695,7 +695,7 @@ cudaError_t gemm_tc_run(int M, int N, int K, float alpha, GemmOp A, GemmOp B, fl
 
 // Products below this many multiply-adds stay on the SIMT engine: the packing
 // passes and the 3 MMAs per k-step do not pay for themselves there.
-static constexpr double TC_MIN_MACS = (double)(1 << 26);
+static constexpr double TC_MIN_MACS = (double)(1 << 24);
 
 static bool tc_shape_ok(int M, int N, int K)
 {
