@@ -1,21 +1,26 @@
 #!/usr/bin/env python
-"""Benchmark of the B200 SVD (libpacosvd.so) on the plain FP32 single-matrix
-workload: M = N = 4096, entries iid N(0,1) from a seed (config 2a of the
-reference's benchmark plan), synthetic data.
+"""Benchmark of the B200 SVD (libpacosvd.so).  The default workload is the
+precision-form configuration: one 8192 x 4096 FP32 matrix whose spectrum is
+512 clusters of 8 singular values (centres log-uniform in [1e-4, 1],
+relative spacing 1e-7 inside a cluster), A = Q1 diag(sigma) Q2^T with
+Haar-random Q1, Q2 from a seed; synthetic data.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload cfg2a|cfg2b|cfg1|cfg3]
+                  [--workload cfg3|cfg2a|cfg2b|cfg1|cfg4|cfg5]
 
 A step is one full SVD (stage 1 bidiagonalization + U/Vt formation, stage 2
 divide and conquer + final products) of a matrix already resident in HBM.
 Metric: SVDs/s (whole job).  One process per GPU; the SVD does not shard, so
 N > 1 runs independent replicas (weak scaling) and takes the max time over
 ranks.  Between timed steps a 512 MiB buffer is written to flush L2.
+Accuracy of the last step is reported against FP64 LAPACK dgesdd of the FP32
+input (computed on the host, outside the timed region).
 
-`--impl reference` times the reference algorithm on the host CPU: the
-reference itself is Ascend C for a Huawei NPU and cannot be built here, so
-this is the FP64 C restatement in oracle/ (single-threaded), on a bounded
-sample matrix scaled to the workload by the O(n^3) operation count.
+`--impl reference` times the reference's CPU path: the reference itself is
+Ascend C for a Huawei NPU and cannot be built here, so its CPU path is the
+LAPACK golden its own checker compares with (scripts/verify_svd.py:89,
+numpy.linalg.svd = sgesdd in FP32 with the full U, on every host thread),
+run on the full workload matrix at every step.
 """
 from __future__ import annotations
 
@@ -35,43 +40,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "paco-svd_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-WORKLOADS = {
-    "cfg2a": dict(M=4096, N=4096, gen="normal"),
-    "cfg2b": dict(M=4096, N=4096, gen="graded"),
-    "cfg1": dict(M=64, N=32, gen="uniform"),
-    "cfg3": dict(M=8192, N=4096, gen="clustered"),
-    # batched form: 10,000 matrices, M uniform on [32, 512], N uniform on [16, M], iid N(0,1)
-    "cfg4": dict(kind="batched", count=10000, Mlo=32, Mhi=512, Nlo=16, gen="normal"),
-    # serving form: Poisson requests at 2,000/s for 60 s, 90% M log-uniform on [16, 256], 10% on
-    # [256, 2048], N uniform on [M/4, M], 20% graded spectra, 64 GB device working-set cap
-    "cfg5": dict(kind="serving", rate=2000.0, seconds=60.0, cap_gb=64),
-}
+from workloads import WORKLOADS, batched_shapes, make_matrix  # noqa: E402
+
 CPU_SAMPLE_N = 768  # oracle sample size (about 5 s of single-thread work)
-
-
-def make_matrix(wl, seed=1234, with_sigma=False):
-    """The workload's seeded matrix; with_sigma also returns its exact
-    singular values (descending) for the generators that construct them."""
-    M, N, gen = wl["M"], wl["N"], wl["gen"]
-    rng = np.random.default_rng(seed)
-    if gen == "uniform":
-        A = rng.uniform(-1, 1, (M, N)).astype(np.float32)
-        return (A, None) if with_sigma else A
-    if gen == "normal":
-        A = rng.standard_normal((M, N), dtype=np.float32)
-        return (A, None) if with_sigma else A
-
-    def haar(n, m):
-        Q, R = np.linalg.qr(rng.standard_normal((n, m)))
-        return Q * np.sign(np.diag(R))[None, :]
-
-    if gen == "graded":
-        sig = 10.0 ** (-6 * np.arange(N) / (N - 1))
-    else:  # 512 clusters of 8, centres log-uniform in [1e-4, 1], spacing 1e-7
-        centres = 10.0 ** rng.uniform(-4, 0, N // 8)
-        sig = np.sort((centres[:, None] * (1 + 1e-7 * np.arange(8))[None, :]).ravel())[::-1]
-    A = ((haar(M, N) * sig[None, :]) @ haar(N, N).T).astype(np.float32)
-    return (A, np.sort(sig)[::-1].copy()) if with_sigma else A
 
 
 class ClockSampler:
@@ -161,15 +132,6 @@ def whole_job_value(world, steps, total_ms):
     return world * steps / (total_ms / 1000.0)
 
 
-def batched_shapes(wl, seed):
-    rng = np.random.default_rng(seed)
-    out = []
-    for _ in range(wl["count"]):
-        M = int(rng.integers(wl["Mlo"], wl["Mhi"] + 1))
-        out.append((M, int(rng.integers(wl["Nlo"], M + 1))))
-    return out
-
-
 def batched_accuracy(As, Us, Vts, sigmas):
     """Worst sigma error (against FP64 LAPACK dgesdd of the FP32 input),
     residual ||A - U S Vt||_F / ||A||_F and orthogonality ||Q^T Q - I||_F over
@@ -207,9 +169,11 @@ def cpu_baseline_batched(wl, nsample=30):
                       f"({t:.1f} s)"}
 
 
-def cpu_baseline(wl, steps=1):
-    """Oracle port (FP64 C restatement, 1 thread) on a CPU_SAMPLE_N^2 sample,
-    scaled to the workload's SVDs/s by the n^3 work ratio."""
+def cpu_oracle(wl, steps=1):
+    """Oracle port (FP64 C restatement of the reference algorithm, 1 thread)
+    on a CPU_SAMPLE_N-column sample with the workload's aspect ratio, scaled
+    to the workload's SVDs/s by the M*N^2 work ratio.  A side figure only:
+    the measured CPU baseline is lapack_svd_timed on the full matrix."""
     import oracle
     n = min(CPU_SAMPLE_N, wl["N"])
     A = make_matrix(dict(M=n * wl["M"] // wl["N"], N=n, gen=wl["gen"]), seed=99)
@@ -222,16 +186,11 @@ def cpu_baseline(wl, steps=1):
     scale = (wl["M"] * wl["N"] ** 2) / (A.shape[0] * A.shape[1] ** 2)
     return {"value": 1.0 / (t * scale), "unit": "SVDs/s", "cores": 1, "kind": "port",
             "sample": f"oracle.svd on a {A.shape[0]}x{A.shape[1]} {wl['gen']} matrix, median of {len(times)} "
-                      f"({t:.2f} s), scaled by the M*N^2 work ratio {scale:.1f}"}
+                      f"({t:.2f} s), scaled by the M*N^2 work ratio {scale:.1f} (extrapolated; not the baseline)"}
 
 
-def cpu_lapack(wl, n=1024, steps=2):
-    """LAPACK sgesdd (numpy's OpenBLAS, every host thread it uses) on an n-column
-    sample with the workload's aspect ratio, full U as the C ABI returns it,
-    scaled to the workload's SVDs/s by the M*N^2 work ratio: the golden the
-    reference's own checker compares with, timed beside the GPU."""
-    n = min(n, wl["N"])
-    A = make_matrix(dict(M=n * wl["M"] // wl["N"], N=n, gen=wl["gen"]), seed=98)
+def host_threads():
+    """Threads numpy's OpenBLAS runs LAPACK on (all host cores unless limited)."""
     threads = os.cpu_count() or 1
     try:
         import threadpoolctl
@@ -239,19 +198,63 @@ def cpu_lapack(wl, n=1024, steps=2):
                        if i.get("internal_api") == "openblas"] or [threads])
     except Exception:
         pass
+    return int(threads)
+
+
+def lapack_svd_timed(A, steps, budget_s):
+    """Times numpy.linalg.svd(A, full_matrices=True) -- LAPACK sgesdd in FP32
+    with the full M x M U, as the C ABI returns it, on every host thread --
+    on the whole matrix: `steps` calls, or as many as fit in budget_s (at
+    least one).  Returns the seconds of each call."""
     times = []
+    t_all = time.perf_counter()
     for _ in range(max(1, steps)):
         t = time.perf_counter()
         np.linalg.svd(A, full_matrices=True)
         times.append(time.perf_counter() - t)
-    t = min(times)
-    scale = (wl["M"] * wl["N"] ** 2) / (A.shape[0] * A.shape[1] ** 2)
-    return {"value": 1.0 / (t * scale), "unit": "SVDs/s", "cores": int(threads), "kind": "lapack sgesdd",
-            "sample": f"numpy.linalg.svd (OpenBLAS sgesdd, FP32) on a {A.shape[0]}x{A.shape[1]} {wl['gen']} "
-                      f"matrix, best of {len(times)} ({t:.2f} s), scaled by the M*N^2 work ratio {scale:.1f}"}
+        if time.perf_counter() - t_all + times[-1] > budget_s:
+            break
+    return times
+
+
+def cpu_baseline(wl, A):
+    """The reference's CPU path (the LAPACK golden, sgesdd) on the workload's
+    own full matrix, one call, every host thread."""
+    times = lapack_svd_timed(A, 1, 0.0)
+    t = times[0]
+    return {"value": 1.0 / t, "unit": "SVDs/s", "cores": host_threads(), "kind": "lapack sgesdd",
+            "sample": f"numpy.linalg.svd (OpenBLAS sgesdd, FP32, full U) on the workload's own "
+                      f"{A.shape[0]}x{A.shape[1]} matrix, 1 call ({t:.2f} s)"}
+
+
+def dgesdd_sigma(A):
+    """Singular values of the FP32 matrix A by FP64 LAPACK dgesdd (the
+    oracle of scripts/verify_svd.py:89, in double precision)."""
+    import scipy.linalg
+    return scipy.linalg.svd(np.asarray(A, np.float64), compute_uv=False, lapack_driver="gesdd")
+
+
+def single_config(name, wl):
+    """`config` of a single-matrix workload, the same in both arms."""
+    return {"workload": f"{name}: {wl['M']}x{wl['N']} FP32 {wl['gen']}, one full SVD per step (sigma, U {wl['M']}x"
+                        f"{wl['M']}, Vt {wl['N']}x{wl['N']})",
+            "M": wl["M"], "N": wl["N"], "l2": "a 512 MiB buffer is written between timed GPU steps (L2 flush)"}
+
+
+def batched_config(name, wl):
+    """`config` of the batched workload, the same in both arms."""
+    return {"workload": f"{name}: {wl['count']} FP32 N(0,1) matrices, M uniform on [{wl['Mlo']}, {wl['Mhi']}], "
+                        f"N uniform on [{wl['Nlo']}, M], the whole batch per step",
+            "count": wl["count"], "l2": "a 512 MiB buffer is written between timed GPU steps (L2 flush)"}
+
+
+REF_BUDGET_S = 150.0  # timed CPU work of one reference-arm run
 
 
 def run_reference(args, wl, rank):
+    """The reference arm: its CPU path (LAPACK sgesdd, FP32, full U, every
+    host thread) on the same workload, timed on the host.  Under torchrun
+    only rank 0 runs; the other ranks exit without work."""
     if rank != 0:
         return
     batched = wl.get("kind") == "batched"
@@ -259,16 +262,44 @@ def run_reference(args, wl, rank):
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving mode; its CPU "
                           "algorithm is timed per matrix by the batched and single-matrix workloads"}))
         return
-    cb = cpu_baseline_batched(wl) if batched else cpu_baseline(wl, steps=args.steps)
-    line = {"metric": "SVDs/sec", "value": cb["value"], "unit": "SVDs/s", "impl": "reference",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1000.0 / cb["value"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": (f"{args.workload}: {wl['count']} FP32 N(0,1) matrices, M in [{wl['Mlo']}, "
-                                    f"{wl['Mhi']}], N in [{wl['Nlo']}, M], batched SVD") if batched else
-                                   f"{args.workload}: {wl['M']}x{wl['N']} FP32 {wl['gen']}, plain single-matrix SVD"},
-            "cpu_baseline": cb,
-            "e2e": {"value": cb["value"], "unit": "SVDs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    threads = host_threads()
+    if batched:
+        # the batch's own shapes in order, N(0,1) entries, as many matrices as fit in the budget
+        shapes = batched_shapes(wl, 4321)
+        rng = np.random.default_rng(1234)
+        np.linalg.svd(rng.standard_normal((64, 32)).astype(np.float32))  # thread pool start-up
+        done, t0 = 0, time.perf_counter()
+        for M, N in shapes[: wl["count"]]:
+            np.linalg.svd(rng.standard_normal((M, N), dtype=np.float32), full_matrices=True)
+            done += 1
+            if time.perf_counter() - t0 > min(REF_BUDGET_S, 60.0):
+                break
+        t = time.perf_counter() - t0
+        value = done / t
+        sample = (f"numpy.linalg.svd (OpenBLAS sgesdd, FP32, full U) on the first {done} of the batch's "
+                  f"{wl['count']} shapes (N(0,1), {t:.1f} s)")
+        steps_done = 1
+        ms = 1000.0 * wl["count"] / value
+        config = batched_config(args.workload, wl)
+        value_unit = value
+    else:
+        A = make_matrix(wl, seed=1234)
+        warm = lapack_svd_timed(A, 1, 0.0) if args.warmup > 0 else []
+        times = lapack_svd_timed(A, args.steps, REF_BUDGET_S)
+        steps_done = len(times)
+        ms = 1000.0 * statistics.mean(times)
+        value_unit = 1000.0 / ms
+        sample = (f"the full {wl['M']}x{wl['N']} workload matrix at every step: numpy.linalg.svd (OpenBLAS "
+                  f"sgesdd, FP32, full U), {len(warm)} warm-up call, {steps_done} timed calls "
+                  f"(of {args.steps} requested; the run stops after {REF_BUDGET_S:.0f} s of timed work)")
+        config = single_config(args.workload, wl)
+    cb = {"value": value_unit, "unit": "SVDs/s", "cores": threads, "kind": "lapack sgesdd", "sample": sample}
+    line = {"metric": "SVDs/sec", "value": value_unit, "unit": "SVDs/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": steps_done, "steps_requested": args.steps,
+            "warmup": 0 if batched else len(warm), "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config, "parallelism": "host CPU", "cpu_baseline": cb,
+            "e2e": {"value": value_unit, "unit": "SVDs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
@@ -278,7 +309,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg2a", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="cfg3", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end measurement")
     ap.add_argument("--serve-seconds", type=float, default=None, help="length of the serving trace")
@@ -365,9 +396,10 @@ def main():
     if rc:
         raise SystemExit(f"device status {rc} ({info}) in the timed region")
 
-    # accuracy of the last step (FP64 on the device; Frobenius norms): sigma
-    # against the exact spectrum the generator built (graded, clustered), the
-    # reconstruction residual and the orthogonality of U and V
+    # accuracy of the last step (Frobenius norms): sigma against FP64 LAPACK
+    # dgesdd of the FP32 input (host) and, for the graded and clustered
+    # generators, against the exact spectrum they built; the reconstruction
+    # residual and the orthogonality of U and V in FP64 on the device
     s = W.sigma.float().cpu().numpy().astype(np.float64)
     acc = None
     if rank == 0:
@@ -378,11 +410,15 @@ def main():
         eye_m = torch.eye(M, dtype=torch.float64, device="cuda")
         eye_n = torch.eye(N, dtype=torch.float64, device="cuda")
         acc = {"residual": res, "orth_U": torch.linalg.norm(Ud.T @ Ud - eye_m).item(),
-               "orth_V": torch.linalg.norm(Vd @ Vd.T - eye_n).item(), "tolerance": 1e-5 * N,
-               "sigma_err": (float(np.max(np.abs(s - sig_exact)) / sig_exact[0]) if sig_exact is not None
-                             else None),
-               "sigma_reference": "exact spectrum of the generator" if sig_exact is not None else None}
+               "orth_V": torch.linalg.norm(Vd @ Vd.T - eye_n).item(), "tolerance": 1e-5 * N}
         del Ad, Ud, Vd, eye_m, eye_n
+        torch.cuda.empty_cache()
+        ref = dgesdd_sigma(A_host)
+        acc["sigma_err"] = float(np.max(np.abs(s - ref)) / ref[0])
+        acc["sigma_tolerance"] = 1e-5
+        acc["sigma_reference"] = "FP64 LAPACK dgesdd of the FP32 input (scipy, host)"
+        if sig_exact is not None:
+            acc["sigma_err_exact"] = float(np.max(np.abs(s - sig_exact)) / sig_exact[0])
 
     # end to end through the host-buffer C ABI (H2D of A, D2H of U, Vt, sigma)
     e2e_t = None
@@ -431,10 +467,8 @@ def main():
     line = {"metric": "SVDs/sec", "value": value, "unit": "SVDs/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{args.workload}: {M}x{N} FP32 {wl['gen']}, plain single-matrix SVD "
-                                   f"(bidiagonalization + U/Vt formation + divide and conquer)",
-                       "M": M, "N": N, "l2": "512 MiB buffer written between timed steps",
-                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+            "config": single_config(args.workload, wl),
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
             "sigma_max": float(s[0]), "sigma_min": float(s[-1]), "accuracy": acc,
             "autotune": ({"choice": tune["name"], "ms": tune["ms"], "default_ms": tune["default_ms"]}
                          if tune else None),
@@ -444,8 +478,8 @@ def main():
                     if e2e_t else None),
             "gpu_launches": int(launches)}
     if not args.no_cpu_baseline and world == 1:
-        line["cpu_baseline"] = cpu_baseline(wl)
-        line["cpu_lapack"] = cpu_lapack(wl)
+        line["cpu_baseline"] = cpu_baseline(wl, A_host)
+        line["cpu_oracle"] = cpu_oracle(wl)
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
@@ -561,10 +595,8 @@ def run_batched(args, wl, rank, world, local, dist):
     line = {"metric": "SVDs/sec", "value": value, "unit": "SVDs/s", "n_gpus": world, "steps": steps,
             "warmup": max(3, args.warmup), "ms_per_step": total_ms / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{args.workload}: {count} FP32 N(0,1) matrices, M uniform on [{wl['Mlo']}, "
-                                   f"{wl['Mhi']}], N uniform on [{wl['Nlo']}, M], one batched call per step",
-                       "count": count, "l2": "512 MiB buffer written between timed steps",
-                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+            "config": batched_config(args.workload, wl),
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
             "roofline": {"kernel": "bt_bidiag_k (batched bidiagonalization, one CTA per matrix)", "bound": "hbm",
                          "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": None,

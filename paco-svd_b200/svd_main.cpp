@@ -5,6 +5,11 @@
 //   stages on the GPU, writes ../output/sigma.bin (N floats, descending),
 //   ../output/U.bin (M x M) and ../output/Vt.bin (N x N) (main.cpp:171-174).
 // Options --args FILE, --input FILE, --output DIR override those paths.
+// --stage1 runs the bidiagonalization alone and writes ../output/U.bin
+// (M x M), ../output/B.bin (M x N, d on the diagonal, e on the superdiagonal)
+// and ../output/Vt.bin (N x N) with A = U * B * Vt: the stage-1 hook of
+// main.cpp:139-151 (commented out there) whose files scripts/verify_result.py
+// checks (verify_result.py:134-140).
 // Unlike the reference (which logs and continues, data_utils.h:41-47), any
 // failure exits with a non-zero status.
 #include <sys/stat.h>
@@ -15,6 +20,8 @@
 #include <iostream>
 #include <string>
 #include <vector>
+
+#include <cuda_runtime.h>
 
 #include "paco_svd.h"
 
@@ -48,15 +55,74 @@ static bool write_file(const std::string &path, const void *buf, size_t bytes)
     return (bool)f;
 }
 
+static bool cuda_ok(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return true;
+    std::cerr << "[ERROR] " << what << ": " << cudaGetErrorString(e) << "\n";
+    return false;
+}
+
+// Stage 1 alone on caller-allocated device buffers (the two-kernel flow of
+// main.cpp:56-128 up to the bidiagonalization), then U, B, Vt to files.
+static int run_stage1(int M, int N, std::vector<float> &A, std::vector<float> &U, std::vector<float> &Vt,
+                      const std::string &out_dir)
+{
+    size_t sz[12];
+    paco_buffer_sizes(M, N, sz);
+    float *dA = nullptr, *dU = nullptr, *dVt = nullptr, *dd = nullptr, *de = nullptr, *dtq = nullptr,
+          *dtp = nullptr;
+    void *ws = nullptr;
+    const size_t small = sizeof(float) * (size_t)(N + 1);
+    bool ok = cuda_ok(cudaMalloc(&dA, sz[1]), "cudaMalloc A") && cuda_ok(cudaMalloc(&dU, sz[0]), "cudaMalloc U") &&
+              cuda_ok(cudaMalloc(&dVt, sz[2]), "cudaMalloc Vt") && cuda_ok(cudaMalloc(&dd, small), "cudaMalloc d") &&
+              cuda_ok(cudaMalloc(&de, small), "cudaMalloc e") && cuda_ok(cudaMalloc(&dtq, small), "cudaMalloc tauq") &&
+              cuda_ok(cudaMalloc(&dtp, small), "cudaMalloc taup") &&
+              cuda_ok(cudaMalloc(&ws, sz[11]), "cudaMalloc workspace") &&
+              cuda_ok(cudaMemcpy(dA, A.data(), sz[1], cudaMemcpyHostToDevice), "copy A");
+    std::vector<float> d((size_t)N), e((size_t)N, 0.f);
+    if (ok) {
+        std::cout << "before bidiagonalization" << std::endl;
+        int rc = upper_bidiagonalization(M, N, dA, dU, dVt, dd, de, dtq, dtp, ws, nullptr);
+        int info = 0;
+        if (!rc) rc = paco_sync_status(ws, nullptr, &info);
+        if (rc) {
+            std::cerr << "[ERROR] upper_bidiagonalization failed with status " << rc << " (info " << info << ")\n";
+            ok = false;
+        } else {
+            std::cout << "finish bidiagonalization" << std::endl;
+        }
+    }
+    ok = ok && cuda_ok(cudaMemcpy(U.data(), dU, sz[0], cudaMemcpyDeviceToHost), "copy U") &&
+         cuda_ok(cudaMemcpy(Vt.data(), dVt, sz[2], cudaMemcpyDeviceToHost), "copy Vt") &&
+         cuda_ok(cudaMemcpy(d.data(), dd, sizeof(float) * N, cudaMemcpyDeviceToHost), "copy d") &&
+         (N < 2 || cuda_ok(cudaMemcpy(e.data(), de, sizeof(float) * (N - 1), cudaMemcpyDeviceToHost), "copy e"));
+    cudaFree(dA); cudaFree(dU); cudaFree(dVt); cudaFree(dd); cudaFree(de); cudaFree(dtq); cudaFree(dtp);
+    cudaFree(ws);
+    if (!ok) return 1;
+    // B (M x N): d on the diagonal, e on the superdiagonal (main.cpp:143-150)
+    std::vector<float> B((size_t)M * N, 0.f);
+    for (int i = 0; i < N; i++) {
+        B[(size_t)i * N + i] = d[i];
+        if (i + 1 < N) B[(size_t)i * N + i + 1] = e[i];
+    }
+    mkdir(out_dir.c_str(), 0755);
+    ok = write_file(out_dir + "/U.bin", U.data(), U.size() * sizeof(float)) &&
+         write_file(out_dir + "/B.bin", B.data(), B.size() * sizeof(float)) &&
+         write_file(out_dir + "/Vt.bin", Vt.data(), Vt.size() * sizeof(float));
+    return ok ? 0 : 1;
+}
+
 int main(int argc, char **argv)
 {
     std::string args_path = "../args.txt", in_path = "../input/A_gm.bin", out_dir = "../output";
-    for (int i = 1; i + 1 < argc; i += 2) {
-        if (!strcmp(argv[i], "--args")) args_path = argv[i + 1];
-        else if (!strcmp(argv[i], "--input")) in_path = argv[i + 1];
-        else if (!strcmp(argv[i], "--output")) out_dir = argv[i + 1];
+    bool stage1 = false;
+    for (int i = 1; i < argc; i++) {
+        if (!strcmp(argv[i], "--stage1")) { stage1 = true; continue; }
+        if (i + 1 < argc && !strcmp(argv[i], "--args")) args_path = argv[++i];
+        else if (i + 1 < argc && !strcmp(argv[i], "--input")) in_path = argv[++i];
+        else if (i + 1 < argc && !strcmp(argv[i], "--output")) out_dir = argv[++i];
         else {
-            std::cerr << "usage: svd_main [--args FILE] [--input FILE] [--output DIR]\n";
+            std::cerr << "usage: svd_main [--stage1] [--args FILE] [--input FILE] [--output DIR]\n";
             return 2;
         }
     }
@@ -72,6 +138,7 @@ int main(int argc, char **argv)
     }
     std::vector<float> A((size_t)M * N), U((size_t)M * M), Vt((size_t)N * N), sigma((size_t)N);
     if (!read_file(in_path, A.data(), A.size() * sizeof(float))) return 1;
+    if (stage1) return run_stage1((int)M, (int)N, A, U, Vt, out_dir);
     paco_ctx *ctx = nullptr;
     int rc = paco_ctx_create((int)M, (int)N, &ctx);
     if (rc) {

@@ -2,8 +2,9 @@
 cudaMalloc (a framework allocator owns the device memory, or the host must
 not grow its memory after start-up).  Its scratch is a device array inside
 the library, so the test checks that two calls in a row, sharing that array,
-each give the same SVD as the allocating entry point paco_svd, within the
-tolerances of the other GPU tests.  The file name sorts last so that a run
+each give the same SVD as the allocating entry point paco_svd, and singular
+values within 1e-5 * sigma_1 of FP64 LAPACK dgesdd, within the tolerances of
+the other GPU tests.  The file name sorts last so that a run
 that stops at the first failure has already run every other test."""
 import ctypes
 
@@ -52,6 +53,7 @@ def test_noalloc_matches_allocating_entry_point_twice(shapes):
         s, U, Vt = (x.cpu().numpy().astype(np.float64) for x in (s, U, Vt))
         s_ref, U_ref, Vt_ref = (x.cpu().numpy().astype(np.float64) for x in (s_ref, U_ref, Vt_ref))
         assert O.sigma_err(s, s_ref) <= SIGMA_TOL
+        assert O.sigma_err(s, O.lapack_dgesdd_sigma(A)) <= SIGMA_TOL
         assert np.max(np.abs(U[:, :N] - U_ref[:, :N])) <= tol_n(N)
         assert np.max(np.abs(Vt - Vt_ref)) <= tol_n(N)
         assert O.residual(A, U, s, Vt) <= tol_n(N)
