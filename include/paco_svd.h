@@ -129,19 +129,24 @@ void paco_ctx_destroy(paco_ctx *ctx);
  * and returns the device status of the run. */
 int paco_svd_noalloc(int M, int N, float *A, float *U, float *Vt, float *sigma, void *stream);
 
-/* Largest M (and so N) of a matrix of the batched form. */
+/* Largest M (and so N) of a matrix of the batched form's one-CTA-per-matrix
+ * kernels; larger matrices of one shape go to the multi-matrix form. */
 #define PACO_BATCH_MAX_M 2048
 
 /* Batched form (the reference runs one matrix per launch; this replaces a
  * host loop over main.cpp:126-158 for many independent small matrices).
  * Bytes of workspace paco_svd_batched needs for these shapes; 0 if a shape
- * is invalid (N < 1, M < N) or M > PACO_BATCH_MAX_M. */
+ * is invalid (N < 1, M < N), or M > PACO_BATCH_MAX_M in a list whose shapes
+ * are not all the same. */
 size_t paco_batched_workspace_size(int count, const int *M, const int *N);
 
 /* SVD of `count` independent row-major FP32 matrices in one persistent
  * launch: each CTA takes the next matrix (largest first) from a work queue
  * and runs bidiagonalization, divide and conquer and the back-transforms for
- * it.  M, N and the pointer arrays are host arrays; A[b] (M x N), U[b]
+ * it.  When every matrix has one shape with M > PACO_BATCH_MAX_M the call is
+ * paco_svd_multi (and paco_batched_workspace_size returns its workspace
+ * size); other lists with such a matrix are PACO_ERR_UNSUPPORTED.
+ * M, N and the pointer arrays are host arrays; A[b] (M x N), U[b]
  * (M x M), Vt[b] (N x N) and sigma[b] (N) are device buffers; A is read only.
  * `status` (device, count ints, may be null) receives each matrix's
  * PACO_* code.  Asynchronous on `stream`; the workspace and outputs must stay
@@ -149,6 +154,24 @@ size_t paco_batched_workspace_size(int count, const int *M, const int *N);
 int paco_svd_batched(int count, const int *M, const int *N, const float *const *A, float *const *U,
                      float *const *Vt, float *const *sigma, int *status, void *workspace, size_t ws_bytes,
                      void *stream);
+
+/* Multi-matrix form for large matrices of one shape (a host loop over
+ * main.cpp:126-158 in the reference, one matrix per launch): `count` SVDs
+ * share the GPU in groups of k.  Stage 1 of a group runs in lockstep, each
+ * persistent panel launch serving all k matrices with num_SMs / k CTAs each
+ * (the column steps are latency-bound, so k matrices take little longer than
+ * one); the divide-and-conquer runs of a group then proceed concurrently on
+ * internal streams.  A[b] is read only; U[b] (M x M), Vt[b] (N x N),
+ * sigma[b] (N) as paco_svd.  `status` (device, count ints, may be null)
+ * receives each matrix's PACO_* code when its group has finished.
+ * Asynchronous on `stream` (recorded as a CUDA graph per buffers on a
+ * capturable stream); the workspace must stay alive until it has run. */
+size_t paco_svd_multi_workspace_size(int count, int M, int N);
+int paco_svd_multi(int count, int M, int N, const float *const *A, float *const *U, float *const *Vt,
+                   float *const *sigma, int *status, void *workspace, size_t ws_bytes, void *stream);
+/* Matrices per lockstep group of paco_svd_multi (1..8; 0 = automatic, 4);
+ * returns the previous setting.  Set it before computing workspace sizes. */
+int paco_multi_group(int k);
 
 /* Library version string. */
 const char *paco_version(void);

@@ -945,6 +945,12 @@ extern "C" int paco_debug_batched_phases(const void *workspace, double out[12])
 static bool g_bt_timing = false;
 static cudaEvent_t g_bt_ev[4];
 
+// Sets this unit's secular iteration limit (a test hook; synchronous).
+void bt_set_sec_maxit(int n)
+{
+    cudaMemcpyToSymbol(g_sec_maxit, &n, sizeof(int));
+}
+
 extern "C" void paco_debug_batched_timing(int on)
 {
     if (on && !g_bt_timing)
@@ -995,8 +1001,20 @@ static cudaError_t bt_copy_items(void *dst, const void *src, size_t bytes, cudaS
     return err;
 }
 
+// Matrices larger than PACO_BATCH_MAX_M go to the multi-matrix form
+// (paco_svd_multi), which takes one shape: true when every matrix of the list
+// has the shape of the first and it is larger than that limit.
+static bool bt_route_multi(int count, const int *M, const int *N)
+{
+    if (count < 1 || !M || !N || M[0] <= PACO_BATCH_MAX_M) return false;
+    for (int b = 1; b < count; b++)
+        if (M[b] != M[0] || N[b] != N[0]) return false;
+    return true;
+}
+
 size_t paco_batched_workspace_size(int count, const int *M, const int *N)
 {
+    if (bt_route_multi(count, M, N)) return paco_svd_multi_workspace_size(count, M[0], N[0]);
     BtPlan p;
     return bt_plan(count, M, N, &p) ? p.total : 0;
 }
@@ -1005,6 +1023,8 @@ int paco_svd_batched(int count, const int *M, const int *N, const float *const *
                      float *const *Vt, float *const *sigma, int *status, void *workspace, size_t ws_bytes,
                      void *stream)
 {
+    if (bt_route_multi(count, M, N))
+        return paco_svd_multi(count, M[0], N[0], A, U, Vt, sigma, status, workspace, ws_bytes, stream);
     BtPlan p;
     if (!bt_plan(count, M, N, &p)) {
         for (int b = 0; b < count && M && N; b++)

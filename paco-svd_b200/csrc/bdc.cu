@@ -174,6 +174,12 @@ size_t bdc_workspace_bytes(int M, int N)
 
 static bool bdc_attrs_set = false;
 
+// Sets this unit's secular iteration limit (a test hook; synchronous).
+void bdc_set_sec_maxit(int n)
+{
+    cudaMemcpyToSymbol(g_sec_maxit, &n, sizeof(int));
+}
+
 void bdc_init_attrs()
 {
     if (!bdc_attrs_set) {

@@ -94,5 +94,9 @@ __host__ __device__ inline int leaf_partition(int N, int *starts, int *ends)
 
 size_t bdc_workspace_bytes(int M, int N);
 void bdc_init_attrs();
+// Secular-solver iteration limit of the single-matrix (bdc.cu) and batched
+// (batched.cu) kernels; a test hook that forces the non-convergence report.
+void bdc_set_sec_maxit(int n);
+void bt_set_sec_maxit(int n);
 int bdc_run(int M, int N, float *a, float *u, float *vt, float *d, float *e, float *qt, float *wt, uint32_t *idx,
             void *workspace, const uint8_t *tiling, cudaStream_t s);

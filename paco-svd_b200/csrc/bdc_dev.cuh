@@ -21,6 +21,11 @@
 #include "gemm.cuh"
 
 #define BDC_SEC_MAXIT 100
+// Iteration limit the secular solver applies (BDC_SEC_MAXIT unless a test
+// lowers it to force the non-convergence report).  Each translation unit
+// that includes this header has its own copy; bdc_set_sec_maxit (bdc.cu) and
+// bt_set_sec_maxit (batched.cu) set theirs.
+static __device__ int g_sec_maxit = BDC_SEC_MAXIT;
 #define BDC_MAX_LEVELS 32
 #define GATHER_ROWS 16
 
@@ -442,7 +447,8 @@ static __device__ void bdc_secular_dev(const LevelArgs &A, int nm, int gw, int l
     double tau = 0.5 * (tlo + thi), fprev = 1e300;
     const double di = ds[i], dn = (i + 1 < k) ? (double)ds[i + 1] : 0.0;
     bool conv = false;
-    for (int it = 0; it < BDC_SEC_MAXIT; it++) {
+    const int maxit = g_sec_maxit;
+    for (int it = 0; it < maxit; it++) {
         double p1 = 0, p2 = 0, q1 = 0, q2 = 0;
         for (int j = lane; j < k; j += G) {
             double dj = ds[j];

@@ -733,39 +733,53 @@ void bd_init_attrs()
     cudaFuncSetAttribute(bd_build_t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(NBF * NBF * sizeof(float)));
     gemm_tc_init_attrs();
     bd_tail_init();
+    bd_fork_events();
     rp_attrs_set = true;
 }
 
-int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, float *d, float *e, float *tauq,
-           float *taup, void *workspace, cudaStream_t s, int num_sms)
+// Stage 1 of k matrices of one shape (jobs[0..k)): set-up, the panels in
+// lockstep (one persistent panel launch serves every matrix, G = num_sms / k
+// CTAs each; the last columns of every matrix on its own cluster launch, on
+// side[j] when k > 1), the trailing updates, the formation of U and V.
+int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s, cudaStream_t *side, int num_sms)
 {
-    BdWs w;
-    bd_carve(workspace, M, N, &w);
+    if (k < 1 || k > PK_KMAX) return PACO_ERR_INVALID_ARG;
+    const int M = jobs[0].M, N = jobs[0].N;
+    for (int j = 1; j < k; j++)
+        if (jobs[j].M != M || jobs[j].N != N) return PACO_ERR_INVALID_ARG;
     bd_init_attrs();
     const PacoTune tune = paco_tune_for(M, N);
-    if (!tune.tc) w.tcs = nullptr;  // the large products stay on the SIMT engine
     prof_begin(s);
-    BdArgs a;
-    a.M = M; a.N = N; a.ldw = w.ldw; a.st = w.st;
-    a.W = w.W; a.Yt = w.Yt; a.X = w.X; a.ypart = w.ypart; a.tpart = w.tpart; a.cpart = w.cpart;
-    a.rowbuf = w.rowbuf; a.inv_v0c = w.inv_v0c; a.inv_v0r = w.inv_v0r; a.sc = w.sc;
-    a.d = d; a.e = e; a.tauq = tauq; a.taup = taup;
-    a.bcA = w.bcA; a.bcB = w.bcB;
-    unsigned pk_cnt = 0; // arrivals on the persistent kernel's barrier counter so far
     // PACO_PK_TRACE=<p0>: phase timestamps of the panel starting at column p0
     static int trace_env = -2;
     if (trace_env == -2) {
         const char *v = getenv("PACO_PK_TRACE");
         trace_env = v ? atoi(v) : -1;
     }
-    a.trace = (trace_env >= 0) ? w.trace : nullptr;
-    a.trace_p0 = trace_env;
+    BdWs w[PK_KMAX];
+    BdArgs a[PK_KMAX];
+    PkCtl *ctl[PK_KMAX];
+    unsigned pk_cnt[PK_KMAX]; // arrivals on each matrix's barrier counter so far
+    for (int j = 0; j < k; j++) {
+        const BdJob &J = jobs[j];
+        bd_carve(J.workspace, M, N, &w[j]);
+        if (!tune.tc) w[j].tcs = nullptr;  // the large products stay on the SIMT engine
+        BdArgs &x = a[j];
+        x.M = M; x.N = N; x.ldw = w[j].ldw; x.st = w[j].st;
+        x.W = w[j].W; x.Yt = w[j].Yt; x.X = w[j].X; x.ypart = w[j].ypart; x.tpart = w[j].tpart;
+        x.cpart = w[j].cpart; x.rowbuf = w[j].rowbuf; x.inv_v0c = w[j].inv_v0c; x.inv_v0r = w[j].inv_v0r;
+        x.sc = w[j].sc;
+        x.d = J.d; x.e = J.e; x.tauq = J.tauq; x.taup = J.taup;
+        x.bcA = w[j].bcA; x.bcB = w[j].bcB;
+        x.trace = (trace_env >= 0 && j == 0) ? w[j].trace : nullptr;
+        x.trace_p0 = trace_env;
+        ctl[j] = w[j].ctl;
+        pk_cnt[j] = 0;
+    }
 
-    const int gmax = std::max(1, std::min(RB_CAP, num_sms));
+    const int gmax = std::max(1, std::min(RB_CAP, num_sms / k));
     const int rpc = std::max(1, tune.rows_per_cta);
     auto grid_rows = [&](int rows) { return std::max(1, std::min(gmax, ceil_div(rows, rpc))); };
-    cudaMemsetAsync(w.st->counters, 0, sizeof(w.st->counters), s);
-    cudaMemsetAsync(w.ctl, 0, sizeof(PkCtl), s);
     bd_pk_init_attrs();
     // the persistent panel kernel needs every CTA co-resident (one per SM)
     static int use_pk_env = -1;
@@ -774,25 +788,54 @@ int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, f
         use_pk_env = !(v && v[0] == '0');
     }
     const bool use_pk = use_pk_env != 0 && tune.persistent;
-    cudaMemsetAsync(w.Yt, 0, sizeof(float) * NB * w.ldw, s);
-    cudaMemsetAsync(w.X, 0, sizeof(float) * (size_t)M * NB, s);
-    paco_count_launch(), bd_copy_in<<<std::min(4096, ceil_div((long)M * w.ldw, 256)), 256, 0, s>>>(a_in, w.W, M, N, w.ldw, w.st);
+    for (int j = 0; j < k; j++) {
+        cudaMemsetAsync(w[j].st->counters, 0, sizeof(w[j].st->counters), s);
+        cudaMemsetAsync(w[j].ctl, 0, sizeof(PkCtl), s);
+        cudaMemsetAsync(w[j].Yt, 0, sizeof(float) * NB * w[j].ldw, s);
+        cudaMemsetAsync(w[j].X, 0, sizeof(float) * (size_t)M * NB, s);
+        paco_count_launch(), bd_copy_in<<<std::min(4096, ceil_div((long)M * w[j].ldw, 256)), 256, 0, s>>>(
+            jobs[j].a_in, w[j].W, M, N, w[j].ldw, w[j].st);
+    }
+    // fork / join of the side streams (k > 1)
+    cudaEvent_t *fe = bd_fork_events();
+    auto fork = [&]() {
+        cudaEventRecord(fe[0], s);
+        for (int j = 0; j < k; j++) cudaStreamWaitEvent(side[j], fe[0], 0);
+    };
+    auto join = [&]() {
+        for (int j = 0; j < k; j++) {
+            cudaEventRecord(fe[1 + j], side[j]);
+            cudaStreamWaitEvent(s, fe[1 + j], 0);
+        }
+    };
 
     // the last columns, once their block fits in a cluster's shared memory,
-    // go to the cluster kernel in one launch
+    // go to the cluster kernel in one launch per matrix
     const int tail_p = (use_pk && !tune.no_tail) ? bd_tail_start(M, N) : N;
     for (int p0 = 0; p0 < N; p0 += NB) {
         if (p0 == tail_p) {
             cudaEvent_t e0 = nullptr, e1 = nullptr;
             if (g_prof.on) prof_record(e0 = prof_event(), s);
-            const bool done = bd_tail_launch(a, p0, s);
+            int ran = 0;
+            if (k == 1) {
+                ran = bd_tail_launch(a[0], p0, s) ? 1 : 0;
+            } else {
+                fork();
+                for (int j = 0; j < k; j++) ran += bd_tail_launch(a[j], p0, side[j]) ? 1 : 0;
+                join();
+            }
+            const bool done = ran == k;
             if (g_prof.on) {
                 prof_record(e1 = prof_event(), s);
                 g_prof.cur.ev.push_back(e0);
                 g_prof.cur.ev.push_back(e1);
-                g_prof.cur.bytes.push_back(done ? 4.0 * (double)(M - p0) * (double)(N - p0) : 0.0);
+                g_prof.cur.bytes.push_back(done ? 4.0 * k * (double)(M - p0) * (double)(N - p0) : 0.0);
             }
             if (done) break;
+            // a cluster launch that could not run leaves its matrix untouched, so
+            // when none ran the panels simply go on; some but not all cannot
+            // happen for one shape unless a launch failed
+            if (ran > 0) return PACO_ERR_CUDA;
         }
         const int p1 = std::min(N, p0 + NB), nbp = p1 - p0;
         const int Gp = grid_rows(M - p0);
@@ -800,57 +843,85 @@ int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, f
         if (use_pk) {
             cudaEvent_t e0 = nullptr, e1 = nullptr;
             if (g_prof.on) prof_record(e0 = prof_event(), s);
-            pk = bd_panel_pk_launch(a, w.ctl, p0, p1, Gp, &pk_cnt, s);
+            pk = bd_panel_pk_launch_multi(k, a, ctl, p0, p1, Gp, pk_cnt, s);
             if (g_prof.on) {
                 prof_record(e1 = prof_event(), s);
                 g_prof.cur.ev.push_back(e0);
                 g_prof.cur.ev.push_back(e1);
-                g_prof.cur.bytes.push_back(pk_alg_bytes(M, N, p0, p1, Gp, w.ldw));
+                g_prof.cur.bytes.push_back(k * pk_alg_bytes(M, N, p0, p1, Gp, w[0].ldw));
                 g_prof.kind = 1;
             }
         }
-        if (!pk) {
-            for (int i = p0; i < p1; i++) {
-                int G = grid_rows(M - i);
-                int mode = RP_DO_COL | ((i > p0) ? RP_DO_X : 0);
-                rp(a, i, p0, mode, G, s);
-                if (i < N - 1) paco_count_launch(), bd_col_pass<<<ceil_div(N - i - 1, 32), CP_THREADS, 0, s>>>(a, i, p0, G);
+        for (int j = 0; j < k; j++) {
+            if (!pk) {
+                for (int i = p0; i < p1; i++) {
+                    int G = grid_rows(M - i);
+                    int mode = RP_DO_COL | ((i > p0) ? RP_DO_X : 0);
+                    rp(a[j], i, p0, mode, G, s);
+                    if (i < N - 1)
+                        paco_count_launch(), bd_col_pass<<<ceil_div(N - i - 1, 32), CP_THREADS, 0, s>>>(a[j], i, p0, G);
+                }
             }
-        }
-        if (p1 < N) {
-            if (!pk) rp(a, p1, p0, RP_DO_X | RP_PANEL_END, grid_rows(M - p1), s);
-            // A[p1:, p1:] -= [V | X] [Y^T ; U]
-            GemmOp A = gop(w.W + (long)p1 * w.ldw + p0, w.ldw, 1);
-            A.p2 = w.X + (long)p1 * NB; A.rs2 = NB; A.cs2 = 1; A.ksplit = nbp;
-            GemmOp B = gop(w.Yt + p1, w.ldw, 1);
-            B.p2 = w.W + (long)p0 * w.ldw + p1; B.rs2 = w.ldw; B.cs2 = 1; B.ksplit = nbp;
-            gemm_any(M - p1, N - p1, 2 * nbp, -1.f, A, B, 1.f, w.W + (long)p1 * w.ldw + p1, w.ldw, 1, nullptr, w.tcs,
-                     w.tcs_floats, w.st, s);
-        } else if (M > N) {
-            paco_count_launch(), bd_scale_last_col<<<std::min(1024, ceil_div(M - N, 256)), 256, 0, s>>>(w.W, w.ldw, M, N, w.inv_v0c);
+            if (p1 < N) {
+                if (!pk) rp(a[j], p1, p0, RP_DO_X | RP_PANEL_END, grid_rows(M - p1), s);
+                // A[p1:, p1:] -= [V | X] [Y^T ; U]
+                const BdWs &x = w[j];
+                GemmOp A = gop(x.W + (long)p1 * x.ldw + p0, x.ldw, 1);
+                A.p2 = x.X + (long)p1 * NB; A.rs2 = NB; A.cs2 = 1; A.ksplit = nbp;
+                GemmOp B = gop(x.Yt + p1, x.ldw, 1);
+                B.p2 = x.W + (long)p0 * x.ldw + p1; B.rs2 = x.ldw; B.cs2 = 1; B.ksplit = nbp;
+                gemm_any(M - p1, N - p1, 2 * nbp, -1.f, A, B, 1.f, x.W + (long)p1 * x.ldw + p1, x.ldw, 1, nullptr,
+                         x.tcs, x.tcs_floats, x.st, s);
+            } else if (M > N) {
+                paco_count_launch(), bd_scale_last_col<<<std::min(1024, ceil_div(M - N, 256)), 256, 0, s>>>(
+                    w[j].W, w[j].ldw, M, N, w[j].inv_v0c);
+            }
         }
     }
 
-    // U = H_0 ... H_{N-1} (backward accumulation of the column reflectors,
-    // NBF reflectors per block update)
-    paco_count_launch(), bd_set_identity<<<std::min(8192, ceil_div((long)M * M, 256)), 256, 0, s>>>(u, M, M);
-    for (int p0 = ((N - 1) / NBF) * NBF; p0 >= 0; p0 -= NBF) {
-        int nbp = std::min(N, p0 + NBF) - p0, Lp = M - p0;
-        paco_count_launch(), bd_panel_vectors<<<std::min(4096, ceil_div((long)Lp * NBF, 256)), 256, 0, s>>>(
-            w.W, w.ldw, p0, nbp, Lp, 0, w.Vp);
-        apply_block_reflector(w, u, M, p0, Lp, nbp, tauq + p0, s);
+    for (int j = 0; j < k; j++) {
+        const BdWs &x = w[j];
+        const BdJob &J = jobs[j];
+        // U = H_0 ... H_{N-1} (backward accumulation of the column reflectors,
+        // NBF reflectors per block update)
+        paco_count_launch(), bd_set_identity<<<std::min(8192, ceil_div((long)M * M, 256)), 256, 0, s>>>(J.u, M, M);
+        for (int p0 = ((N - 1) / NBF) * NBF; p0 >= 0; p0 -= NBF) {
+            int nbp = std::min(N, p0 + NBF) - p0, Lp = M - p0;
+            paco_count_launch(), bd_panel_vectors<<<std::min(4096, ceil_div((long)Lp * NBF, 256)), 256, 0, s>>>(
+                x.W, x.ldw, p0, nbp, Lp, 0, x.Vp);
+            apply_block_reflector(x, J.u, M, p0, Lp, nbp, J.tauq + p0, s);
+        }
+        // V = G_0 ... G_{N-2} (row reflectors), then Vt = V^T
+        paco_count_launch(), bd_set_identity<<<std::min(8192, ceil_div((long)N * N, 256)), 256, 0, s>>>(x.Vtmp, N, N);
+        for (int p0 = ((N - 1) / NBF) * NBF; p0 >= 0; p0 -= NBF) {
+            int nbp = std::min(N - 1, p0 + NBF) - p0, Lp = N - p0 - 1;
+            if (nbp <= 0 || Lp <= 0) continue;
+            paco_count_launch(), bd_panel_vectors<<<std::min(4096, ceil_div((long)Lp * NBF, 256)), 256, 0, s>>>(
+                x.W, x.ldw, p0, nbp, Lp, 1, x.Vp);
+            apply_block_reflector(x, x.Vtmp, N, p0 + 1, Lp, nbp, J.taup + p0, s);
+        }
+        paco_count_launch(), bd_transpose<<<dim3(ceil_div(N, 32), ceil_div(N, 32)), dim3(32, 8), 0, s>>>(x.Vtmp, J.vt, N);
     }
-    // V = G_0 ... G_{N-2} (row reflectors), then Vt = V^T
-    paco_count_launch(), bd_set_identity<<<std::min(8192, ceil_div((long)N * N, 256)), 256, 0, s>>>(w.Vtmp, N, N);
-    for (int p0 = ((N - 1) / NBF) * NBF; p0 >= 0; p0 -= NBF) {
-        int nbp = std::min(N - 1, p0 + NBF) - p0, Lp = N - p0 - 1;
-        if (nbp <= 0 || Lp <= 0) continue;
-        paco_count_launch(), bd_panel_vectors<<<std::min(4096, ceil_div((long)Lp * NBF, 256)), 256, 0, s>>>(
-            w.W, w.ldw, p0, nbp, Lp, 1, w.Vp);
-        apply_block_reflector(w, w.Vtmp, N, p0 + 1, Lp, nbp, taup + p0, s);
-    }
-    paco_count_launch(), bd_transpose<<<dim3(ceil_div(N, 32), ceil_div(N, 32)), dim3(32, 8), 0, s>>>(w.Vtmp, vt, N);
     prof_end();
-    paco_count_launch(), bd_copy_out<<<std::min(4096, ceil_div((long)M * N, 256)), 256, 0, s>>>(a_out, w.W, M, N, w.ldw, d, e);
+    for (int j = 0; j < k; j++)
+        paco_count_launch(), bd_copy_out<<<std::min(4096, ceil_div((long)M * N, 256)), 256, 0, s>>>(
+            jobs[j].a_out, w[j].W, M, N, w[j].ldw, jobs[j].d, jobs[j].e);
     return cudaGetLastError() == cudaSuccess ? PACO_OK : PACO_ERR_CUDA;
+}
+
+int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, float *d, float *e, float *tauq,
+           float *taup, void *workspace, cudaStream_t s, int num_sms)
+{
+    BdJob job = {M, N, a_in, a_out, u, vt, d, e, tauq, taup, workspace};
+    return bd_run_multi(1, &job, s, nullptr, num_sms);
+}
+
+// Events of the fork / join of the side streams: created once (outside any
+// stream capture, by bd_init_attrs), reused by every call.
+cudaEvent_t *bd_fork_events()
+{
+    static cudaEvent_t ev[1 + PK_KMAX] = {};
+    if (!ev[0])
+        for (auto &e : ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    return ev;
 }

@@ -47,6 +47,16 @@ struct BdArgs {
     float *bcA, *bcB; // broadcast slots of the persistent kernel's reflectors
 };
 
+// Arguments of one launch of the persistent panel kernel: the same panel of
+// up to PK_KMAX matrices of one shape, G CTAs (and one barrier) per matrix.
+constexpr int PK_KMAX = 8;
+struct PkMulti {
+    BdArgs a[PK_KMAX];
+    PkCtl *ctl[PK_KMAX];
+    unsigned cnt_base[PK_KMAX];  // barrier counter of each matrix before the launch
+    int G;
+};
+
 struct BdWs {
     DevStatus *st;
     long ldw;
@@ -156,6 +166,11 @@ static __device__ __forceinline__ void reduce_records(const float *rec, int ncta
 }
 
 bool bd_panel_pk_launch(const BdArgs &a, PkCtl *ctl, int p0, int p1, int G, unsigned *cnt, cudaStream_t s);
+bool bd_panel_pk_launch_multi(int k, const BdArgs *a, PkCtl *const *ctl, int p0, int p1, int G, unsigned *cnt,
+                              cudaStream_t s);
+// Test hook: a cooperative launch of G CTAs whose grid barrier never
+// completes; its bounded waits give up after max_cycles.
+bool bd_pk_debug_timeout(PkCtl *ctl, DevStatus *st, int G, long long max_cycles, cudaStream_t s);
 // Cluster kernel for the last columns: its set-up (once, outside stream
 // capture), the first panel boundary p from which the block A[p:, p:] goes to
 // it (N when it never does), and that launch (false: not possible, the panels
@@ -171,5 +186,18 @@ void bd_profile_read(double out[4]);
 int bd_profile_last_graph_run();
 void bd_profile_replayed(int id);
 void bd_init_attrs();
+// One matrix of a stage-1 run.
+struct BdJob {
+    int M, N;
+    const float *a_in;
+    float *a_out, *u, *vt, *d, *e, *tauq, *taup;
+    void *workspace;
+};
+// Stage 1 of k <= PK_KMAX matrices of one shape, the panels of all of them in
+// lockstep (one persistent panel launch per panel serves every matrix); the
+// cluster launches of their last columns run on side[0..k) (k > 1).
+int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s, cudaStream_t *side, int num_sms);
+// Fork/join events of the side streams (1 + PK_KMAX), created on first use.
+cudaEvent_t *bd_fork_events();
 int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, float *d, float *e, float *tauq,
            float *taup, void *workspace, cudaStream_t s, int num_sms);

@@ -24,6 +24,8 @@
 // per panel instead of once per step; otherwise they are re-staged with TMA
 // bulk copies at every step (double-buffered).  Data other CTAs wrote earlier
 // in the same launch is read with ld.global.cg (L2), never from L1.
+#include <cstring>
+
 #include "bidiag.cuh"
 #include "tma.cuh"
 
@@ -53,7 +55,8 @@ __device__ __forceinline__ void red_release_add(unsigned *p, unsigned v)
 // Arrive at a grid barrier and wait (bounded) until `target` arrivals.  The
 // arrival is a release (it publishes every write the CTA made before the
 // __syncthreads) and the poll an acquire, so no further fences are needed.
-__device__ bool pk_barrier(PkCtl *c, unsigned target, DevStatus *st, int where, int *s_ok)
+__device__ bool pk_barrier(PkCtl *c, unsigned target, DevStatus *st, int where, int *s_ok,
+                           long long max_cycles = 4000000000LL)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -62,7 +65,7 @@ __device__ bool pk_barrier(PkCtl *c, unsigned target, DevStatus *st, int where, 
         long long t0 = clock64();
         while (ld_acquire(&c->cnt) < target) {
             if (ld_acquire(&c->abort)) { ok = 0; break; }
-            if (clock64() - t0 > 4000000000LL) {
+            if (clock64() - t0 > max_cycles) {
                 atomicAdd(&st->wait_timeouts, 1);
                 dev_fail(st, PACO_ERR_TIMEOUT, where);
                 atomicExch(&c->abort, 1u);
@@ -121,8 +124,13 @@ constexpr int PK_XOWN = 64;
 // RB: rows per row-pass batch the unrolled loops cover (R <= RB).
 template <int CPT, int RB>
 __global__ void __launch_bounds__(RP_THREADS, 1)
-    bd_panel_pk(BdArgs a, PkCtl *ctl, int p0, int p1, int resident, int R, unsigned cnt_base)
+    bd_panel_pk(const __grid_constant__ PkMulti pm, int p0, int p1, int resident, int R)
 {
+    // CTAs [j*G, (j+1)*G) run the panel of matrix j with their own barrier
+    const int mi = blockIdx.x / pm.G;
+    const BdArgs &a = pm.a[mi];
+    PkCtl *const ctl = pm.ctl[mi];
+    const unsigned cnt_base = pm.cnt_base[mi];
     extern __shared__ __align__(128) float tiles[];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ float red[RP_THREADS / 32][PK_RMAX];
@@ -137,7 +145,7 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
 
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int M = a.M, N = a.N, G = gridDim.x, b = blockIdx.x;
+    const int M = a.M, N = a.N, G = pm.G, b = blockIdx.x - mi * pm.G;
     const long ldw = a.ldw;
     const int L = (int)(ldw - p0);
     DevStatus *st = a.st;
@@ -597,14 +605,17 @@ static unsigned pk_barriers(int N, int p0, int p1)
     return (unsigned)(2 * nbp - (p1 == N ? 1 : 0));
 }
 
-// Host side: launches the persistent kernel for panel [p0, p1) cooperatively.
-// *cnt is the arrival counter's value before the launch; it is advanced by
-// the arrivals this launch makes.  Returns false when a cooperative launch of
-// G CTAs is not possible.
-bool bd_panel_pk_launch(const BdArgs &a, PkCtl *ctl, int p0, int p1, int G, unsigned *cnt, cudaStream_t s)
+// Host side: launches the persistent kernel for panel [p0, p1) of k matrices
+// of one shape cooperatively, G CTAs per matrix.  cnt[j] is matrix j's
+// arrival counter value before the launch; it is advanced by the arrivals
+// this launch makes.  Returns false when a cooperative launch of k * G CTAs
+// is not possible.
+bool bd_panel_pk_launch_multi(int k, const BdArgs *a, PkCtl *const *ctl, int p0, int p1, int G, unsigned *cnt,
+                              cudaStream_t s)
 {
-    const int L = (int)(a.ldw - p0);
-    const int own = (a.M - p0 + G - 1) / G;
+    if (k < 1 || k > PK_KMAX) return false;
+    const int L = (int)(a[0].ldw - p0);
+    const int own = (a[0].M - p0 + G - 1) / G;
     const long budget = 200 * 1024;
     int resident = ((long)own * L * 4 <= budget) ? 1 : 0;
     int R = std::max(1, std::min(RMAX, (int)(budget / (2L * L * 4))));
@@ -617,16 +628,44 @@ bool bd_panel_pk_launch(const BdArgs &a, PkCtl *ctl, int p0, int p1, int G, unsi
                                                                                  : (void *)bd_panel_pk<4, PK_RMAX>;
     else fn = chunks <= 1 ? (void *)bd_panel_pk<1, RMAX> : chunks == 2 ? (void *)bd_panel_pk<2, RMAX>
                                                                        : (void *)bd_panel_pk<4, RMAX>;
-    BdArgs aa = a;
-    unsigned base = *cnt;
-    void *args[] = {&aa, &ctl, &p0, &p1, &resident, &R, &base};
+    PkMulti pm;
+    memset(&pm, 0, sizeof(pm));
+    pm.G = G;
+    for (int j = 0; j < k; j++) {
+        pm.a[j] = a[j];
+        pm.ctl[j] = ctl[j];
+        pm.cnt_base[j] = cnt[j];
+    }
+    void *args[] = {&pm, &p0, &p1, &resident, &R};
     paco_count_launch();
-    if (cudaLaunchCooperativeKernel(fn, dim3(G), dim3(RP_THREADS), args, smem, s) != cudaSuccess) {
+    if (cudaLaunchCooperativeKernel(fn, dim3(k * G), dim3(RP_THREADS), args, smem, s) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
-    *cnt = base + pk_barriers(a.N, p0, p1) * (unsigned)G;
+    for (int j = 0; j < k; j++) cnt[j] += pk_barriers(a[j].N, p0, p1) * (unsigned)G;
     return true;
+}
+
+bool bd_panel_pk_launch(const BdArgs &a, PkCtl *ctl, int p0, int p1, int G, unsigned *cnt, cudaStream_t s)
+{
+    return bd_panel_pk_launch_multi(1, &a, &ctl, p0, p1, G, cnt, s);
+}
+
+// Test hook: every CTA of a cooperative grid arrives at a grid barrier whose
+// target (one arrival more than the grid has) is never reached; the waits
+// give up after max_cycles, record PACO_ERR_TIMEOUT and raise the abort flag.
+__global__ void pk_dbg_barrier_timeout(PkCtl *ctl, DevStatus *st, long long max_cycles)
+{
+    __shared__ int s_ok;
+    pk_barrier(ctl, gridDim.x + 1, st, 999, &s_ok, max_cycles);
+}
+
+bool bd_pk_debug_timeout(PkCtl *ctl, DevStatus *st, int G, long long max_cycles, cudaStream_t s)
+{
+    if (cudaMemsetAsync(ctl, 0, sizeof(PkCtl), s) != cudaSuccess) return false;
+    void *args[] = {&ctl, &st, &max_cycles};
+    paco_count_launch();
+    return cudaLaunchCooperativeKernel((void *)pk_dbg_barrier_timeout, dim3(G), dim3(64), args, 0, s) == cudaSuccess;
 }
 
 void bd_pk_init_attrs()

@@ -187,6 +187,42 @@ int paco_debug_bd_layout(int M, int N, size_t out[24])
     return 24;
 }
 
+// Test hook (not part of the public header): makes a bounded device-side
+// wait run out and returns the status the library reports for it.
+//   which 0: a tcgen05 kernel's mbarrier wait (one CTA holding tensor memory)
+//   which 1: the persistent panel kernel's grid barrier (cooperative grid of
+//            `ctas` CTAs whose barrier target is never reached)
+// The waits give up after max_cycles SM cycles.  `ws` holds at least
+// paco_debug_timeout_ws_bytes() bytes of device memory.  Synchronous.
+size_t paco_debug_timeout_ws_bytes(void) { return 512 + sizeof(PkCtl); }
+
+int paco_debug_wait_timeout(int which, long long max_cycles, int ctas, void *ws, void *stream)
+{
+    if (!ws || max_cycles <= 0 || (which != 0 && which != 1) || ctas < 1 || ctas > device_sms())
+        return PACO_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    DevStatus *st = (DevStatus *)ws;
+    PkCtl *ctl = (PkCtl *)((char *)ws + 512);
+    if (cudaMemsetAsync(st, 0, sizeof(DevStatus), s) != cudaSuccess) return PACO_ERR_CUDA;
+    const bool ok = which == 0 ? gemm_tc_debug_timeout(st, max_cycles, s)
+                               : bd_pk_debug_timeout(ctl, st, ctas, max_cycles, s);
+    if (!ok) {
+        cudaGetLastError();
+        return PACO_ERR_CUDA;
+    }
+    return paco_sync_status(ws, stream, nullptr);
+}
+
+// Test hook (not part of the public header): the iteration limit of the
+// secular-equation solver (100 unless lowered; values below 1 restore it),
+// for the single-matrix and the batched form.  Synchronous.
+void paco_debug_secular_maxit(int n)
+{
+    if (n < 1) n = 100;
+    bdc_set_sec_maxit(n);
+    bt_set_sec_maxit(n);
+}
+
 const char *paco_version(void) { return "paco-svd-b200 1.0 (sm_100a)"; }
 
 void paco_profile_enable(int on)
@@ -301,21 +337,25 @@ static int svd_direct(int M, int N, float *A, float *U, float *Vt, float *sigma,
                   b + L.ws, nullptr, stream);
 }
 
-// The one-shot path issues thousands of small launches per SVD; on a
-// capturable stream it is recorded once into a CUDA graph per (shape,
-// buffers, stream) and replayed with a single cudaGraphLaunch afterwards.
-// PACO_GRAPHS=0 in the environment turns this off.
+// The one-shot paths issue thousands of small launches per SVD; on a
+// capturable stream a call is recorded once into a CUDA graph per key (shape,
+// buffers, stream, tuning generation, profiling state) and replayed with a
+// single cudaGraphLaunch afterwards.  PACO_GRAPHS=0 in the environment turns
+// this off.  The cache is shared by host threads under a lock.
+}  // extern "C"
+
 namespace {
 struct GraphEntry {
-    int M, N, prof;
-    unsigned tune_gen;  // autotuner generation the graph was recorded under
-    void *A, *U, *Vt, *sigma, *ws;
+    std::vector<uintptr_t> key;
     cudaStream_t s;
+    int prof;
+    unsigned tune_gen;  // autotuner generation the graph was recorded under
     cudaGraphExec_t exec;
     int prof_run;
     unsigned long long kernels; // kernel launches recorded into the graph
 };
 std::vector<GraphEntry> g_graphs;
+std::mutex g_graphs_mu;
 bool graphs_enabled()
 {
     static int on = -1;
@@ -325,23 +365,19 @@ bool graphs_enabled()
     }
     return on != 0;
 }
-}  // namespace
 
-int paco_svd(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws, size_t ws_bytes, void *stream)
+// Runs direct() (which enqueues the work on s and returns a PACO_* status)
+// through the graph cache.
+template <class F>
+int run_cached(const std::vector<uintptr_t> &key, cudaStream_t s, F &&direct)
 {
-    if (!shape_ok(M, N)) return (N >= 1 && M >= N) ? PACO_ERR_UNSUPPORTED : PACO_ERR_INVALID_ARG;
-    if (!A || !U || !Vt || !sigma || !ws) return PACO_ERR_INVALID_ARG;
-    SvdLayout L = svd_layout(M, N);
-    if (ws_bytes < L.total) return PACO_ERR_INVALID_ARG;
-    char *b = (char *)ws;
-    cudaStream_t s = (cudaStream_t)stream;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (!graphs_enabled() || s == nullptr || s == cudaStreamLegacy || s == cudaStreamPerThread ||
         cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
-        return svd_direct(M, N, A, U, Vt, sigma, b, L, stream);
+        return direct();
+    std::lock_guard<std::mutex> lock(g_graphs_mu);
     for (GraphEntry &g : g_graphs) {
-        if (g.M == M && g.N == N && g.A == A && g.U == U && g.Vt == Vt && g.sigma == sigma && g.ws == ws &&
-            g.s == s && g.prof == g_prof_on && g.tune_gen == g_tune_gen) {
+        if (g.key == key && g.s == s && g.prof == g_prof_on && g.tune_gen == g_tune_gen) {
             if (cudaGraphLaunch(g.exec, s) != cudaSuccess) return PACO_ERR_CUDA;
             bd_profile_replayed(g.prof_run);
             g_launches += g.kernels;
@@ -352,10 +388,10 @@ int paco_svd(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws
     bdc_init_attrs();
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         cudaGetLastError();
-        return svd_direct(M, N, A, U, Vt, sigma, b, L, stream);
+        return direct();
     }
     const unsigned long long k0 = g_launches;
-    int rc = svd_direct(M, N, A, U, Vt, sigma, b, L, stream);
+    int rc = direct();
     const unsigned long long kernels = g_launches - k0;
     g_launches = k0; // recorded, not yet run
     cudaGraph_t graph = nullptr;
@@ -363,18 +399,17 @@ int paco_svd(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws
     if (rc || err != cudaSuccess || !graph) {
         if (graph) cudaGraphDestroy(graph);
         cudaGetLastError();
-        return rc ? rc : svd_direct(M, N, A, U, Vt, sigma, b, L, stream);
+        return rc ? rc : direct();
     }
     GraphEntry g;
-    g.M = M; g.N = N; g.prof = g_prof_on; g.A = A; g.U = U; g.Vt = Vt; g.sigma = sigma; g.ws = ws; g.s = s;
-    g.tune_gen = g_tune_gen;
+    g.key = key; g.s = s; g.prof = g_prof_on; g.tune_gen = g_tune_gen;
     g.prof_run = g_prof_on ? bd_profile_last_graph_run() : -1;
     g.kernels = kernels;
     err = cudaGraphInstantiate(&g.exec, graph, 0);
     cudaGraphDestroy(graph);
     if (err != cudaSuccess) {
         cudaGetLastError();
-        return svd_direct(M, N, A, U, Vt, sigma, b, L, stream);
+        return direct();
     }
     if (g_graphs.size() >= 16) {
         cudaGraphExecDestroy(g_graphs.front().exec);
@@ -385,6 +420,179 @@ int paco_svd(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws
     bd_profile_replayed(g.prof_run);
     g_launches += g.kernels;
     return PACO_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int paco_svd(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws, size_t ws_bytes, void *stream)
+{
+    if (!shape_ok(M, N)) return (N >= 1 && M >= N) ? PACO_ERR_UNSUPPORTED : PACO_ERR_INVALID_ARG;
+    if (!A || !U || !Vt || !sigma || !ws) return PACO_ERR_INVALID_ARG;
+    SvdLayout L = svd_layout(M, N);
+    if (ws_bytes < L.total) return PACO_ERR_INVALID_ARG;
+    char *b = (char *)ws;
+    const std::vector<uintptr_t> key = {1, (uintptr_t)M, (uintptr_t)N, (uintptr_t)A, (uintptr_t)U, (uintptr_t)Vt,
+                                        (uintptr_t)sigma, (uintptr_t)ws};
+    return run_cached(key, (cudaStream_t)stream, [&]() { return svd_direct(M, N, A, U, Vt, sigma, b, L, stream); });
+}
+
+// ------------------------------------------------ multi-matrix form
+// k SVDs of one large shape share the GPU: stage 1 of a group of k matrices
+// runs in lockstep (each persistent panel launch serves all k, num_sms / k
+// CTAs per matrix, so the latency of one column step is paid once for k
+// matrices), then the k divide-and-conquer runs proceed concurrently on side
+// streams.  Groups of k follow one another.  A is read only.
+}  // extern "C"
+
+namespace {
+int g_multi_k = 0;  // matrices per lockstep group; 0 = automatic
+std::mutex g_side_mu;
+cudaStream_t g_side[64][PK_KMAX];
+
+// Side streams of the current device, created once (outside stream capture).
+cudaStream_t *side_streams()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(g_side_mu);
+    if (!g_side[dev][0])
+        for (auto &st : g_side[dev])
+            if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+    return g_side[dev];
+}
+
+int multi_group(int count)
+{
+    const int k = g_multi_k > 0 ? g_multi_k : 4;
+    return std::max(1, std::min({count, k, PK_KMAX}));
+}
+
+struct MultiLayout {
+    SvdLayout L;
+    size_t a_off, per, total;
+    int k;
+};
+
+MultiLayout multi_layout(int count, int M, int N)
+{
+    MultiLayout m;
+    m.L = svd_layout(M, N);
+    m.a_off = m.L.total;  // the M x N scratch that replaces A (A stays read only)
+    m.per = (m.a_off + sizeof(float) * (size_t)M * N + 255) & ~(size_t)255;
+    m.k = multi_group(count);
+    m.total = m.per * m.k;
+    return m;
+}
+
+struct StatusPtrs {
+    DevStatus *st[PK_KMAX];
+    int idx[PK_KMAX];
+    int k;
+};
+
+// status[idx[j]] <- the PACO_* code of matrix j's run; its status block is cleared
+__global__ void multi_status_k(StatusPtrs p, int *status)
+{
+    const int j = threadIdx.x;
+    if (j >= p.k) return;
+    DevStatus *st = p.st[j];
+    int c = st->code;
+    if (!c && st->secular_nonconv) c = PACO_ERR_NONCONVERGENCE;
+    if (status) status[p.idx[j]] = c;
+    st->code = 0;
+    st->info = 0;
+    st->secular_nonconv = 0;
+    st->wait_timeouts = 0;
+}
+
+int svd_multi_direct(int count, int M, int N, const float *const *A, float *const *U, float *const *Vt,
+                     float *const *sigma, int *status, char *ws, const MultiLayout &ml, cudaStream_t s)
+{
+    cudaStream_t *side = side_streams();
+    if (!side) return PACO_ERR_CUDA;
+    cudaEvent_t *fe = bd_fork_events();
+    const SvdLayout &L = ml.L;
+    for (int g0 = 0; g0 < count; g0 += ml.k) {
+        const int k = std::min(ml.k, count - g0);
+        BdJob jobs[PK_KMAX];
+        StatusPtrs sp;
+        sp.k = k;
+        for (int j = 0; j < k; j++) {
+            char *b = ws + (size_t)j * ml.per;
+            float *a = (float *)(b + ml.a_off);
+            jobs[j] = {M, N, A[g0 + j], a, U[g0 + j], Vt[g0 + j], sigma[g0 + j], (float *)(b + L.e),
+                       (float *)(b + L.tauq), (float *)(b + L.taup), b + L.ws};
+            sp.st[j] = (DevStatus *)(b + L.ws);
+            sp.idx[j] = g0 + j;
+            paco_count_launch(), dev_status_begin<<<1, 64, 0, s>>>(sp.st[j], 1);
+        }
+        int rc = bd_run_multi(k, jobs, s, side, device_sms());
+        if (rc) return rc;
+        if (k == 1) {
+            paco_count_launch(), dev_status_begin<<<1, 64, 0, s>>>(sp.st[0], 2);
+            char *b = ws;
+            rc = bdc_run(M, N, jobs[0].a_out, U[g0], Vt[g0], sigma[g0], jobs[0].e, (float *)(b + L.qt),
+                         (float *)(b + L.wt), (uint32_t *)(b + L.idx), b + L.ws, nullptr, s);
+        } else {
+            cudaEventRecord(fe[0], s);
+            for (int j = 0; j < k && !rc; j++) {
+                char *b = ws + (size_t)j * ml.per;
+                cudaStreamWaitEvent(side[j], fe[0], 0);
+                paco_count_launch(), dev_status_begin<<<1, 64, 0, side[j]>>>(sp.st[j], 2);
+                rc = bdc_run(M, N, jobs[j].a_out, U[g0 + j], Vt[g0 + j], sigma[g0 + j], jobs[j].e,
+                             (float *)(b + L.qt), (float *)(b + L.wt), (uint32_t *)(b + L.idx), b + L.ws, nullptr,
+                             side[j]);
+            }
+            for (int j = 0; j < k; j++) {
+                cudaEventRecord(fe[1 + j], side[j]);
+                cudaStreamWaitEvent(s, fe[1 + j], 0);
+            }
+        }
+        if (rc) return rc;
+        paco_count_launch(), multi_status_k<<<1, 32, 0, s>>>(sp, status);
+    }
+    return cudaGetLastError() == cudaSuccess ? PACO_OK : PACO_ERR_CUDA;
+}
+}  // namespace
+
+extern "C" {
+
+size_t paco_svd_multi_workspace_size(int count, int M, int N)
+{
+    if (count < 1 || !shape_ok(M, N)) return 0;
+    return multi_layout(count, M, N).total;
+}
+
+int paco_multi_group(int k)
+{
+    const int prev = g_multi_k;
+    if (k >= 0 && k <= PK_KMAX) g_multi_k = k;
+    return prev;
+}
+
+int paco_svd_multi(int count, int M, int N, const float *const *A, float *const *U, float *const *Vt,
+                   float *const *sigma, int *status, void *workspace, size_t ws_bytes, void *stream)
+{
+    if (count < 1 || !A || !U || !Vt || !sigma || !workspace) return PACO_ERR_INVALID_ARG;
+    if (!shape_ok(M, N)) return (N >= 1 && M >= N) ? PACO_ERR_UNSUPPORTED : PACO_ERR_INVALID_ARG;
+    for (int b = 0; b < count; b++)
+        if (!A[b] || !U[b] || !Vt[b] || !sigma[b]) return PACO_ERR_INVALID_ARG;
+    const MultiLayout ml = multi_layout(count, M, N);
+    if (ws_bytes < ml.total) return PACO_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!side_streams()) return PACO_ERR_CUDA;
+    std::vector<uintptr_t> key = {2, (uintptr_t)count, (uintptr_t)M, (uintptr_t)N, (uintptr_t)ml.k,
+                                  (uintptr_t)workspace, (uintptr_t)status};
+    for (int b = 0; b < count; b++) {
+        key.push_back((uintptr_t)A[b]);
+        key.push_back((uintptr_t)U[b]);
+        key.push_back((uintptr_t)Vt[b]);
+        key.push_back((uintptr_t)sigma[b]);
+    }
+    return run_cached(key, s, [&]() {
+        return svd_multi_direct(count, M, N, A, U, Vt, sigma, status, (char *)workspace, ml, s);
+    });
 }
 
 // ------------------------------------------------ tiling autotuner

@@ -625,6 +625,43 @@ static bool tc_persistent()
     return g_tc_persistent == 1;
 }
 
+// Test hook: one CTA holds tensor memory while thread 0 waits on an mbarrier
+// nothing arrives at; the wait gives up after max_cycles and records
+// PACO_ERR_TIMEOUT, then the tensor memory is freed (the path every tcgen05
+// kernel here takes when a wait gives up).
+__global__ void __launch_bounds__(128) tc_dbg_wait_timeout(DevStatus *st, long long max_cycles)
+{
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t s_tmem;
+    const int warp = threadIdx.x >> 5;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(32)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_init_fence();
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    if (threadIdx.x == 0) mbar_wait_bounded(&bar, 0, st, 998, max_cycles);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32) : "memory");
+}
+
+bool gemm_tc_debug_timeout(DevStatus *st, long long max_cycles, cudaStream_t s)
+{
+    paco_count_launch();
+    tc_dbg_wait_timeout<<<1, 128, 0, s>>>(st, max_cycles);
+    return cudaGetLastError() == cudaSuccess;
+}
+
 int gemm_tc_set_persistent(int on)
 {
     const int prev = tc_persistent() ? 1 : 0;

@@ -42,3 +42,8 @@ cudaError_t gemm_any(int M, int N, int K, float alpha, GemmOp A, GemmOp B, float
 // for the given list of shapes (max over them); 0 when the tensor-core path
 // is not used for any of them.
 size_t gemm_tc_scratch_for(const int (*shapes)[3], int n);
+
+// Test hook: a kernel holding tensor memory whose mbarrier wait never
+// completes; the wait gives up after max_cycles (PACO_ERR_TIMEOUT in st) and
+// the tensor memory is freed before the CTA exits.
+bool gemm_tc_debug_timeout(DevStatus *st, long long max_cycles, cudaStream_t s);

@@ -84,6 +84,13 @@ def lib():
         L.paco_svd_batched.argtypes = [i, ip, ip, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
                                        ctypes.POINTER(vp), vp, vp, ctypes.c_size_t, vp]
         L.paco_svd_batched.restype = i
+        L.paco_svd_multi_workspace_size.argtypes = [i, i, i]
+        L.paco_svd_multi_workspace_size.restype = ctypes.c_size_t
+        L.paco_svd_multi.argtypes = [i, i, i, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                     ctypes.POINTER(vp), vp, vp, ctypes.c_size_t, vp]
+        L.paco_svd_multi.restype = i
+        L.paco_multi_group.argtypes = [i]
+        L.paco_multi_group.restype = i
         _lib = L
     return _lib
 
@@ -342,6 +349,66 @@ def svd_batched(As, check=True):
         for k, c in enumerate(st):
             _check(c, f"paco_svd_batched matrix {k}")
     return [s.clone() for s in b.sigma], [u.clone() for u in b.U], [v.clone() for v in b.Vt], st
+
+
+def multi_group(k: int) -> int:
+    """Matrices per lockstep group of the multi-matrix form (1..8, 0 =
+    automatic); returns the previous setting."""
+    return int(lib().paco_multi_group(int(k)))
+
+
+class Multi:
+    """Device buffers of the multi-matrix form (paco_svd_multi) for `count`
+    matrices of one shape (M >= N), reusable across calls: A (count x M x N,
+    read only), U (count x M x M), Vt (count x N x N), sigma (count x N) and
+    the per-matrix status.  The lockstep group size is fixed when the
+    workspace is sized (multi_group)."""
+
+    def __init__(self, count: int, M: int, N: int, device="cuda"):
+        torch = _torch()
+        self.count, self.M, self.N = int(count), int(M), int(N)
+        self.nbytes = int(lib().paco_svd_multi_workspace_size(self.count, self.M, self.N))
+        if self.nbytes == 0:
+            raise PacoError(PACO_ERR_UNSUPPORTED if N >= 1 and M >= N else PACO_ERR_INVALID_ARG,
+                            "paco_svd_multi_workspace_size")
+        self.ws = torch.empty(self.nbytes, dtype=torch.uint8, device=device)
+        self.A = torch.empty(self.count, M, N, device=device)
+        self.U = torch.empty(self.count, M, M, device=device)
+        self.Vt = torch.empty(self.count, N, N, device=device)
+        self.sigma = torch.empty(self.count, N, device=device)
+        self.status = torch.zeros(self.count, dtype=torch.int32, device=device)
+        vpa = ctypes.c_void_p * self.count
+        self._pA = vpa(*[self.A[b].data_ptr() for b in range(self.count)])
+        self._pU = vpa(*[self.U[b].data_ptr() for b in range(self.count)])
+        self._pV = vpa(*[self.Vt[b].data_ptr() for b in range(self.count)])
+        self._ps = vpa(*[self.sigma[b].data_ptr() for b in range(self.count)])
+
+    def run(self, stream=None):
+        """Enqueues the SVDs of the resident A on `stream`."""
+        rc = lib().paco_svd_multi(self.count, self.M, self.N, self._pA, self._pU, self._pV, self._ps,
+                                  _ptr(self.status), _ptr(self.ws), self.nbytes, _stream(stream))
+        _check(rc, "paco_svd_multi")
+
+    def statuses(self):
+        return self.status.cpu().tolist()
+
+
+def svd_multi(As, check=True):
+    """SVDs of a list of float32 matrices of one shape through the
+    multi-matrix form.  Returns lists (sigma, U, Vt) and the statuses."""
+    torch = _torch()
+    As = [a if hasattr(a, "data_ptr") else torch.from_numpy(np.ascontiguousarray(a, np.float32)) for a in As]
+    M, N = As[0].shape
+    m = Multi(len(As), M, N)
+    for b, a in enumerate(As):
+        m.A[b].copy_(a)
+    m.run()
+    torch.cuda.synchronize()
+    st = m.statuses()
+    if check:
+        for k, c in enumerate(st):
+            _check(c, f"paco_svd_multi matrix {k}")
+    return [x.clone() for x in m.sigma], [x.clone() for x in m.U], [x.clone() for x in m.Vt], st
 
 
 class HostContext:

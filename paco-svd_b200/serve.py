@@ -10,7 +10,10 @@ on the GPU.  The loop
     stream of its own as soon as a stream is free, so batches that arrive
     while others run overlap with them on the device,
   * polls each batch's completion event, stamps its requests done and
-    releases their memory.
+    releases their memory,
+  * cancels a request on demand: one not yet launched leaves at once (its
+    memory is released), one whose batch is on the GPU is dropped when the
+    batch completes; the other matrices of that batch are not affected.
 Every result depends only on its own matrix (one CTA per matrix), so it is
 bit for bit the same alone and in any mix.
 
@@ -29,9 +32,12 @@ import numpy as np
 import pacosvd as P
 
 
+CANCELLED = -1  # Request.status of a cancelled request
+
+
 class Request:
     __slots__ = ("rid", "M", "N", "A", "arrival", "admitted", "done", "U", "Vt", "sigma", "status", "keep",
-                 "nbytes")
+                 "nbytes", "cancel")
 
     def __init__(self, rid, A, arrival=0.0, keep=False):
         self.rid = rid
@@ -43,6 +49,7 @@ class Request:
         self.status = None
         self.keep = keep
         self.nbytes = footprint(self.M, self.N)
+        self.cancel = False
 
 
 def footprint(M: int, N: int) -> int:
@@ -81,6 +88,8 @@ class SvdServer:
         self.inflight = 0                       # bytes held by admitted requests and batch scratch
         self.peak_inflight = 0
         self.completed = []
+        self.cancelled = []
+        self.live = {}                          # rid -> request, from submit until done or cancelled
         self.batches = 0
         self.lib = P.lib()
 
@@ -89,6 +98,32 @@ class SvdServer:
         if not (1 <= req.N <= req.M <= P.PACO_BATCH_MAX_M):
             raise P.PacoError(P.PACO_ERR_UNSUPPORTED, f"request {req.rid}: {req.M}x{req.N}")
         self.waiting.append(req)
+        self.live[req.rid] = req
+
+    def cancel(self, rid, now=0.0) -> bool:
+        """Cancels request `rid`.  Not yet on the GPU: it leaves now and its
+        memory is released.  On the GPU: its batch runs on and the result is
+        dropped when the batch completes.  Returns False for an unknown or
+        finished request."""
+        r = self.live.get(rid)
+        if r is None:
+            return False
+        r.cancel = True
+        for q in (self.waiting, self.pending[0], self.pending[1]):
+            if r in q:
+                q.remove(r)
+                if r.admitted is not None:
+                    self.inflight -= r.nbytes
+                self._drop(r, now)
+                return True
+        return True  # in flight: _finish drops it
+
+    def _drop(self, r, t):
+        r.status = CANCELLED
+        r.done = t
+        r.A = None
+        self.live.pop(r.rid, None)
+        self.cancelled.append(r)
 
     def _admit(self, now):
         while self.waiting and self.inflight + self.waiting[0].nbytes <= self.cap:
@@ -156,6 +191,13 @@ class SvdServer:
         st = b.status.cpu().tolist()
         ou = ov = os_ = 0
         for j, r in enumerate(b.reqs):
+            if r.cancel:
+                self.inflight -= r.nbytes
+                self._drop(r, t)
+                ou += r.M * r.M
+                ov += r.N * r.N
+                os_ += r.N
+                continue
             r.done = t
             if r.keep:
                 r.U = b.U[ou:ou + r.M * r.M].view(r.M, r.M).clone()
@@ -167,6 +209,7 @@ class SvdServer:
             os_ += r.N
             self.inflight -= r.nbytes
             r.A = None
+            self.live.pop(r.rid, None)
             self.completed.append(r)
         # the copies above run on the current stream: keep the batch's buffers
         # out of the allocator's reach until they have, or the next batch on
@@ -235,7 +278,7 @@ def run_trace(server, reqs, arrivals, poll_sleep=0.0):
     t0 = time.perf_counter()
     now = lambda: time.perf_counter() - t0
     i, n = 0, len(reqs)
-    while len(server.completed) < n:
+    while len(server.completed) + len(server.cancelled) < n:
         t = now()
         while i < n and arrivals[i] <= t:
             reqs[i].arrival = arrivals[i]

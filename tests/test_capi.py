@@ -111,16 +111,23 @@ def test_noalloc_scratch_covers_its_largest_shape():
 def test_batched_workspace_rejects_bad_shapes():
     assert P.batched_workspace_size([(4, 8)]) == 0               # M < N
     assert P.batched_workspace_size([(10, 0)]) == 0              # N = 0
-    assert P.batched_workspace_size([(2049, 10)]) == 0           # M beyond the batched limit
+    # beyond the one-CTA-per-matrix limit only lists of one shape (the multi-matrix form)
+    assert P.batched_workspace_size([(2049, 10), (2049, 11)]) == 0
+    assert P.batched_workspace_size([(2049, 10), (100, 10)]) == 0
+    assert P.batched_workspace_size([(2049, 10)] * 3) == P.lib().paco_svd_multi_workspace_size(3, 2049, 10) > 0
     assert P.batched_workspace_size([]) == 0
 
 
 def test_batched_entry_validates_before_touching_the_device():
     import ctypes as C
     L = P.lib()
-    Ms, Ns = (C.c_int * 1)(3000), (C.c_int * 1)(10)
-    nul = (C.c_void_p * 1)(None)
-    assert L.paco_svd_batched(1, Ms, Ns, nul, nul, nul, nul, None, None, 0, None) == P.PACO_ERR_UNSUPPORTED
+    Ms, Ns = (C.c_int * 2)(3000, 100), (C.c_int * 2)(10, 10)
+    nul = (C.c_void_p * 2)(None, None)
+    # a large matrix among other shapes has no kernel
+    assert L.paco_svd_batched(2, Ms, Ns, nul, nul, nul, nul, None, None, 0, None) == P.PACO_ERR_UNSUPPORTED
+    # one large shape goes to the multi-matrix form, which checks its pointers
+    assert L.paco_svd_batched(1, Ms, Ns, nul, nul, nul, nul, None, None, 0, None) == P.PACO_ERR_INVALID_ARG
+    assert L.paco_svd_multi(1, 3000, 10, nul, nul, nul, nul, None, None, 0, None) == P.PACO_ERR_INVALID_ARG
     Ms[0] = 3
     assert L.paco_svd_batched(1, Ms, Ns, nul, nul, nul, nul, None, None, 0, None) == P.PACO_ERR_INVALID_ARG
 
