@@ -241,6 +241,14 @@ def single_config(name, wl):
             "M": wl["M"], "N": wl["N"], "l2": "a 512 MiB buffer is written between timed GPU steps (L2 flush)"}
 
 
+def multi_config(name, wl):
+    """`config` of the multi-matrix workload, the same in both arms."""
+    return {"workload": f"{name}: {wl['count']} FP32 {wl['M']}x{wl['N']} matrices with clustered spectra "
+                        f"(512 clusters of 8, spacing 1e-7), full SVD of each per step",
+            "count": wl["count"], "M": wl["M"], "N": wl["N"],
+            "l2": "a 512 MiB buffer is written between timed GPU steps (L2 flush)"}
+
+
 def batched_config(name, wl):
     """`config` of the batched workload, the same in both arms."""
     return {"workload": f"{name}: {wl['count']} FP32 N(0,1) matrices, M uniform on [{wl['Mlo']}, {wl['Mhi']}], "
@@ -263,6 +271,7 @@ def run_reference(args, wl, rank):
                           "algorithm is timed per matrix by the batched and single-matrix workloads"}))
         return
     threads = host_threads()
+    multi = wl.get("kind") == "multi"
     if batched:
         # the batch's own shapes in order, N(0,1) entries, as many matrices as fit in the budget
         shapes = batched_shapes(wl, 4321)
@@ -283,7 +292,7 @@ def run_reference(args, wl, rank):
         config = batched_config(args.workload, wl)
         value_unit = value
     else:
-        A = make_matrix(wl, seed=1234)
+        A = make_matrix(dict(M=wl["M"], N=wl["N"], gen=wl["gen"]), seed=1234)
         warm = lapack_svd_timed(A, 1, 0.0) if args.warmup > 0 else []
         times = lapack_svd_timed(A, args.steps, REF_BUDGET_S)
         steps_done = len(times)
@@ -292,7 +301,9 @@ def run_reference(args, wl, rank):
         sample = (f"the full {wl['M']}x{wl['N']} workload matrix at every step: numpy.linalg.svd (OpenBLAS "
                   f"sgesdd, FP32, full U), {len(warm)} warm-up call, {steps_done} timed calls "
                   f"(of {args.steps} requested; the run stops after {REF_BUDGET_S:.0f} s of timed work)")
-        config = single_config(args.workload, wl)
+        config = multi_config(args.workload, wl) if multi else single_config(args.workload, wl)
+        if multi:
+            sample += f"; one matrix per timed call (the workload has {wl['count']} per step)"
     cb = {"value": value_unit, "unit": "SVDs/s", "cores": threads, "kind": "lapack sgesdd", "sample": sample}
     line = {"metric": "SVDs/sec", "value": value_unit, "unit": "SVDs/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": steps_done, "steps_requested": args.steps,
@@ -314,6 +325,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end measurement")
     ap.add_argument("--serve-seconds", type=float, default=None, help="length of the serving trace")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default configuration (no paco_autotune)")
+    ap.add_argument("--multi-group", type=int, default=0, help="matrices per lockstep group of the multi form")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
 
@@ -339,6 +351,9 @@ def main():
         return
     if wl.get("kind") == "serving":
         run_serving(args, wl, rank, world, local, dist)
+        return
+    if wl.get("kind") == "multi":
+        run_multi(args, wl, rank, world, local, dist)
         return
     M, N = wl["M"], wl["N"]
     # the tiling autotuner picks this shape's configuration before the clock starts
@@ -480,6 +495,188 @@ def main():
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(wl, A_host)
         line["cpu_oracle"] = cpu_oracle(wl)
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_multi(args, wl, rank, world, local, dist):
+    """cfg3x8: one step = one paco_svd_multi call over `count` matrices of the
+    precision-form shape.  Beside it, the same matrices one at a time through
+    paco_svd: the plain FP32 form (SIMT FP32 products, tuning entry tc = 0)
+    and the precision form (3xTF32 tcgen05 products, the default)."""
+    import torch
+    import pacosvd as P
+    from workloads import make_clustered_device
+
+    M, N, count = wl["M"], wl["N"], wl["count"]
+    lib = P.lib()
+    lib.paco_launch_count.restype = ctypes.c_ulonglong
+    lib.paco_profile_read.argtypes = [ctypes.POINTER(ctypes.c_double)]
+    if args.multi_group:
+        P.multi_group(args.multi_group)
+    group = P.multi_group(0)
+    P.multi_group(group)
+    m = P.Multi(count, M, N)
+    sig_exact = []
+    for b in range(count):
+        A, sg = make_clustered_device(M, N, 5000 + 100 * rank + b)
+        m.A[b].copy_(A)
+        sig_exact.append(sg)
+        del A
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream()
+    prof = (ctypes.c_double * 4)()
+    lib.paco_profile_enable(1)
+    with torch.cuda.stream(stream):
+        for _ in range(max(3, args.warmup)):
+            m.run(stream)
+    stream.synchronize()
+    bad = [c for c in m.statuses() if c]
+    if bad:
+        raise SystemExit(f"statuses {bad} during warm-up")
+    lib.paco_profile_enable(1)
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = lib.paco_launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.fill_(k & 0xff)
+            ev[k][0].record(stream)
+            m.run(stream)
+            ev[k][1].record(stream)
+            stream.synchronize()
+            lib.paco_profile_read(prof)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = lib.paco_launch_count() - launches0
+    lib.paco_profile_enable(0)
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = max_over_ranks(sum(step_ms), dist)
+    if any(m.statuses()):
+        raise SystemExit(f"statuses {m.statuses()} in the timed region")
+
+    # accuracy of two matrices of the last call against dgesdd and the exact spectrum
+    acc = None
+    if rank == 0:
+        worst = {"sigma_err": 0.0, "sigma_err_exact": 0.0, "residual": 0.0, "orth_U": 0.0, "orth_V": 0.0}
+        for b in (0, count - 1):
+            Ad, Ud, Vd = m.A[b].double(), m.U[b].double(), m.Vt[b].double()
+            sd = m.sigma[b].double()
+            r = {"residual": (torch.linalg.norm(Ad - (Ud[:, :N] * sd[None, :]) @ Vd) / torch.linalg.norm(Ad)).item(),
+                 "orth_U": torch.linalg.norm(Ud.T @ Ud - torch.eye(M, dtype=torch.float64, device="cuda")).item(),
+                 "orth_V": torch.linalg.norm(Vd @ Vd.T - torch.eye(N, dtype=torch.float64, device="cuda")).item()}
+            del Ud, Vd
+            s = m.sigma[b].cpu().numpy().astype(np.float64)
+            ref = dgesdd_sigma(m.A[b].cpu().numpy())
+            r["sigma_err"] = float(np.max(np.abs(s - ref)) / ref[0])
+            r["sigma_err_exact"] = float(np.max(np.abs(s - sig_exact[b])) / sig_exact[b][0])
+            for key, v in r.items():
+                worst[key] = max(worst[key], v)
+            del Ad
+            torch.cuda.empty_cache()
+        acc = dict(worst, matrices=2, tolerance=1e-5 * N, sigma_tolerance=1e-5,
+                   sigma_reference="FP64 LAPACK dgesdd of the FP32 input (scipy, host)")
+
+    # the same matrices one at a time through paco_svd: plain FP32 form (SIMT
+    # products) and the precision form (tcgen05 3xTF32 products)
+    singles = {}
+    if rank == 0:
+        W = P.Workspace(M, N)
+        for name, cfg in (("plain_fp32_single", [1, 16, 0, 0]), ("precision_single", None)):
+            if cfg is not None:
+                P.tune_set(M, N, cfg)
+            else:
+                P.tune_set(M, N, [1, 16, 1, 0])
+            times = []
+            with torch.cuda.stream(stream):
+                for k in range(3 + 3):
+                    W.A.copy_(m.A[k % count])
+                    flush.fill_(k & 0xff)
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    W.run(stream=stream)
+                    e1.record(stream)
+                    stream.synchronize()
+                    if k >= 3:
+                        times.append(e0.elapsed_time(e1))
+            rc, info = P.sync_status(W.ws, stream)
+            if rc:
+                raise SystemExit(f"single-matrix status {rc} ({info})")
+            singles[name] = {"value": 1000.0 / statistics.mean(times), "unit": "SVDs/s",
+                             "ms_per_svd": statistics.mean(times),
+                             "form": ("one paco_svd call per matrix, SIMT FP32 products (tuning entry tc = 0)"
+                                      if cfg is not None else
+                                      "one paco_svd call per matrix, 3xTF32 tcgen05 products")}
+        P.tune_set(M, N, [1, 16, 1, 0])
+        del W
+
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda t: torch.empty(t.shape, dtype=t.dtype).pin_memory()
+        Ah, Uh, Vh, sh = pin(m.A), pin(m.U), pin(m.Vt), pin(m.sigma)
+        Ah.copy_(m.A.cpu())
+        times = []
+        for k in range(max(1, min(args.steps, 3))):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+                m.A.copy_(Ah, non_blocking=True)
+                m.run(stream)
+                Uh.copy_(m.U, non_blocking=True)
+                Vh.copy_(m.Vt, non_blocking=True)
+                sh.copy_(m.sigma, non_blocking=True)
+                e1.record(stream)
+            stream.synchronize()
+            times.append(e0.elapsed_time(e1))
+        e2e = {"value": world * count / (statistics.median(times) / 1000.0), "unit": "SVDs/s",
+               "h2d_bytes_per_step": 4 * m.A.numel(),
+               "d2h_bytes_per_step": 4 * (m.U.numel() + m.Vt.numel() + m.sigma.numel())}
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    peaks, peak_kind = measured_peaks()
+    rp_ms, rp_launches = prof[0], prof[1]
+    classic = 8.0 * sum((M - i) * (N - i) for i in range(N))
+    n_launch = max(rp_launches, 1)
+    alg_per_launch = classic * count * args.steps / n_launch
+    avg_s = rp_ms / 1e3 / n_launch
+    achieved = (alg_per_launch / 1e9) / avg_s if rp_ms > 0 else None
+    value = whole_job_value(world, args.steps * count, total_ms)
+    lat = sorted(step_ms)
+    plain = singles.get("plain_fp32_single")
+    prec = singles.get("precision_single")
+    line = {"metric": "SVDs/sec", "value": value, "unit": "SVDs/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": multi_config(args.workload, wl),
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+            "form": f"paco_svd_multi, lockstep groups of {group or 4}, 3xTF32 tcgen05 products",
+            "latency": {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                        "definition": "a result is delivered when its call returns: the call's duration"},
+            "accuracy": acc, "clocks": clk,
+            "roofline": {"kernel": "bd_panel_pk (persistent stage-1 panel kernel, k matrices per launch) and "
+                                   "bd_tail_k", "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                         "unit": "GB/s", "frac": (achieved / peaks["hbm_gbs"]) if achieved else None,
+                         "traffic": None, "alg_bytes_per_launch": alg_per_launch,
+                         "alg_bytes_definition": "8*sum_i (M-i)(N-i) per matrix, summed over the matrices",
+                         "avg_launch_us": 1e6 * avg_s, "launches": int(rp_launches),
+                         "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)"},
+            "e2e": e2e, "gpu_launches": int(launches), "singles": singles,
+            "multi_over_plain_fp32_single": (value / world / plain["value"]) if plain else None,
+            "multi_over_precision_single": (value / world / prec["value"]) if prec else None}
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(wl, m.A[0].cpu().numpy())
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()

@@ -65,6 +65,15 @@ int paco_autotune(int M, int N, void *stream, double out[4]);
 int paco_tune_get(int M, int N, int cfg[4]);
 int paco_tune_set(int M, int N, const int cfg[4]);
 
+/* QR-first reduction for tall matrices (no counterpart in the reference,
+ * which lists it as future work, README.md:22): A = Q R, the SVD pipeline on
+ * the N x N factor R, U = Q blockdiag(U_R, I).  It applies to shapes with
+ * M > N and N >= 1024 whose QR blocks fit one thread-block cluster (M up to
+ * about 13,000); mode 0 = off, 1 = on, 2 = automatic (on when M >= 1.6 N, the
+ * default), -1 = query.  paco_autotune times both choices for such shapes.
+ * Returns the mode stored (or queried), -1 for an invalid argument. */
+int paco_tune_qr(int M, int N, int mode);
+
 /* Buffer sizes in bytes of main.cpp:33-43, in this order:
  * [0] U M*M, [1] A M*N, [2] Vt N*N, [3] d N, [4] e N-1, [5] tauq N,
  * [6] taup N-1, [7] qt 2*N*N, [8] wt 2*N*N, [9] tiling, [10] idx 16*N*u32,

@@ -29,6 +29,7 @@
 
 #include "bidiag.cuh"
 #include "gemm.cuh"
+#include "qr.cuh"
 #include "tma.cuh"
 
 using namespace bd;
@@ -516,35 +517,59 @@ __global__ void __launch_bounds__(256) bd_build_t(const float *gram, int nbp, co
     for (int j = 0; j < J; j++) T[(long)r * NBF + lane + 32 * j] = t[j];
 }
 
+// Q_sub <- (I - Vp T' Vp^T) Q_sub for Q_sub = Q[ro:ro+Lr, co:co+Lc] (ld ldq),
+// T' = T (forward block reflector H_0 ... H_{nbp-1}) or its transpose (the
+// transposed product, as a QR factorization applies to its trailing columns).
+// Vp (Lr x NBF) must hold the block's reflectors.
+cudaError_t apply_block_reflector_ex(const BdWs &w, float *Q, long ldq, long ro, int Lr, long co, int Lc, int nbp,
+                                     const float *tau, bool transT, cudaStream_t s)
+{
+    const int splits = std::max(1, std::min(SPLITS, ceil_div(Lr, 512)));
+    // G = Vp^T Vp: one 128 x 128 tile, so the long k = Lr dimension is split
+    // finely (64 rows per CTA, as many splits as the partial buffer holds)
+    // (the partial buffer holds SPLITS * NBF * max(M, N) >= SPLITS * NBF * ldq floats)
+    const int gsplits = (int)std::max(1L, std::min({(long)ceil_div(Lr, 64), 64L, (long)SPLITS * ldq / NBF}));
+    cudaError_t err = gemm_run(nbp, nbp, Lr, 1.f, gop(w.Vp, 1, NBF), gop(w.Vp, NBF, 1), 0.f, w.gram, NBF, gsplits,
+                               w.gscr, s);
+    if (err) return err;
+    paco_count_launch(), bd_build_t<<<NBF / 8, 256, (size_t)NBF * NBF * sizeof(float), s>>>(w.gram, nbp, tau, w.T);
+    float *Qs = Q + ro * ldq + co;
+    // G1 = Vp^T Q_sub  (nbp x Lc)
+    err = gemm_any(nbp, Lc, Lr, 1.f, gop(w.Vp, 1, NBF), gop(Qs, ldq, 1), 0.f, w.G1, Lc, splits, w.gscr, w.tcs,
+                   w.tcs_floats, w.st, s);
+    if (err) return err;
+    // G2 = T' G1 (128 x Lc x 128: small, but on the SIMT engine it runs on
+    // only Lc / 128 CTAs, so it goes to the tensor cores from Lc = 256 on)
+    const GemmOp Top = transT ? gop(w.T, 1, NBF) : gop(w.T, NBF, 1);
+    if (w.tcs && gemm_tc_enabled() && Lc >= 256 && gemm_tc_scratch_floats(nbp, Lc, nbp) <= w.tcs_floats)
+        err = gemm_tc_run(nbp, Lc, nbp, 1.f, Top, gop(w.G1, Lc, 1), 0.f, w.G2, Lc, w.tcs, w.st, s);
+    else
+        err = gemm_any(nbp, Lc, nbp, 1.f, Top, gop(w.G1, Lc, 1), 0.f, w.G2, Lc, 1, nullptr, w.tcs, w.tcs_floats,
+                       w.st, s);
+    if (err) return err;
+    // Q_sub -= Vp G2
+    return gemm_any(Lr, Lc, nbp, -1.f, gop(w.Vp, NBF, 1), gop(w.G2, Lc, 1), 1.f, Qs, ldq, 1, nullptr, w.tcs,
+                    w.tcs_floats, w.st, s);
+}
+
 // Q_sub <- (I - Vp T Vp^T) Q_sub for Q_sub = Q[off:off+Lp, off:off+Lp] (ld ldq)
 static cudaError_t apply_block_reflector(const BdWs &w, float *Q, long ldq, long off, int Lp, int nbp,
                                          const float *tau, cudaStream_t s)
 {
-    const int splits = std::max(1, std::min(SPLITS, ceil_div(Lp, 512)));
-    // G = Vp^T Vp: one 128 x 128 tile, so the long k = Lp dimension is split
-    // finely (64 rows per CTA, as many splits as the partial buffer holds)
-    // (the partial buffer holds SPLITS * NBF * max(M, N) >= SPLITS * NBF * ldq floats)
-    const int gsplits = (int)std::max(1L, std::min({(long)ceil_div(Lp, 64), 64L, (long)SPLITS * ldq / NBF}));
-    cudaError_t err = gemm_run(nbp, nbp, Lp, 1.f, gop(w.Vp, 1, NBF), gop(w.Vp, NBF, 1), 0.f, w.gram, NBF, gsplits,
-                               w.gscr, s);
-    if (err) return err;
-    paco_count_launch(), bd_build_t<<<NBF / 8, 256, (size_t)NBF * NBF * sizeof(float), s>>>(w.gram, nbp, tau, w.T);
-    float *Qs = Q + off * ldq + off;
-    // G1 = Vp^T Q_sub  (nbp x Lp)
-    err = gemm_any(nbp, Lp, Lp, 1.f, gop(w.Vp, 1, NBF), gop(Qs, ldq, 1), 0.f, w.G1, Lp, splits, w.gscr, w.tcs,
-                   w.tcs_floats, w.st, s);
-    if (err) return err;
-    // G2 = T G1 (128 x Lp x 128: small, but on the SIMT engine it runs on
-    // only Lp / 128 CTAs, so it goes to the tensor cores from Lp = 256 on)
-    if (w.tcs && gemm_tc_enabled() && Lp >= 256 && gemm_tc_scratch_floats(nbp, Lp, nbp) <= w.tcs_floats)
-        err = gemm_tc_run(nbp, Lp, nbp, 1.f, gop(w.T, NBF, 1), gop(w.G1, Lp, 1), 0.f, w.G2, Lp, w.tcs, w.st, s);
-    else
-        err = gemm_any(nbp, Lp, nbp, 1.f, gop(w.T, NBF, 1), gop(w.G1, Lp, 1), 0.f, w.G2, Lp, 1, nullptr, w.tcs,
-                       w.tcs_floats, w.st, s);
-    if (err) return err;
-    // Q_sub -= Vp G2
-    return gemm_any(Lp, Lp, nbp, -1.f, gop(w.Vp, NBF, 1), gop(w.G2, Lp, 1), 1.f, Qs, ldq, 1, nullptr, w.tcs,
-                    w.tcs_floats, w.st, s);
+    return apply_block_reflector_ex(w, Q, ldq, off, Lp, off, Lp, nbp, tau, false, s);
+}
+
+// Vp (Lp x NBF) <- the explicit reflectors of column block [p0, p0 + nbp) of W
+// (column vectors below the diagonal, unit diagonal)
+void bd_column_vectors(const float *W, long ldw, int p0, int nbp, int Lp, float *Vp, cudaStream_t s)
+{
+    paco_count_launch(), bd_panel_vectors<<<std::min(4096, ceil_div((long)Lp * NBF, 256)), 256, 0, s>>>(
+        W, ldw, p0, nbp, Lp, 0, Vp);
+}
+
+void bd_copy_in_launch(const float *a, float *W, int M, int N, long ldw, DevStatus *st, cudaStream_t s)
+{
+    paco_count_launch(), bd_copy_in<<<std::min(4096, ceil_div((long)M * ldw, 256)), 256, 0, s>>>(a, W, M, N, ldw, st);
 }
 
 // ------------------------------------------------------------ host driver
@@ -733,6 +758,7 @@ void bd_init_attrs()
     cudaFuncSetAttribute(bd_build_t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(NBF * NBF * sizeof(float)));
     gemm_tc_init_attrs();
     bd_tail_init();
+    qr_init();
     bd_fork_events();
     rp_attrs_set = true;
 }

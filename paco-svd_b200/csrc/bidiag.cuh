@@ -181,6 +181,14 @@ bool bd_tail_launch(const BdArgs &a, int p, cudaStream_t s);
 void bd_pk_init_attrs();
 
 size_t bd_workspace_bytes(int M, int N);
+// Q[ro:ro+Lr, co:co+Lc] <- (I - Vp T' Vp^T) Q[...] with T' = T, or T^T when
+// transT, for the nbp reflectors in w.Vp (T built from their Gram matrix).
+cudaError_t apply_block_reflector_ex(const BdWs &w, float *Q, long ldq, long ro, int Lr, long co, int Lc, int nbp,
+                                     const float *tau, bool transT, cudaStream_t s);
+// w.Vp-style explicit block of the column reflectors [p0, p0 + nbp) stored in W.
+void bd_column_vectors(const float *W, long ldw, int p0, int nbp, int Lp, float *Vp, cudaStream_t s);
+// W (M x ldw, zero padded) <- a (M x N); non-finite entries are reported and replaced by 0.
+void bd_copy_in_launch(const float *a, float *W, int M, int N, long ldw, DevStatus *st, cudaStream_t s);
 void bd_profile_enable(int on);
 void bd_profile_read(double out[4]);
 int bd_profile_last_graph_run();

@@ -7,6 +7,7 @@
 
 #include "bdc.cuh"
 #include "bidiag.cuh"
+#include "qr.cuh"
 
 namespace {
 
@@ -45,6 +46,38 @@ SvdLayout svd_layout(int M, int N)
     L.total = (off + 255) & ~(size_t)255;
     return L;
 }
+
+// QR-first layout (tall matrices): the N x N pipeline's layout first (its
+// status block at offset 0 is the call's), then tau of the QR, R, U_R and the
+// M x N stage-1 workspace that holds the QR factorization and the scratch of
+// the products with M rows.
+struct QrLayout {
+    SvdLayout LR;
+    size_t tau, ar, ur, bw, total;
+};
+
+QrLayout qr_layout(int M, int N)
+{
+    QrLayout Q;
+    Q.LR = svd_layout(N, N);
+    size_t off = Q.LR.total;
+    auto take = [&](size_t bytes) {
+        off = (off + 255) & ~(size_t)255;
+        size_t p = off;
+        off += bytes;
+        return p;
+    };
+    const size_t nn = (size_t)N * N;
+    Q.tau = take(sizeof(float) * N);
+    Q.ar = take(sizeof(float) * nn);
+    Q.ur = take(sizeof(float) * nn);
+    Q.bw = take(bd_workspace_bytes(M, N));
+    Q.total = (off + 255) & ~(size_t)255;
+    return Q;
+}
+
+// Shapes that may take the QR-first path (their workspace size covers it).
+bool qr_possible(int M, int N) { return M > N && N >= 1024; }
 
 } // namespace
 
@@ -88,6 +121,31 @@ void tune_store(int M, int N, const PacoTune &cfg)
     g_tune_gen++;
 }
 }  // namespace
+
+// QR-first choice per (M, N): 0 off, 1 on, 2 automatic (M >= 1.6 N), the default
+namespace {
+struct QrEntry {
+    int M, N, mode;
+};
+std::vector<QrEntry> g_qr_modes;
+}  // namespace
+
+static int qr_mode_for(int M, int N)
+{
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    for (const QrEntry &e : g_qr_modes)
+        if (e.M == M && e.N == N) return e.mode;
+    return 2;
+}
+
+static bool qr_chosen(int M, int N)
+{
+    if (!qr_possible(M, N)) return false;
+    const int mode = qr_mode_for(M, N);
+    if (mode == 0) return false;
+    if (mode == 2 && (long)M * 10 < 16L * N) return false;
+    return qr_fits(M, N);
+}
 
 PacoTune paco_tune_for(int M, int N)
 {
@@ -324,7 +382,52 @@ int paco_sync_status(void *workspace, void *stream, int *info)
 size_t paco_svd_workspace_size(int M, int N)
 {
     if (!shape_ok(M, N)) return 0;
-    return svd_layout(M, N).total;
+    const size_t one = svd_layout(M, N).total;
+    return qr_possible(M, N) ? std::max(one, qr_layout(M, N).total) : one;
+}
+
+int paco_tune_qr(int M, int N, int mode)
+{
+    if (!shape_ok(M, N) || mode < -1 || mode > 2) return -1;
+    if (mode == -1) return qr_mode_for(M, N);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        bool found = false;
+        for (QrEntry &e : g_qr_modes)
+            if (e.M == M && e.N == N) { e.mode = mode; found = true; }
+        if (!found) g_qr_modes.push_back({M, N, mode});
+        g_tune_gen++;
+    }
+    return mode;
+}
+
+// QR-first SVD of a tall matrix: A = Q R, the one-matrix pipeline on R
+// (N x N), then U = Q blockdiag(U_R, I).  A is read only.
+static int svd_direct_qr(int M, int N, const float *A, float *U, float *Vt, float *sigma, char *b,
+                         const QrLayout &Q, void *stream)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    const SvdLayout &L = Q.LR;
+    DevStatus *st = (DevStatus *)(b + L.ws);
+    float *e = (float *)(b + L.e), *tq = (float *)(b + L.tauq), *tp = (float *)(b + L.taup);
+    float *tau = (float *)(b + Q.tau), *AR = (float *)(b + Q.ar), *UR = (float *)(b + Q.ur);
+    BdWs wq;
+    bd_carve(b + Q.bw, M, N, &wq);
+    wq.st = st;  // the QR phase reports into the call's status block
+    if (!paco_tune_for(M, N).tc) wq.tcs = nullptr;
+    bd_init_attrs();
+    paco_count_launch(), dev_status_begin<<<1, 64, 0, s>>>(st, 1);
+    bd_copy_in_launch(A, wq.W, M, N, wq.ldw, st, s);
+    int rc = qr_factor(wq, M, N, tau, s);
+    if (rc) return rc;
+    qr_extract_r_launch(wq, N, AR, s);
+    rc = bd_run(N, N, AR, AR, UR, Vt, sigma, e, tq, tp, b + L.ws, s, device_sms());
+    if (rc) return rc;
+    paco_count_launch(), dev_status_begin<<<1, 64, 0, s>>>(st, 2);
+    rc = bdc_run(N, N, AR, UR, Vt, sigma, e, (float *)(b + L.qt), (float *)(b + L.wt), (uint32_t *)(b + L.idx),
+                 b + L.ws, nullptr, s);
+    if (rc) return rc;
+    return qr_form_u(wq, M, N, tau, UR, U, s);
 }
 
 static int svd_direct(int M, int N, float *A, float *U, float *Vt, float *sigma, char *b, const SvdLayout &L,
@@ -335,6 +438,15 @@ static int svd_direct(int M, int N, float *A, float *U, float *Vt, float *sigma,
     if (rc) return rc;
     return svd_DC(M, N, A, U, Vt, sigma, e, (float *)(b + L.qt), (float *)(b + L.wt), (uint32_t *)(b + L.idx),
                   b + L.ws, nullptr, stream);
+}
+
+// The single-matrix SVD in the configuration of (M, N): QR-first for tall
+// matrices when chosen, otherwise the one-stage pipeline.  b holds
+// paco_svd_workspace_size(M, N) bytes.
+static int svd_any(int M, int N, float *A, float *U, float *Vt, float *sigma, char *b, void *stream)
+{
+    if (qr_chosen(M, N)) return svd_direct_qr(M, N, A, U, Vt, sigma, b, qr_layout(M, N), stream);
+    return svd_direct(M, N, A, U, Vt, sigma, b, svd_layout(M, N), stream);
 }
 
 // The one-shot paths issue thousands of small launches per SVD; on a
@@ -429,12 +541,11 @@ int paco_svd(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws
 {
     if (!shape_ok(M, N)) return (N >= 1 && M >= N) ? PACO_ERR_UNSUPPORTED : PACO_ERR_INVALID_ARG;
     if (!A || !U || !Vt || !sigma || !ws) return PACO_ERR_INVALID_ARG;
-    SvdLayout L = svd_layout(M, N);
-    if (ws_bytes < L.total) return PACO_ERR_INVALID_ARG;
+    if (ws_bytes < paco_svd_workspace_size(M, N)) return PACO_ERR_INVALID_ARG;
     char *b = (char *)ws;
     const std::vector<uintptr_t> key = {1, (uintptr_t)M, (uintptr_t)N, (uintptr_t)A, (uintptr_t)U, (uintptr_t)Vt,
                                         (uintptr_t)sigma, (uintptr_t)ws};
-    return run_cached(key, (cudaStream_t)stream, [&]() { return svd_direct(M, N, A, U, Vt, sigma, b, L, stream); });
+    return run_cached(key, (cudaStream_t)stream, [&]() { return svd_any(M, N, A, U, Vt, sigma, b, stream); });
 }
 
 // ------------------------------------------------ multi-matrix form
@@ -480,6 +591,7 @@ MultiLayout multi_layout(int count, int M, int N)
     m.L = svd_layout(M, N);
     m.a_off = m.L.total;  // the M x N scratch that replaces A (A stays read only)
     m.per = (m.a_off + sizeof(float) * (size_t)M * N + 255) & ~(size_t)255;
+    if (qr_possible(M, N)) m.per = std::max(m.per, qr_layout(M, N).total);  // QR-first reads A only
     m.k = multi_group(count);
     m.total = m.per * m.k;
     return m;
@@ -506,6 +618,72 @@ __global__ void multi_status_k(StatusPtrs p, int *status)
     st->wait_timeouts = 0;
 }
 
+// The multi-matrix form with the QR-first reduction: per group, the QR of
+// every matrix on its own side stream, stage 1 of the k factors R in lockstep,
+// then per matrix (side streams) divide and conquer and U = Q blockdiag(U_R, I).
+int svd_multi_qr(int count, int M, int N, const float *const *A, float *const *U, float *const *Vt,
+                 float *const *sigma, int *status, char *ws, const MultiLayout &ml, cudaStream_t s,
+                 cudaStream_t *side)
+{
+    cudaEvent_t *fe = bd_fork_events();
+    const QrLayout Q = qr_layout(M, N);
+    const SvdLayout &L = Q.LR;
+    const bool tc = paco_tune_for(M, N).tc != 0;
+    auto fork = [&](int k) {
+        cudaEventRecord(fe[0], s);
+        for (int j = 0; j < k; j++) cudaStreamWaitEvent(side[j], fe[0], 0);
+    };
+    auto join = [&](int k) {
+        for (int j = 0; j < k; j++) {
+            cudaEventRecord(fe[1 + j], side[j]);
+            cudaStreamWaitEvent(s, fe[1 + j], 0);
+        }
+    };
+    for (int g0 = 0; g0 < count; g0 += ml.k) {
+        const int k = std::min(ml.k, count - g0);
+        BdJob jobs[PK_KMAX];
+        BdWs wq[PK_KMAX];
+        StatusPtrs sp;
+        sp.k = k;
+        int rc = PACO_OK;
+        for (int j = 0; j < k; j++) {
+            char *b = ws + (size_t)j * ml.per;
+            sp.st[j] = (DevStatus *)(b + L.ws);
+            sp.idx[j] = g0 + j;
+            paco_count_launch(), dev_status_begin<<<1, 64, 0, s>>>(sp.st[j], 1);
+            bd_carve(b + Q.bw, M, N, &wq[j]);
+            wq[j].st = sp.st[j];
+            if (!tc) wq[j].tcs = nullptr;
+            float *AR = (float *)(b + Q.ar);
+            jobs[j] = {N, N, AR, AR, (float *)(b + Q.ur), Vt[g0 + j], sigma[g0 + j], (float *)(b + L.e),
+                       (float *)(b + L.tauq), (float *)(b + L.taup), b + L.ws};
+        }
+        fork(k);
+        for (int j = 0; j < k && !rc; j++) {
+            char *b = ws + (size_t)j * ml.per;
+            bd_copy_in_launch(A[g0 + j], wq[j].W, M, N, wq[j].ldw, sp.st[j], side[j]);
+            rc = qr_factor(wq[j], M, N, (float *)(b + Q.tau), side[j]);
+            qr_extract_r_launch(wq[j], N, (float *)(b + Q.ar), side[j]);
+        }
+        join(k);
+        if (rc) return rc;
+        rc = bd_run_multi(k, jobs, s, side, device_sms());
+        if (rc) return rc;
+        fork(k);
+        for (int j = 0; j < k && !rc; j++) {
+            char *b = ws + (size_t)j * ml.per;
+            paco_count_launch(), dev_status_begin<<<1, 64, 0, side[j]>>>(sp.st[j], 2);
+            rc = bdc_run(N, N, jobs[j].a_out, jobs[j].u, Vt[g0 + j], sigma[g0 + j], jobs[j].e, (float *)(b + L.qt),
+                         (float *)(b + L.wt), (uint32_t *)(b + L.idx), b + L.ws, nullptr, side[j]);
+            if (!rc) rc = qr_form_u(wq[j], M, N, (float *)(b + Q.tau), jobs[j].u, U[g0 + j], side[j]);
+        }
+        join(k);
+        if (rc) return rc;
+        paco_count_launch(), multi_status_k<<<1, 32, 0, s>>>(sp, status);
+    }
+    return cudaGetLastError() == cudaSuccess ? PACO_OK : PACO_ERR_CUDA;
+}
+
 int svd_multi_direct(int count, int M, int N, const float *const *A, float *const *U, float *const *Vt,
                      float *const *sigma, int *status, char *ws, const MultiLayout &ml, cudaStream_t s)
 {
@@ -513,6 +691,7 @@ int svd_multi_direct(int count, int M, int N, const float *const *A, float *cons
     if (!side) return PACO_ERR_CUDA;
     cudaEvent_t *fe = bd_fork_events();
     const SvdLayout &L = ml.L;
+    if (qr_chosen(M, N)) return svd_multi_qr(count, M, N, A, U, Vt, sigma, status, ws, ml, s, side);
     for (int g0 = 0; g0 < count; g0 += ml.k) {
         const int k = std::min(ml.k, count - g0);
         BdJob jobs[PK_KMAX];
@@ -618,7 +797,7 @@ int paco_autotune(int M, int N, void *stream, double out[4])
 {
     if (!shape_ok(M, N)) return (N >= 1 && M >= N) ? PACO_ERR_UNSUPPORTED : PACO_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
-    const SvdLayout L = svd_layout(M, N);
+    const size_t wsb = paco_svd_workspace_size(M, N);
     float *A0 = nullptr, *A = nullptr, *U = nullptr, *Vt = nullptr, *sg = nullptr;
     char *ws = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -628,42 +807,56 @@ int paco_autotune(int M, int N, void *stream, double out[4])
     err = err ? err : cudaMalloc(&U, sizeof(float) * (size_t)M * M);
     err = err ? err : cudaMalloc(&Vt, sizeof(float) * (size_t)N * N);
     err = err ? err : cudaMalloc(&sg, sizeof(float) * N);
-    err = err ? err : cudaMalloc(&ws, L.total);
+    err = err ? err : cudaMalloc(&ws, wsb);
     err = err ? err : cudaEventCreate(&e0);
     err = err ? err : cudaEventCreate(&e1);
     int rc = err ? PACO_ERR_CUDA : PACO_OK;
     // candidates: the defaults first, then fewer / more rows per CTA, the
     // SIMT engine for the large products, the two-kernel row/column passes,
-    // the last columns on the panel kernel
+    // the last columns on the panel kernel; for tall shapes the best of them
+    // is then also timed with the QR-first choice flipped
     const PacoTune cands[] = {{1, bd::RMIN_PER_BLOCK, 1, 0}, {1, 8, 1, 0}, {1, 32, 1, 0}, {1, bd::RMIN_PER_BLOCK, 0, 0},
                               {0, bd::RMIN_PER_BLOCK, 1, 0}, {1, bd::RMIN_PER_BLOCK, 1, 1}};
     const int nc = (int)(sizeof(cands) / sizeof(cands[0]));
     float best = 1e30f, tdef = 0.f;
-    int bi = 0;
+    int bi = 0, tried = 0;
+    auto time_one = [&]() {
+        float tk = 1e30f;
+        for (int rep = 0; rep < 3; rep++) {
+            cudaMemcpyAsync(A, A0, sizeof(float) * (size_t)M * N, cudaMemcpyDeviceToDevice, s);
+            cudaEventRecord(e0, s);
+            int r = svd_any(M, N, A, U, Vt, sg, ws, stream);
+            cudaEventRecord(e1, s);
+            if (r || cudaEventSynchronize(e1) != cudaSuccess) { rc = r ? r : PACO_ERR_CUDA; break; }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0) tk = std::min(tk, ms);  // the first run warms up
+        }
+        int info = 0;
+        if (!rc && paco_sync_status(ws, stream, &info) != PACO_OK) tk = 1e30f;  // not a usable choice
+        tried++;
+        return tk;
+    };
     if (!rc) {
         paco_count_launch(), tune_fill<<<std::min(4096, ceil_div((long)M * N, 256)), 256, 0, s>>>(A0, (long)M * N,
                                                                                                    12345u);
         for (int k = 0; k < nc && !rc; k++) {
             tune_store(M, N, cands[k]);
-            float tk = 1e30f;
-            for (int rep = 0; rep < 3; rep++) {
-                cudaMemcpyAsync(A, A0, sizeof(float) * (size_t)M * N, cudaMemcpyDeviceToDevice, s);
-                cudaEventRecord(e0, s);
-                int r = svd_direct(M, N, A, U, Vt, sg, ws, L, stream);
-                cudaEventRecord(e1, s);
-                if (r || cudaEventSynchronize(e1) != cudaSuccess) { rc = r ? r : PACO_ERR_CUDA; break; }
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                if (rep > 0) tk = std::min(tk, ms);  // the first run warms up
-            }
-            int info = 0;
-            if (!rc && paco_sync_status(ws + L.ws, stream, &info) != PACO_OK) tk = 1e30f;  // not a usable choice
+            const float tk = time_one();
             if (k == 0) tdef = tk;
             if (tk < best) { best = tk; bi = k; }
         }
         tune_store(M, N, cands[bi]);
+        if (!rc && qr_possible(M, N) && qr_fits(M, N)) {
+            const int mode = qr_mode_for(M, N);
+            const bool on = qr_chosen(M, N);
+            paco_tune_qr(M, N, on ? 0 : 1);
+            const float tq = time_one();
+            if (!rc && tq < best) best = tq;
+            else paco_tune_qr(M, N, mode);
+        }
     }
-    if (out) { out[0] = bi; out[1] = best; out[2] = tdef; out[3] = nc; }
+    if (out) { out[0] = bi; out[1] = best; out[2] = tdef; out[3] = tried; }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     cudaFree(A0); cudaFree(A); cudaFree(U); cudaFree(Vt); cudaFree(sg); cudaFree(ws);

@@ -1,0 +1,330 @@
+// QR-first reduction for tall matrices (M >= 1.6 N by default): A = Q R by
+// blocked Householder QR, then the SVD pipeline runs on the N x N factor R
+// and U = Q * blockdiag(U_R, I).  The reference lists this as future work
+// ("3 step bidiagonalization", README.md:22); it cuts the bandwidth-bound
+// column steps of stage 1 from an M x N to an N x N trailing matrix.
+//
+// qr_block_k   QR of a block of QB = 64 columns, rows [q0, M), in place in
+//              W: one thread-block cluster holds the block's rows in the
+//              shared memory of its CTAs (contiguous chunks, row stride
+//              QB + 1 floats); column by column it forms the reflector of
+//              make_reflector's convention (upper_bidiagonalization.cpp:
+//              182-218: mu = +sqrt, Parlett v0, tau = 2 v0^2/(sigma + v0^2),
+//              implicit v[0] = 1) and applies it to the block's remaining
+//              columns.  The CTAs' partial sums (the column norm, then
+//              v^T A for the remaining columns) are read by every CTA through
+//              distributed shared memory and added in rank order, so each
+//              CTA forms the same reflector; two cluster barriers per column.
+// trailing     A[q0:, q1:N] <- (I - V T^T V^T) A[q0:, q1:N] through the
+//              block-reflector products of stage 1 (Gram on the SIMT engine,
+//              T, then V^T A, T^T G1, A -= V G2 on the tensor cores).
+// U            blockdiag(U_R, I) is written into U, then the reflectors are
+//              applied to it backward in blocks of NBF = 128 (all M columns).
+#include "qr.cuh"
+#include "tma.cuh"
+
+namespace {
+
+constexpr int QT = 256, QW = QT / 32;  // threads and warps per CTA
+
+struct QrArgs {
+    float *W;
+    long ldw;
+    int M, q0, nb, rpc;
+    float *tau;
+};
+
+__device__ __forceinline__ void q_cluster_sync()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t q_dsmem(const void *local, int rank)
+{
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(local)), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ float q_ld(uint32_t addr)
+{
+    float v;
+    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+    return v;
+}
+
+__device__ __forceinline__ unsigned q_rank()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ unsigned q_nrank()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+
+// Sum over the CTA of one value per thread (all threads call it).
+__device__ __forceinline__ float q_block_sum(float v, float *red)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    float t = 0.f;
+#pragma unroll
+    for (int w = 0; w < QW; w++) t += red[w];
+    return t;
+}
+
+__global__ void __launch_bounds__(QT, 1) qr_block_k(QrArgs a)
+{
+    extern __shared__ float qrows[];  // rpc x (QB + 1): this CTA's rows of the block
+    __shared__ float s_sig, s_x0;     // this CTA's partial |x[1:]|^2 and (owner) pivot
+    __shared__ float s_w[QB];         // this CTA's partial v^T A[:, k]
+    __shared__ float wpart[QW][QB];   // per-warp partials
+    __shared__ float red[QW];
+    __shared__ float s_wsum[QB];      // v^T A[:, k] of the current column (all CTAs)
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int rank = (int)q_rank(), CS = (int)q_nrank();
+    const int LD = QB + 1, nb = a.nb;
+    const int r0 = a.q0 + rank * a.rpc;
+    const int nr = max(0, min(a.rpc, a.M - r0));
+    for (int t = tid; t < nr * nb; t += QT) {
+        const int i = t / nb, k = t % nb;
+        qrows[i * LD + k] = a.W[(long)(r0 + i) * a.ldw + a.q0 + k];
+    }
+    __syncthreads();
+    // partial sums of column 0 (rows below its pivot)
+    {
+        float acc = 0.f;
+        for (int i = tid; i < nr; i += QT)
+            if (r0 + i > a.q0) acc += qrows[i * LD] * qrows[i * LD];
+        const float t = q_block_sum(acc, red);
+        if (tid == 0) {
+            s_sig = t;
+            if (a.q0 >= r0 && a.q0 < r0 + nr) s_x0 = qrows[(a.q0 - r0) * LD];
+        }
+    }
+    for (int j = 0; j < nb; j++) {
+        const int pr = a.q0 + j;  // pivot row
+        q_cluster_sync();         // every CTA's sums of column j are published
+        float sig = 0.f;
+        for (int c = 0; c < CS; c++) sig += q_ld(q_dsmem(&s_sig, c));
+        const float x0 = q_ld(q_dsmem(&s_x0, (pr - a.q0) / a.rpc));
+        float beta, tau, v0;
+        make_reflector(x0, sig, a.M - pr, &beta, &tau, &v0);
+        const float inv = 1.f / v0;
+        // v_r = x_r / v0 below the pivot (stored), beta on the diagonal
+        for (int i = tid; i < nr; i += QT) {
+            const int r = r0 + i;
+            if (r > pr) qrows[i * LD + j] *= inv;
+        }
+        __syncthreads();
+        // partial w_k = sum_r v_r A[r, k] over the remaining columns (v_pr = 1)
+        const int kn = nb - j - 1;
+        float acc0 = 0.f, acc1 = 0.f;
+        if (kn > 0) {
+            for (int i = warp; i < nr; i += QW) {
+                const int r = r0 + i;
+                if (r < pr) continue;
+                const float v = (r == pr) ? 1.f : qrows[i * LD + j];
+                const int k0 = j + 1 + lane, k1 = j + 33 + lane;
+                if (k0 < nb) acc0 += v * qrows[i * LD + k0];
+                if (k1 < nb) acc1 += v * qrows[i * LD + k1];
+            }
+            wpart[warp][lane] = acc0;
+            wpart[warp][lane + 32] = acc1;
+        }
+        __syncthreads();
+        if (tid < kn) {
+            float t = 0.f;
+#pragma unroll
+            for (int w = 0; w < QW; w++) t += wpart[w][tid];
+            s_w[tid] = t;
+        }
+        if (tid == 0 && pr >= r0 && pr < r0 + nr) qrows[(pr - r0) * LD + j] = beta;
+        if (tid == 0 && rank == 0) a.tau[pr] = tau;
+        q_cluster_sync();  // every CTA's partial v^T A is published
+        if (kn > 0) {
+            if (tid < kn) {
+                float t = 0.f;
+                for (int c = 0; c < CS; c++) t += q_ld(q_dsmem(&s_w[tid], c));
+                s_wsum[tid] = t * tau;
+            }
+            __syncthreads();
+            // A[r, k] -= tau v_r w_k for the remaining columns; the sums of
+            // column j + 1 (rows below its pivot) on the way
+            float acc = 0.f;
+            for (int i = warp; i < nr; i += QW) {
+                const int r = r0 + i;
+                if (r < pr) continue;
+                const float v = (r == pr) ? 1.f : qrows[i * LD + j];
+                const int k0 = j + 1 + lane, k1 = j + 33 + lane;
+                if (k0 < nb) {
+                    const float x = qrows[i * LD + k0] - v * s_wsum[lane];
+                    qrows[i * LD + k0] = x;
+                    if (lane == 0 && r > pr + 1) acc += x * x;
+                }
+                if (k1 < nb) qrows[i * LD + k1] -= v * s_wsum[lane + 32];
+            }
+            const float t = q_block_sum(acc, red);
+            if (tid == 0) {
+                s_sig = t;
+                if (pr + 1 >= r0 && pr + 1 < r0 + nr) s_x0 = qrows[(pr + 1 - r0) * LD + j + 1];
+            }
+        }
+    }
+    __syncthreads();
+    for (int t = tid; t < nr * nb; t += QT) {
+        const int i = t / nb, k = t % nb;
+        a.W[(long)(r0 + i) * a.ldw + a.q0 + k] = qrows[i * LD + k];
+    }
+    q_cluster_sync();  // no CTA leaves while another may still read its shared memory
+}
+
+// R (N x N, ld N) <- the upper triangle of W[0:N, 0:N]
+__global__ void qr_extract_r(const float *__restrict__ W, long ldw, int N, float *__restrict__ R)
+{
+    const long total = (long)N * N;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        const long r = t / N, c = t % N;
+        R[t] = (c >= r) ? W[r * ldw + c] : 0.f;
+    }
+}
+
+// U (M x M) <- blockdiag(UR (N x N, ld N), I)
+__global__ void qr_blockdiag(const float *__restrict__ UR, int N, int M, float *__restrict__ U)
+{
+    const long total = (long)M * M;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        const long r = t / M, c = t % M;
+        float v;
+        if (r < N && c < N) v = UR[r * N + c];
+        else v = (r == c) ? 1.f : 0.f;
+        U[t] = v;
+    }
+}
+
+struct QrCfg {
+    int cs = 0;        // cluster size that can run (16, 8) or 0
+    int max_smem = 0;  // dynamic shared memory the kernel may use
+};
+
+QrCfg qr_cfg()
+{
+    static QrCfg cfg;
+    static bool done = false;
+    if (done) return cfg;
+    done = true;
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return cfg;
+    }
+    const int smem = optin - 8192;  // room for the static shared memory
+    if (cudaFuncSetAttribute(qr_block_k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+        cudaFuncSetAttribute(qr_block_k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        return cfg;
+    }
+    for (int cs : {16, 8}) {
+        cudaLaunchConfig_t lc = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = cs;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        lc.gridDim = dim3(cs);
+        lc.blockDim = dim3(QT);
+        lc.dynamicSmemBytes = smem;
+        lc.attrs = at;
+        lc.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, qr_block_k, &lc) == cudaSuccess && n >= 1) {
+            cfg.cs = cs;
+            cfg.max_smem = smem;
+            break;
+        }
+        cudaGetLastError();
+    }
+    return cfg;
+}
+
+size_t qr_smem_bytes(int rows, int cs)
+{
+    const int rpc = (rows + cs - 1) / cs;
+    return sizeof(float) * (size_t)rpc * (QB + 1);
+}
+
+}  // namespace
+
+void qr_init() { (void)qr_cfg(); }
+
+bool qr_fits(int M, int N)
+{
+    const QrCfg cfg = qr_cfg();
+    return cfg.cs > 0 && N >= 1 && M >= N && qr_smem_bytes(M, cfg.cs) <= (size_t)cfg.max_smem;
+}
+
+// The columns of W (M x ldw, already holding A) become R (upper triangle) and
+// the Householder vectors (below the diagonal); tau[N] receives the scalars.
+int qr_factor(const BdWs &w, int M, int N, float *tau, cudaStream_t s)
+{
+    const QrCfg cfg = qr_cfg();
+    if (!qr_fits(M, N)) return PACO_ERR_UNSUPPORTED;
+    for (int q0 = 0; q0 < N; q0 += QB) {
+        const int nb = std::min(QB, N - q0), rows = M - q0;
+        QrArgs a;
+        a.W = w.W; a.ldw = w.ldw; a.M = M; a.q0 = q0; a.nb = nb;
+        a.rpc = (rows + cfg.cs - 1) / cfg.cs;
+        a.tau = tau;
+        cudaLaunchConfig_t lc = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = cfg.cs;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        lc.gridDim = dim3(cfg.cs);
+        lc.blockDim = dim3(QT);
+        lc.dynamicSmemBytes = qr_smem_bytes(rows, cfg.cs);
+        lc.stream = s;
+        lc.attrs = at;
+        lc.numAttrs = 1;
+        paco_count_launch();
+        if (cudaLaunchKernelEx(&lc, qr_block_k, a) != cudaSuccess) {
+            cudaGetLastError();
+            return PACO_ERR_CUDA;
+        }
+        const int q1 = q0 + nb;
+        if (q1 < N) {
+            bd_column_vectors(w.W, w.ldw, q0, nb, rows, w.Vp, s);
+            if (apply_block_reflector_ex(w, w.W, w.ldw, q0, rows, q1, N - q1, nb, tau + q0, true, s) != cudaSuccess)
+                return PACO_ERR_CUDA;
+        }
+    }
+    return cudaGetLastError() == cudaSuccess ? PACO_OK : PACO_ERR_CUDA;
+}
+
+void qr_extract_r_launch(const BdWs &w, int N, float *R, cudaStream_t s)
+{
+    paco_count_launch(), qr_extract_r<<<std::min(8192, ceil_div((long)N * N, 256)), 256, 0, s>>>(w.W, w.ldw, N, R);
+}
+
+// U (M x M) <- Q blockdiag(UR, I), Q = H_0 ... H_{N-1} from qr_factor
+int qr_form_u(const BdWs &w, int M, int N, const float *tau, const float *UR, float *U, cudaStream_t s)
+{
+    paco_count_launch(), qr_blockdiag<<<std::min(8192, ceil_div((long)M * M, 256)), 256, 0, s>>>(UR, N, M, U);
+    for (int p0 = ((N - 1) / bd::NBF) * bd::NBF; p0 >= 0; p0 -= bd::NBF) {
+        const int nbp = std::min(N, p0 + bd::NBF) - p0, Lp = M - p0;
+        bd_column_vectors(w.W, w.ldw, p0, nbp, Lp, w.Vp, s);
+        if (apply_block_reflector_ex(w, U, M, p0, Lp, 0, M, nbp, tau + p0, false, s) != cudaSuccess)
+            return PACO_ERR_CUDA;
+    }
+    return cudaGetLastError() == cudaSuccess ? PACO_OK : PACO_ERR_CUDA;
+}

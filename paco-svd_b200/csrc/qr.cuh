@@ -1,0 +1,21 @@
+// QR-first reduction of tall matrices (qr.cu): blocked Householder QR with
+// the blocks factored on one thread-block cluster, and the formation of
+// U = Q blockdiag(U_R, I) after the SVD of R.
+#pragma once
+
+#include "bidiag.cuh"
+
+constexpr int QB = 64;  // columns per QR block
+
+// Set-up of the cluster kernel (once per device, outside stream capture).
+void qr_init();
+// True when the cluster kernel can hold an M-row block of QB columns.
+bool qr_fits(int M, int N);
+// W of the stage-1 workspace w (M x ldw, holding A) <- R in its upper
+// triangle and the Householder vectors below the diagonal; tau[N] the
+// scalars.  Enqueued on s.
+int qr_factor(const BdWs &w, int M, int N, float *tau, cudaStream_t s);
+// R (N x N, ld N) <- the upper triangle of W[0:N, 0:N].
+void qr_extract_r_launch(const BdWs &w, int N, float *R, cudaStream_t s);
+// U (M x M) <- Q blockdiag(UR, I) with Q from qr_factor and UR N x N (ld N).
+int qr_form_u(const BdWs &w, int M, int N, const float *tau, const float *UR, float *U, cudaStream_t s);

@@ -89,6 +89,8 @@ def lib():
         L.paco_svd_multi.argtypes = [i, i, i, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
                                      ctypes.POINTER(vp), vp, vp, ctypes.c_size_t, vp]
         L.paco_svd_multi.restype = i
+        L.paco_tune_qr.argtypes = [i, i, i]
+        L.paco_tune_qr.restype = i
         L.paco_multi_group.argtypes = [i]
         L.paco_multi_group.restype = i
         _lib = L
@@ -260,6 +262,15 @@ def tune_get(M: int, N: int):
     cfg = (ctypes.c_int * 4)()
     _check(lib().paco_tune_get(M, N, cfg), "paco_tune_get")
     return list(cfg)
+
+
+def tune_qr(M: int, N: int, mode: int = -1) -> int:
+    """QR-first choice for (M, N): 0 off, 1 on, 2 automatic (M >= 1.6 N);
+    -1 queries.  Applies to M > N with N >= 1024."""
+    r = int(lib().paco_tune_qr(M, N, int(mode)))
+    if r < 0:
+        raise PacoError(PACO_ERR_INVALID_ARG, "paco_tune_qr")
+    return r
 
 
 def tune_set(M: int, N: int, cfg) -> None:

@@ -15,6 +15,8 @@ WORKLOADS = {
     "cfg3": dict(M=8192, N=4096, gen="clustered"),
     # batched form: 10,000 matrices, M uniform on [32, 512], N uniform on [16, M], iid N(0,1)
     "cfg4": dict(kind="batched", count=10000, Mlo=32, Mhi=512, Nlo=16, gen="normal"),
+    # multi-matrix form: 8 matrices of the precision-form configuration per call
+    "cfg3x8": dict(kind="multi", M=8192, N=4096, count=8, gen="clustered"),
     # serving form: Poisson requests at 2,000/s for 60 s, 90% M log-uniform on [16, 256], 10% on
     # [256, 2048], N uniform on [M/4, M], 20% graded spectra, 64 GB device working-set cap
     "cfg5": dict(kind="serving", rate=2000.0, seconds=60.0, cap_gb=64),
@@ -55,3 +57,23 @@ def batched_shapes(wl, seed):
         M = int(rng.integers(wl["Mlo"], wl["Mhi"] + 1))
         out.append((M, int(rng.integers(wl["Nlo"], M + 1))))
     return out
+
+
+def make_clustered_device(M, N, seed, device="cuda"):
+    """The clustered-spectrum generator of make_matrix on the GPU (torch, FP64
+    QR of seeded Gaussians, cast to FP32), for workloads that need many such
+    matrices: 512 clusters of 8 (for N = 4096), centres log-uniform in
+    [1e-4, 1], relative spacing 1e-7.  Returns (A, exact sigma descending)."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+
+    def haar(n, m):
+        Q, R = torch.linalg.qr(torch.randn(n, m, generator=g, device=device, dtype=torch.float64))
+        return Q * torch.sign(torch.diagonal(R))[None, :]
+
+    centres = 10.0 ** (4.0 * torch.rand(N // 8, generator=g, device=device, dtype=torch.float64) - 4.0)
+    steps = 1.0 + 1e-7 * torch.arange(8, device=device, dtype=torch.float64)
+    sig = torch.sort((centres[:, None] * steps[None, :]).reshape(-1), descending=True).values
+    A = ((haar(M, N) * sig[None, :]) @ haar(N, N).T).float()
+    return A, sig.cpu().numpy()

@@ -82,3 +82,19 @@ def test_batched_rejects_mixed_large_shapes():
     with pytest.raises(P.PacoError) as ei:
         P.Batch([(2100, 700), (300, 200)])
     assert ei.value.code == P.PACO_ERR_UNSUPPORTED
+
+
+def test_multi_with_qr_first_matches_lapack():
+    # tall shape: every matrix takes the QR-first path (QR per matrix on its
+    # own stream, stage 1 of the R factors in lockstep)
+    rng = np.random.default_rng(11)
+    M, N = 2300, 1100
+    As = [rng.standard_normal((M, N)).astype(np.float32) if k != 1 else graded(rng, M, N) for k in range(3)]
+    prev = P.multi_group(2)
+    try:
+        s, U, Vt, st = P.svd_multi(As)
+    finally:
+        P.multi_group(prev)
+    assert st == [0, 0, 0]
+    for k in range(3):
+        check(As[k], s[k], U[k], Vt[k])
