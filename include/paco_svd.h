@@ -132,7 +132,9 @@ void paco_ctx_destroy(paco_ctx *ctx);
  * PACO_ERR_UNSUPPORTED).  All scratch lives in a 16 MiB device array inside
  * the library, which every GPU that loads the library holds until the process
  * exits; no device memory is allocated per call.  The first call on a device
- * looks up that array's address (make it before any stream capture).  Calls
+ * looks up that array's address (make it before any stream capture) and keeps
+ * it for the life of the process, so a device reset with cudaDeviceReset
+ * must not be followed by further calls on that device.  Calls
  * share the array: calls that overlap on the GPU, from any stream or thread,
  * race and must be serialized by the caller.  The call synchronizes `stream`
  * and returns the device status of the run. */

@@ -887,14 +887,14 @@ static bool bt_plan(int count, const int *M, const int *N, BtPlan *p)
         cudaGetLastError();
         sms = 148;
     }
-    static bool attr = false;
-    if (!attr) {
+    static bool attr[PACO_MAX_DEVICES] = {};
+    if (!attr[paco_device()]) {
         cudaFuncSetAttribute(bt_bdc_k, cudaFuncAttributeMaxDynamicSharedMemorySize, 48 * 1024);
         const int big = (int)bt_sweep_smem(PACO_BATCH_MAX_M);
         cudaFuncSetAttribute(bt_bidiag_k, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         cudaFuncSetAttribute(bt_apply_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bt_apply_smem());
         cudaGetLastError();
-        attr = true;
+        attr[paco_device()] = true;
     }
     p->maxc1 = (Nx + 31) & ~31;
     p->maxc3 = (Mx + 31) & ~31;

@@ -172,7 +172,7 @@ size_t bdc_workspace_bytes(int M, int N)
     return bdc_carve(nullptr, M, N, &w);
 }
 
-static bool bdc_attrs_set = false;
+static bool bdc_attrs_set[PACO_MAX_DEVICES] = {};
 
 // Sets this unit's secular iteration limit (a test hook; synchronous).
 void bdc_set_sec_maxit(int n)
@@ -182,10 +182,11 @@ void bdc_set_sec_maxit(int n)
 
 void bdc_init_attrs()
 {
-    if (!bdc_attrs_set) {
+    const int dev = paco_device();
+    if (!bdc_attrs_set[dev]) {
         cudaFuncSetAttribute(bdc_prepare, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         gemm_tc_init_attrs();
-        bdc_attrs_set = true;
+        bdc_attrs_set[dev] = true;
     }
 }
 

@@ -747,10 +747,11 @@ static void rp_launch(const BdArgs &a, int i, int p0, int mode, int G, cudaStrea
     else launch_rp<4>(a, i, p0, mode, G, R, L, s);
 }
 
-static bool rp_attrs_set = false;
+static bool rp_attrs_set[PACO_MAX_DEVICES] = {};
 void bd_init_attrs()
 {
-    if (rp_attrs_set) return;
+    const int dev = paco_device();
+    if (rp_attrs_set[dev]) return;
     int maxs = 200 * 1024;
     cudaFuncSetAttribute(bd_row_pass<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
     cudaFuncSetAttribute(bd_row_pass<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
@@ -760,7 +761,7 @@ void bd_init_attrs()
     bd_tail_init();
     qr_init();
     bd_fork_events();
-    rp_attrs_set = true;
+    rp_attrs_set[dev] = true;
 }
 
 // Stage 1 of k matrices of one shape (jobs[0..k)): set-up, the panels in

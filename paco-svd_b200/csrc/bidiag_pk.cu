@@ -670,8 +670,9 @@ bool bd_pk_debug_timeout(PkCtl *ctl, DevStatus *st, int G, long long max_cycles,
 
 void bd_pk_init_attrs()
 {
-    static bool done = false;
-    if (done) return;
+    static bool done[PACO_MAX_DEVICES] = {};
+    const int dev = paco_device();
+    if (done[dev]) return;
     int maxs = 200 * 1024 + PK_XOWN * NB * 4 + 1024;
     cudaFuncSetAttribute(bd_panel_pk<1, PK_RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
     cudaFuncSetAttribute(bd_panel_pk<2, PK_RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
@@ -679,5 +680,5 @@ void bd_pk_init_attrs()
     cudaFuncSetAttribute(bd_panel_pk<1, RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
     cudaFuncSetAttribute(bd_panel_pk<2, RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
     cudaFuncSetAttribute(bd_panel_pk<4, RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
-    done = true;
+    done[dev] = true;
 }

@@ -299,10 +299,12 @@ struct TailCfg {
 
 TailCfg tail_cfg()
 {
-    static TailCfg cfg;
-    static bool done = false;
-    if (done) return cfg;
-    done = true;
+    static TailCfg cfgs[PACO_MAX_DEVICES];
+    static bool done[PACO_MAX_DEVICES] = {};
+    const int devi = paco_device();
+    TailCfg &cfg = cfgs[devi];
+    if (done[devi]) return cfg;
+    done[devi] = true;
     int dev = 0, optin = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {

@@ -85,6 +85,16 @@ static unsigned long long g_launches = 0;
 static int g_prof_on = 0;
 void paco_count_launch() { g_launches++; }
 
+int paco_device()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        dev = 0;
+    }
+    return (dev >= 0 && dev < PACO_MAX_DEVICES) ? dev : 0;
+}
+
 // ------------------------------------------------ tiling autotuner state
 // The reference fixes its tiling on the host (svd_tiling.cpp:11-66: one
 // 1024^3 matmul tile and the leaf partition).  Here the shape-dependent

@@ -73,6 +73,12 @@ __device__ __forceinline__ bool last_block_ticket(int *counter, int nblocks, int
 // Host-side count of kernel launches issued by the library (paco_launch_count).
 void paco_count_launch();
 
+// Ordinal of the current device (0..PACO_MAX_DEVICES-1): the index of the
+// per-device caches (kernel attributes, launch configurations, SM counts) a
+// process that drives several GPUs keeps apart.
+#define PACO_MAX_DEVICES 64
+int paco_device();
+
 // Shape-dependent choices of the single-matrix path (the tiling autotuner's
 // output, paco_autotune): the persistent panel kernel or the two-kernel row /
 // column passes, rows per CTA of a panel (sets the grid: fewer CTAs meet at

@@ -577,14 +577,14 @@ static size_t tc_p_smem_bytes() { return tc_smem_bytes() + 4 * 32 * 33 * sizeof(
 
 static int tc_sms()
 {
-    static int n = 0;
-    if (!n) {
-        int dev = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) !=
-                                                      cudaSuccess || n < 1)
-            n = 148;
+    static int sms[PACO_MAX_DEVICES] = {};
+    const int dev = paco_device();
+    if (!sms[dev]) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = 148;
+        sms[dev] = n;
     }
-    return n;
+    return sms[dev];
 }
 
 // Tensor map of C (FP32, M rows of N columns, row stride ldc floats) with a

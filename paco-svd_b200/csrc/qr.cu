@@ -217,10 +217,12 @@ struct QrCfg {
 
 QrCfg qr_cfg()
 {
-    static QrCfg cfg;
-    static bool done = false;
-    if (done) return cfg;
-    done = true;
+    static QrCfg cfgs[PACO_MAX_DEVICES];
+    static bool done[PACO_MAX_DEVICES] = {};
+    const int devi = paco_device();
+    QrCfg &cfg = cfgs[devi];
+    if (done[devi]) return cfg;
+    done[devi] = true;
     int dev = 0, optin = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
