@@ -70,8 +70,10 @@ int paco_tune_set(int M, int N, const int cfg[4]);
  * the N x N factor R, U = Q blockdiag(U_R, I).  It applies to shapes with
  * M > N and N >= 1024 whose QR blocks fit one thread-block cluster (M up to
  * about 13,000); mode 0 = off, 1 = on, 2 = automatic (on when M >= 1.6 N, the
- * default), -1 = query.  paco_autotune times both choices for such shapes.
- * Returns the mode stored (or queried), -1 for an invalid argument. */
+ * default), -1 = query the mode, -2 = query whether calls of this shape take
+ * the QR-first path now (1) or not (0).  paco_autotune times both choices for
+ * such shapes.  Returns the mode stored (or the answer), -1 for an invalid
+ * argument. */
 int paco_tune_qr(int M, int N, int mode);
 
 /* Buffer sizes in bytes of main.cpp:33-43, in this order:

@@ -768,8 +768,9 @@ void bd_init_attrs()
 // lockstep (one persistent panel launch serves every matrix, G = num_sms / k
 // CTAs each; the last columns of every matrix on its own cluster launch, on
 // side[j] when k > 1), the trailing updates, the formation of U and V.
-int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s, cudaStream_t *side, int num_sms)
+int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s0, cudaStream_t *side, int num_sms)
 {
+    cudaStream_t s = s0;
     if (k < 1 || k > PK_KMAX) return PACO_ERR_INVALID_ARG;
     const int M = jobs[0].M, N = jobs[0].N;
     for (int j = 1; j < k; j++)
@@ -787,6 +788,7 @@ int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s, cudaStream_t *side, i
     BdArgs a[PK_KMAX];
     PkCtl *ctl[PK_KMAX];
     unsigned pk_cnt[PK_KMAX]; // arrivals on each matrix's barrier counter so far
+    unsigned pk_ep[PK_KMAX];  // epochs of each matrix's tagged hand-overs so far
     for (int j = 0; j < k; j++) {
         const BdJob &J = jobs[j];
         bd_carve(J.workspace, M, N, &w[j]);
@@ -798,10 +800,12 @@ int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s, cudaStream_t *side, i
         x.sc = w[j].sc;
         x.d = J.d; x.e = J.e; x.tauq = J.tauq; x.taup = J.taup;
         x.bcA = w[j].bcA; x.bcB = w[j].bcB;
+        x.cpart_t = w[j].cpart_t; x.bcB_t = w[j].bcB_t; x.rowbuf_t = w[j].rowbuf_t;
         x.trace = (trace_env >= 0 && j == 0) ? w[j].trace : nullptr;
         x.trace_p0 = trace_env;
         ctl[j] = w[j].ctl;
         pk_cnt[j] = 0;
+        pk_ep[j] = 0;
     }
 
     const int gmax = std::max(1, std::min(RB_CAP, num_sms / k));
@@ -818,6 +822,10 @@ int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s, cudaStream_t *side, i
     for (int j = 0; j < k; j++) {
         cudaMemsetAsync(w[j].st->counters, 0, sizeof(w[j].st->counters), s);
         cudaMemsetAsync(w[j].ctl, 0, sizeof(PkCtl), s);
+        // tagged hand-overs start at epoch 1 each run: no stale word can match
+        cudaMemsetAsync(w[j].cpart_t, 0, sizeof(unsigned long long) * (size_t)PR * PCAP, s);
+        cudaMemsetAsync(w[j].bcB_t, 0, sizeof(unsigned long long) * PR, s);
+        cudaMemsetAsync(w[j].rowbuf_t, 0, sizeof(unsigned long long) * (size_t)w[j].ldw, s);
         cudaMemsetAsync(w[j].Yt, 0, sizeof(float) * NB * w[j].ldw, s);
         cudaMemsetAsync(w[j].X, 0, sizeof(float) * (size_t)M * NB, s);
         paco_count_launch(), bd_copy_in<<<std::min(4096, ceil_div((long)M * w[j].ldw, 256)), 256, 0, s>>>(
@@ -870,7 +878,7 @@ int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s, cudaStream_t *side, i
         if (use_pk) {
             cudaEvent_t e0 = nullptr, e1 = nullptr;
             if (g_prof.on) prof_record(e0 = prof_event(), s);
-            pk = bd_panel_pk_launch_multi(k, a, ctl, p0, p1, Gp, pk_cnt, s);
+            pk = bd_panel_pk_launch_multi(k, a, ctl, p0, p1, Gp, pk_cnt, pk_ep, s);
             if (g_prof.on) {
                 prof_record(e1 = prof_event(), s);
                 g_prof.cur.ev.push_back(e0);
@@ -906,9 +914,12 @@ int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s, cudaStream_t *side, i
         }
     }
 
+    // the formation of U and V: each matrix on its own side stream (k > 1)
+    if (k > 1) fork();
     for (int j = 0; j < k; j++) {
         const BdWs &x = w[j];
         const BdJob &J = jobs[j];
+        cudaStream_t s = (k > 1) ? side[j] : s0;
         // U = H_0 ... H_{N-1} (backward accumulation of the column reflectors,
         // NBF reflectors per block update)
         paco_count_launch(), bd_set_identity<<<std::min(8192, ceil_div((long)M * M, 256)), 256, 0, s>>>(J.u, M, M);
@@ -928,11 +939,11 @@ int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s, cudaStream_t *side, i
             apply_block_reflector(x, x.Vtmp, N, p0 + 1, Lp, nbp, J.taup + p0, s);
         }
         paco_count_launch(), bd_transpose<<<dim3(ceil_div(N, 32), ceil_div(N, 32)), dim3(32, 8), 0, s>>>(x.Vtmp, J.vt, N);
-    }
-    prof_end();
-    for (int j = 0; j < k; j++)
         paco_count_launch(), bd_copy_out<<<std::min(4096, ceil_div((long)M * N, 256)), 256, 0, s>>>(
-            jobs[j].a_out, w[j].W, M, N, w[j].ldw, jobs[j].d, jobs[j].e);
+            J.a_out, x.W, M, N, x.ldw, J.d, J.e);
+    }
+    if (k > 1) join();
+    prof_end();
     return cudaGetLastError() == cudaSuccess ? PACO_OK : PACO_ERR_CUDA;
 }
 

@@ -398,8 +398,9 @@ size_t paco_svd_workspace_size(int M, int N)
 
 int paco_tune_qr(int M, int N, int mode)
 {
-    if (!shape_ok(M, N) || mode < -1 || mode > 2) return -1;
+    if (!shape_ok(M, N) || mode < -2 || mode > 2) return -1;
     if (mode == -1) return qr_mode_for(M, N);
+    if (mode == -2) return qr_chosen(M, N) ? 1 : 0;
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         bool found = false;
@@ -438,6 +439,30 @@ static int svd_direct_qr(int M, int N, const float *A, float *U, float *Vt, floa
                  b + L.ws, nullptr, s);
     if (rc) return rc;
     return qr_form_u(wq, M, N, tau, UR, U, s);
+}
+
+// Test hook (not part of the public header): the QR-first path's R factor
+// (N x N, ld N, zeros below the diagonal) of A (M x N, M > N, N >= 1024);
+// ws holds paco_svd_workspace_size(M, N) bytes.  Synchronous.
+extern "C" int paco_debug_qr_r(int M, int N, const float *A, float *R, void *ws, size_t ws_bytes, void *stream)
+{
+    if (!shape_ok(M, N) || !qr_possible(M, N) || !qr_fits(M, N) || !A || !R || !ws ||
+        ws_bytes < paco_svd_workspace_size(M, N))
+        return PACO_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    char *b = (char *)ws;
+    const QrLayout Q = qr_layout(M, N);
+    DevStatus *st = (DevStatus *)(b + Q.LR.ws);
+    BdWs wq;
+    bd_carve(b + Q.bw, M, N, &wq);
+    wq.st = st;
+    bd_init_attrs();
+    cudaMemsetAsync(st, 0, sizeof(DevStatus), s);
+    bd_copy_in_launch(A, wq.W, M, N, wq.ldw, st, s);
+    int rc = qr_factor(wq, M, N, (float *)(b + Q.tau), s);
+    if (rc) return rc;
+    qr_extract_r_launch(wq, N, R, s);
+    return paco_sync_status(ws, stream, nullptr);
 }
 
 static int svd_direct(int M, int N, float *A, float *U, float *Vt, float *sigma, char *b, const SvdLayout &L,

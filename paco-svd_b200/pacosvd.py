@@ -266,7 +266,8 @@ def tune_get(M: int, N: int):
 
 def tune_qr(M: int, N: int, mode: int = -1) -> int:
     """QR-first choice for (M, N): 0 off, 1 on, 2 automatic (M >= 1.6 N);
-    -1 queries.  Applies to M > N with N >= 1024."""
+    -1 queries the mode, -2 whether calls of this shape take the QR-first
+    path now.  Applies to M > N with N >= 1024."""
     r = int(lib().paco_tune_qr(M, N, int(mode)))
     if r < 0:
         raise PacoError(PACO_ERR_INVALID_ARG, "paco_tune_qr")
