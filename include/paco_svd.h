@@ -118,6 +118,16 @@ size_t paco_svd_workspace_size(int M, int N);
 int paco_svd(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws,
              size_t ws_bytes, void *stream);
 
+/* Thin-U form of paco_svd: U is M x N, the first N left singular vectors
+ * (A = U diag(sigma) Vt), where the reference always forms the M x M U
+ * (main.cpp:33,173).  The reflectors are applied to [I; 0] (or, for a tall
+ * matrix on the QR-first path, to [U_R; 0]) instead of forming M x M
+ * products: for M = 2N about a third of the formation's multiply-adds and
+ * half of U's memory.  Same workspace (paco_svd_workspace_size) and rules as
+ * paco_svd. */
+int paco_svd_thin(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws,
+                  size_t ws_bytes, void *stream);
+
 /* Host-buffer SVD through a reusable context (device buffers and pinned
  * staging allocated once): copies A to the device, runs both stages, copies
  * U, Vt, sigma back, synchronizes.  The path svd_main takes (main.cpp:64-174). */

@@ -191,8 +191,9 @@ void bdc_init_attrs()
 }
 
 int bdc_run(int M, int N, float *a, float *u, float *vt, float *d, float *e, float *qt, float *wt, uint32_t *idx,
-            void *workspace, const uint8_t *tiling, cudaStream_t s)
+            void *workspace, const uint8_t *tiling, cudaStream_t s, long ldu)
 {
+    const long lu = ldu > 0 ? ldu : M;
     BdcWs w;
     bdc_carve(workspace, M, N, &w);
     bdc_init_attrs();
@@ -250,8 +251,8 @@ int bdc_run(int M, int N, float *a, float *u, float *vt, float *d, float *e, flo
     }
     paco_count_launch(), bdc_sort_desc<<<ceil_div(N, 256), 256, 0, s>>>(N, d, w.perm, w.sig);
     // U[:, :N] <- U[:, :N] Q with Q(:, r) = qt row perm[r]; result staged in a (M x N)
-    gemm_any(M, N, N, 1.f, gop(u, M, 1), gop(qt, 1, N, w.perm), 0.f, a, N, 1, nullptr, w.tcs, w.tcs_floats, w.st, s);
-    paco_count_launch(), bdc_copy_cols<<<std::min(8192, ceil_div((long)M * N, 256)), 256, 0, s>>>(a, N, u, M, M, N);
+    gemm_any(M, N, N, 1.f, gop(u, lu, 1), gop(qt, 1, N, w.perm), 0.f, a, N, 1, nullptr, w.tcs, w.tcs_floats, w.st, s);
+    paco_count_launch(), bdc_copy_cols<<<std::min(8192, ceil_div((long)M * N, 256)), 256, 0, s>>>(a, N, u, lu, M, N);
     // Vt <- W^T Vt with W^T row r = wt row perm[r]; staged in Us
     gemm_any(N, N, N, 1.f, gop(wt, N, 1, w.perm), gop(vt, N, 1), 0.f, w.Us, N, 1, nullptr, w.tcs, w.tcs_floats, w.st,
              s);

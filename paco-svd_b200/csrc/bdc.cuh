@@ -98,5 +98,7 @@ void bdc_init_attrs();
 // (batched.cu) kernels; a test hook that forces the non-convergence report.
 void bdc_set_sec_maxit(int n);
 void bt_set_sec_maxit(int n);
+// u holds U with ldu floats per row (ldu = M for the M x M U; N for the thin
+// M x N U of paco_svd_thin); only its first N columns are read and written.
 int bdc_run(int M, int N, float *a, float *u, float *vt, float *d, float *e, float *qt, float *wt, uint32_t *idx,
-            void *workspace, const uint8_t *tiling, cudaStream_t s);
+            void *workspace, const uint8_t *tiling, cudaStream_t s, long ldu = 0);

@@ -79,6 +79,14 @@ __global__ void bd_set_identity(float *Q, long n, long ld)
     }
 }
 
+// Q (rows x cols, ld cols) <- the rows x cols block of the identity
+__global__ void bd_set_eye(float *Q, long rows, long cols)
+{
+    long total = rows * cols;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x)
+        Q[t] = (t / cols == t % cols) ? 1.f : 0.f;
+}
+
 __global__ void bd_transpose(const float *__restrict__ src, float *__restrict__ dst, int n)
 {
     __shared__ float tile[32][33];
@@ -922,12 +930,14 @@ int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s0, cudaStream_t *side, 
         cudaStream_t s = (k > 1) ? side[j] : s0;
         // U = H_0 ... H_{N-1} (backward accumulation of the column reflectors,
         // NBF reflectors per block update)
-        paco_count_launch(), bd_set_identity<<<std::min(8192, ceil_div((long)M * M, 256)), 256, 0, s>>>(J.u, M, M);
+        const int uc = J.thin ? N : M;  // columns of U formed
+        paco_count_launch(), bd_set_eye<<<std::min(8192, ceil_div((long)M * uc, 256)), 256, 0, s>>>(J.u, M, uc);
         for (int p0 = ((N - 1) / NBF) * NBF; p0 >= 0; p0 -= NBF) {
             int nbp = std::min(N, p0 + NBF) - p0, Lp = M - p0;
             paco_count_launch(), bd_panel_vectors<<<std::min(4096, ceil_div((long)Lp * NBF, 256)), 256, 0, s>>>(
                 x.W, x.ldw, p0, nbp, Lp, 0, x.Vp);
-            apply_block_reflector(x, J.u, M, p0, Lp, nbp, J.tauq + p0, s);
+            // columns < p0 of [I; 0] have no entries in rows >= p0: the block leaves them
+            apply_block_reflector_ex(x, J.u, uc, p0, Lp, p0, uc - p0, nbp, J.tauq + p0, false, s);
         }
         // V = G_0 ... G_{N-2} (row reflectors), then Vt = V^T
         paco_count_launch(), bd_set_identity<<<std::min(8192, ceil_div((long)N * N, 256)), 256, 0, s>>>(x.Vtmp, N, N);
@@ -950,7 +960,7 @@ int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s0, cudaStream_t *side, 
 int bd_run(int M, int N, const float *a_in, float *a_out, float *u, float *vt, float *d, float *e, float *tauq,
            float *taup, void *workspace, cudaStream_t s, int num_sms)
 {
-    BdJob job = {M, N, a_in, a_out, u, vt, d, e, tauq, taup, workspace};
+    BdJob job = {M, N, a_in, a_out, u, vt, d, e, tauq, taup, workspace, 0};
     return bd_run_multi(1, &job, s, nullptr, num_sms);
 }
 

@@ -211,6 +211,7 @@ struct BdJob {
     const float *a_in;
     float *a_out, *u, *vt, *d, *e, *tauq, *taup;
     void *workspace;
+    int thin;  // 1: u is the M x N thin U (ld N), U[:, :N] = H_0 ... H_{N-1} [I; 0]
 };
 // Stage 1 of k <= PK_KMAX matrices of one shape, the panels of all of them in
 // lockstep (one persistent panel launch per panel serves every matrix); the

@@ -415,7 +415,7 @@ int paco_tune_qr(int M, int N, int mode)
 // QR-first SVD of a tall matrix: A = Q R, the one-matrix pipeline on R
 // (N x N), then U = Q blockdiag(U_R, I).  A is read only.
 static int svd_direct_qr(int M, int N, const float *A, float *U, float *Vt, float *sigma, char *b,
-                         const QrLayout &Q, void *stream)
+                         const QrLayout &Q, void *stream, bool thin = false)
 {
     cudaStream_t s = (cudaStream_t)stream;
     const SvdLayout &L = Q.LR;
@@ -438,7 +438,24 @@ static int svd_direct_qr(int M, int N, const float *A, float *U, float *Vt, floa
     rc = bdc_run(N, N, AR, UR, Vt, sigma, e, (float *)(b + L.qt), (float *)(b + L.wt), (uint32_t *)(b + L.idx),
                  b + L.ws, nullptr, s);
     if (rc) return rc;
-    return qr_form_u(wq, M, N, tau, UR, U, s);
+    return qr_form_u(wq, M, N, tau, UR, U, s, thin ? N : M);
+}
+
+// One-stage SVD with the thin U (M x N): stage 1 forms H_0 ... H_{N-1} [I; 0]
+// only, and stage 2 updates those N columns.
+static int svd_direct_thin(int M, int N, float *A, float *U, float *Vt, float *sigma, char *b, const SvdLayout &L,
+                           void *stream)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    float *e = (float *)(b + L.e), *tq = (float *)(b + L.tauq), *tp = (float *)(b + L.taup);
+    DevStatus *st = (DevStatus *)(b + L.ws);
+    paco_count_launch(), dev_status_begin<<<1, 64, 0, s>>>(st, 1);
+    BdJob job = {M, N, A, A, U, Vt, sigma, e, tq, tp, b + L.ws, 1};
+    int rc = bd_run_multi(1, &job, s, nullptr, device_sms());
+    if (rc) return rc;
+    paco_count_launch(), dev_status_begin<<<1, 64, 0, s>>>(st, 2);
+    return bdc_run(M, N, A, U, Vt, sigma, e, (float *)(b + L.qt), (float *)(b + L.wt), (uint32_t *)(b + L.idx),
+                   b + L.ws, nullptr, s, N);
 }
 
 // Test hook (not part of the public header): the QR-first path's R factor
@@ -478,9 +495,11 @@ static int svd_direct(int M, int N, float *A, float *U, float *Vt, float *sigma,
 // The single-matrix SVD in the configuration of (M, N): QR-first for tall
 // matrices when chosen, otherwise the one-stage pipeline.  b holds
 // paco_svd_workspace_size(M, N) bytes.
-static int svd_any(int M, int N, float *A, float *U, float *Vt, float *sigma, char *b, void *stream)
+static int svd_any(int M, int N, float *A, float *U, float *Vt, float *sigma, char *b, void *stream,
+                   bool thin = false)
 {
-    if (qr_chosen(M, N)) return svd_direct_qr(M, N, A, U, Vt, sigma, b, qr_layout(M, N), stream);
+    if (qr_chosen(M, N)) return svd_direct_qr(M, N, A, U, Vt, sigma, b, qr_layout(M, N), stream, thin);
+    if (thin) return svd_direct_thin(M, N, A, U, Vt, sigma, b, svd_layout(M, N), stream);
     return svd_direct(M, N, A, U, Vt, sigma, b, svd_layout(M, N), stream);
 }
 
@@ -581,6 +600,19 @@ int paco_svd(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws
     const std::vector<uintptr_t> key = {1, (uintptr_t)M, (uintptr_t)N, (uintptr_t)A, (uintptr_t)U, (uintptr_t)Vt,
                                         (uintptr_t)sigma, (uintptr_t)ws};
     return run_cached(key, (cudaStream_t)stream, [&]() { return svd_any(M, N, A, U, Vt, sigma, b, stream); });
+}
+
+int paco_svd_thin(int M, int N, float *A, float *U, float *Vt, float *sigma, void *ws, size_t ws_bytes,
+                  void *stream)
+{
+    if (!shape_ok(M, N)) return (N >= 1 && M >= N) ? PACO_ERR_UNSUPPORTED : PACO_ERR_INVALID_ARG;
+    if (!A || !U || !Vt || !sigma || !ws) return PACO_ERR_INVALID_ARG;
+    if (ws_bytes < paco_svd_workspace_size(M, N)) return PACO_ERR_INVALID_ARG;
+    char *b = (char *)ws;
+    const std::vector<uintptr_t> key = {3, (uintptr_t)M, (uintptr_t)N, (uintptr_t)A, (uintptr_t)U, (uintptr_t)Vt,
+                                        (uintptr_t)sigma, (uintptr_t)ws};
+    return run_cached(key, (cudaStream_t)stream,
+                      [&]() { return svd_any(M, N, A, U, Vt, sigma, b, stream, true); });
 }
 
 // ------------------------------------------------ multi-matrix form

@@ -197,12 +197,12 @@ __global__ void qr_extract_r(const float *__restrict__ W, long ldw, int N, float
     }
 }
 
-// U (M x M) <- blockdiag(UR (N x N, ld N), I)
-__global__ void qr_blockdiag(const float *__restrict__ UR, int N, int M, float *__restrict__ U)
+// U (M x uc, ld uc) <- the first uc columns of blockdiag(UR (N x N, ld N), I)
+__global__ void qr_blockdiag(const float *__restrict__ UR, int N, int M, int uc, float *__restrict__ U)
 {
-    const long total = (long)M * M;
+    const long total = (long)M * uc;
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-        const long r = t / M, c = t % M;
+        const long r = t / uc, c = t % uc;
         float v;
         if (r < N && c < N) v = UR[r * N + c];
         else v = (r == c) ? 1.f : 0.f;
@@ -318,14 +318,16 @@ void qr_extract_r_launch(const BdWs &w, int N, float *R, cudaStream_t s)
     paco_count_launch(), qr_extract_r<<<std::min(8192, ceil_div((long)N * N, 256)), 256, 0, s>>>(w.W, w.ldw, N, R);
 }
 
-// U (M x M) <- Q blockdiag(UR, I), Q = H_0 ... H_{N-1} from qr_factor
-int qr_form_u(const BdWs &w, int M, int N, const float *tau, const float *UR, float *U, cudaStream_t s)
+// U (M x uc, ld uc; uc = M, or N for the thin U) <- the first uc columns of
+// Q blockdiag(UR, I), Q = H_0 ... H_{N-1} from qr_factor
+int qr_form_u(const BdWs &w, int M, int N, const float *tau, const float *UR, float *U, cudaStream_t s, int uc)
 {
-    paco_count_launch(), qr_blockdiag<<<std::min(8192, ceil_div((long)M * M, 256)), 256, 0, s>>>(UR, N, M, U);
+    if (uc <= 0) uc = M;
+    paco_count_launch(), qr_blockdiag<<<std::min(8192, ceil_div((long)M * uc, 256)), 256, 0, s>>>(UR, N, M, uc, U);
     for (int p0 = ((N - 1) / bd::NBF) * bd::NBF; p0 >= 0; p0 -= bd::NBF) {
         const int nbp = std::min(N, p0 + bd::NBF) - p0, Lp = M - p0;
         bd_column_vectors(w.W, w.ldw, p0, nbp, Lp, w.Vp, s);
-        if (apply_block_reflector_ex(w, U, M, p0, Lp, 0, M, nbp, tau + p0, false, s) != cudaSuccess)
+        if (apply_block_reflector_ex(w, U, uc, p0, Lp, 0, uc, nbp, tau + p0, false, s) != cudaSuccess)
             return PACO_ERR_CUDA;
     }
     return cudaGetLastError() == cudaSuccess ? PACO_OK : PACO_ERR_CUDA;

@@ -89,6 +89,8 @@ def lib():
         L.paco_svd_multi.argtypes = [i, i, i, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
                                      ctypes.POINTER(vp), vp, vp, ctypes.c_size_t, vp]
         L.paco_svd_multi.restype = i
+        L.paco_svd_thin.argtypes = [i, i, f32p, f32p, f32p, f32p, vp, ctypes.c_size_t, vp]
+        L.paco_svd_thin.restype = i
         L.paco_tune_qr.argtypes = [i, i, i]
         L.paco_tune_qr.restype = i
         L.paco_multi_group.argtypes = [i]
@@ -228,6 +230,28 @@ class Workspace:
                             _ptr(self.ws), self.nbytes, _stream(stream))
         _check(rc, "paco_svd")
         return self.sigma, self.U, self.Vt
+
+
+def svd_thin(A, check=True):
+    """SVD with the thin U: returns (sigma, U M x N, Vt N x N) for a float32
+    CUDA matrix A (M >= N), A = U diag(sigma) Vt."""
+    torch = _torch()
+    A = _check_matrix(A)
+    M, N = A.shape
+    nbytes = int(lib().paco_svd_workspace_size(M, N))
+    if nbytes == 0:
+        raise PacoError(PACO_ERR_UNSUPPORTED if N >= 1 and M >= N else PACO_ERR_INVALID_ARG, "paco_svd_thin")
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=A.device)
+    Aw = A.clone()
+    U = torch.empty(M, N, device=A.device)
+    Vt = torch.empty(N, N, device=A.device)
+    s = torch.empty(N, device=A.device)
+    _check(lib().paco_svd_thin(M, N, _ptr(Aw), _ptr(U), _ptr(Vt), _ptr(s), _ptr(ws), nbytes, _stream()),
+           "paco_svd_thin")
+    if check:
+        rc, info = sync_status(ws)
+        _check(rc, f"paco_svd_thin (device, info={info})")
+    return s, U, Vt
 
 
 def svd(A, check=True):
