@@ -796,7 +796,6 @@ int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s0, cudaStream_t *side, 
     BdArgs a[PK_KMAX];
     PkCtl *ctl[PK_KMAX];
     unsigned pk_cnt[PK_KMAX]; // arrivals on each matrix's barrier counter so far
-    unsigned pk_ep[PK_KMAX];  // epochs of each matrix's tagged hand-overs so far
     for (int j = 0; j < k; j++) {
         const BdJob &J = jobs[j];
         bd_carve(J.workspace, M, N, &w[j]);
@@ -808,12 +807,10 @@ int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s0, cudaStream_t *side, 
         x.sc = w[j].sc;
         x.d = J.d; x.e = J.e; x.tauq = J.tauq; x.taup = J.taup;
         x.bcA = w[j].bcA; x.bcB = w[j].bcB;
-        x.cpart_t = w[j].cpart_t; x.bcB_t = w[j].bcB_t; x.rowbuf_t = w[j].rowbuf_t;
         x.trace = (trace_env >= 0 && j == 0) ? w[j].trace : nullptr;
         x.trace_p0 = trace_env;
         ctl[j] = w[j].ctl;
         pk_cnt[j] = 0;
-        pk_ep[j] = 0;
     }
 
     const int gmax = std::max(1, std::min(RB_CAP, num_sms / k));
@@ -830,10 +827,6 @@ int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s0, cudaStream_t *side, 
     for (int j = 0; j < k; j++) {
         cudaMemsetAsync(w[j].st->counters, 0, sizeof(w[j].st->counters), s);
         cudaMemsetAsync(w[j].ctl, 0, sizeof(PkCtl), s);
-        // tagged hand-overs start at epoch 1 each run: no stale word can match
-        cudaMemsetAsync(w[j].cpart_t, 0, sizeof(unsigned long long) * (size_t)PR * PCAP, s);
-        cudaMemsetAsync(w[j].bcB_t, 0, sizeof(unsigned long long) * PR, s);
-        cudaMemsetAsync(w[j].rowbuf_t, 0, sizeof(unsigned long long) * (size_t)w[j].ldw, s);
         cudaMemsetAsync(w[j].Yt, 0, sizeof(float) * NB * w[j].ldw, s);
         cudaMemsetAsync(w[j].X, 0, sizeof(float) * (size_t)M * NB, s);
         paco_count_launch(), bd_copy_in<<<std::min(4096, ceil_div((long)M * w[j].ldw, 256)), 256, 0, s>>>(
@@ -886,7 +879,7 @@ int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s0, cudaStream_t *side, 
         if (use_pk) {
             cudaEvent_t e0 = nullptr, e1 = nullptr;
             if (g_prof.on) prof_record(e0 = prof_event(), s);
-            pk = bd_panel_pk_launch_multi(k, a, ctl, p0, p1, Gp, pk_cnt, pk_ep, s);
+            pk = bd_panel_pk_launch_multi(k, a, ctl, p0, p1, Gp, pk_cnt, s);
             if (g_prof.on) {
                 prof_record(e1 = prof_event(), s);
                 g_prof.cur.ev.push_back(e0);

@@ -45,10 +45,6 @@ struct BdArgs {
     unsigned long long *trace; // phase timestamps of one traced panel (or null)
     int trace_p0;
     float *bcA, *bcB; // broadcast slots of the persistent kernel's reflectors
-    // tagged copies (value | epoch << 32) of what the persistent kernel's column
-    // pass hands to every CTA's next row pass: partial records, pivot-row slots,
-    // the updated row
-    unsigned long long *cpart_t, *bcB_t, *rowbuf_t;
 };
 
 // Arguments of one launch of the persistent panel kernel: the same panel of
@@ -58,9 +54,7 @@ struct PkMulti {
     BdArgs a[PK_KMAX];
     PkCtl *ctl[PK_KMAX];
     unsigned cnt_base[PK_KMAX];  // barrier counter of each matrix before the launch
-    unsigned ep_base[PK_KMAX];   // epoch of the tagged hand-overs before the launch
     int G;
-    int tagged;                  // hand the column pass's results over by tagged values (no second barrier)
 };
 
 struct BdWs {
@@ -78,7 +72,6 @@ struct BdWs {
     PkCtl *ctl;
     unsigned long long *trace; // NB+1 steps x 16 slots x 2 CTAs
     float *bcA, *bcB;          // PR each: pivot and panel entries of a reflector
-    unsigned long long *cpart_t, *bcB_t, *rowbuf_t;  // tagged hand-overs (PR x PCAP, PR, ldw)
     float *Vp;     // max(M,N) x NBF explicit reflector block (formation of U, V)
     float *T;      // NBF x NBF
     float *gram;   // NBF x NBF  Vp^T Vp
@@ -119,9 +112,6 @@ static inline size_t bd_carve(void *base, int M, int N, BdWs *w)
     w->trace = (unsigned long long *)take(sizeof(unsigned long long) * (NB + 1) * 16 * 2);
     w->bcA = (float *)take(sizeof(float) * PR);
     w->bcB = (float *)take(sizeof(float) * PR);
-    w->cpart_t = (unsigned long long *)take(sizeof(unsigned long long) * (size_t)PR * PCAP);
-    w->bcB_t = (unsigned long long *)take(sizeof(unsigned long long) * PR);
-    w->rowbuf_t = (unsigned long long *)take(sizeof(unsigned long long) * (size_t)ldw);
     w->Vp = (float *)take(sizeof(float) * (size_t)mx * NBF);
     w->T = (float *)take(sizeof(float) * NBF * NBF);
     w->gram = (float *)take(sizeof(float) * NBF * NBF);
@@ -175,10 +165,9 @@ static __device__ __forceinline__ void reduce_records(const float *rec, int ncta
     __syncthreads();
 }
 
-bool bd_panel_pk_launch(const BdArgs &a, PkCtl *ctl, int p0, int p1, int G, unsigned *cnt, unsigned *ep,
-                        cudaStream_t s);
+bool bd_panel_pk_launch(const BdArgs &a, PkCtl *ctl, int p0, int p1, int G, unsigned *cnt, cudaStream_t s);
 bool bd_panel_pk_launch_multi(int k, const BdArgs *a, PkCtl *const *ctl, int p0, int p1, int G, unsigned *cnt,
-                              unsigned *ep, cudaStream_t s);
+                              cudaStream_t s);
 // Test hook: a cooperative launch of G CTAs whose grid barrier never
 // completes; its bounded waits give up after max_cycles.
 bool bd_pk_debug_timeout(PkCtl *ctl, DevStatus *st, int G, long long max_cycles, cudaStream_t s);

@@ -24,7 +24,6 @@
 // per panel instead of once per step; otherwise they are re-staged with TMA
 // bulk copies at every step (double-buffered).  Data other CTAs wrote earlier
 // in the same launch is read with ld.global.cg (L2), never from L1.
-#include <cstdlib>
 #include <cstring>
 
 #include "bidiag.cuh"
@@ -114,127 +113,6 @@ __device__ __forceinline__ void reduce_records_fast(const float *rec, int G, int
     __syncthreads();
 }
 
-// Tagged values: a float and the epoch of the hand-over that wrote it in one
-// 64-bit word, stored and loaded single-copy atomic, so a reader that sees
-// the epoch it expects sees the value written with it.
-__device__ __forceinline__ void st_tag(unsigned long long *p, float v, unsigned ep)
-{
-    const unsigned long long u = ((unsigned long long)ep << 32) | __float_as_uint(v);
-    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(u) : "memory");
-}
-
-__device__ __forceinline__ unsigned long long ld_tag(const unsigned long long *p)
-{
-    unsigned long long u;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(u) : "l"(p) : "memory");
-    return u;
-}
-
-// The hand-over of a column pass to the next step's row pass without a grid
-// barrier: every thread polls its share of the tagged values until each
-// carries epoch `ep` -- the partial records rec[t * PCAP + cta] (t < nval,
-// cta < G) summed as reduce_records_fast sums them, the pivot-row slots
-// bc[0..nbc) (into bc_dst), and the updated row's entries row[j] for
-// j in [jlo, jhi) of this thread's CPT float4 chunks from column c0 (rb; other
-// entries read as 0).  Bounded: gives up after ~2 s of SM clock or when
-// another CTA raised the abort flag.  Called by every thread of the CTA.
-template <int CPT>
-__device__ bool reduce_tagged(const unsigned long long *rec, int G, int nval, float *out,
-                              const unsigned long long *bc, float *bc_dst, int nbc, const unsigned long long *row,
-                              int c0, int jlo, int jhi, float4 (&rb)[CPT], unsigned ep, PkCtl *ctl, DevStatus *st,
-                              int where, int *s_ok)
-{
-    constexpr int NW = RP_THREADS / 32, VPW = 5, LPV = 5;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    float x[VPW][LPV];
-    float bcv = 0.f;
-    float r[CPT][4];
-    unsigned need = 0;  // bit v*LPV+k: record value still to come; bit 25: bc; bits 26+: row entries
-    unsigned rneed[CPT];
-#pragma unroll
-    for (int v = 0; v < VPW; v++)
-#pragma unroll
-        for (int k = 0; k < LPV; k++) {
-            x[v][k] = 0.f;
-            if (warp + NW * v < nval && lane + 32 * k < G) need |= 1u << (v * LPV + k);
-        }
-    if (tid < nbc) need |= 1u << 25;
-#pragma unroll
-    for (int q = 0; q < CPT; q++) {
-        rneed[q] = 0;
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const int j = c0 + 4 * (tid + q * RP_THREADS) + e;
-            r[q][e] = 0.f;
-            if (j >= jlo && j < jhi) rneed[q] |= 1u << e;
-        }
-    }
-    bool ok = true;
-    const long long t0 = clock64();
-    for (int it = 0;; it++) {
-        unsigned rn = 0;
-#pragma unroll
-        for (int v = 0; v < VPW; v++)
-#pragma unroll
-            for (int k = 0; k < LPV; k++)
-                if (need & (1u << (v * LPV + k))) {
-                    const unsigned long long u = ld_tag(&rec[(long)(warp + NW * v) * PCAP + lane + 32 * k]);
-                    if ((unsigned)(u >> 32) == ep) {
-                        x[v][k] = __uint_as_float((unsigned)u);
-                        need &= ~(1u << (v * LPV + k));
-                    }
-                }
-        if (need & (1u << 25)) {
-            const unsigned long long u = ld_tag(&bc[tid]);
-            if ((unsigned)(u >> 32) == ep) {
-                bcv = __uint_as_float((unsigned)u);
-                need &= ~(1u << 25);
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < CPT; q++) {
-#pragma unroll
-            for (int e = 0; e < 4; e++)
-                if (rneed[q] & (1u << e)) {
-                    const unsigned long long u = ld_tag(&row[c0 + 4 * (tid + q * RP_THREADS) + e]);
-                    if ((unsigned)(u >> 32) == ep) {
-                        r[q][e] = __uint_as_float((unsigned)u);
-                        rneed[q] &= ~(1u << e);
-                    }
-                }
-            rn |= rneed[q];
-        }
-        if (!need && !rn) break;
-        if ((it & 15) == 15) {
-            if (ld_acquire(&ctl->abort)) { ok = false; break; }
-            if (clock64() - t0 > 4000000000LL) {
-                atomicAdd(&st->wait_timeouts, 1);
-                dev_fail(st, PACO_ERR_TIMEOUT, where);
-                atomicExch(&ctl->abort, 1u);
-                ok = false;
-                break;
-            }
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < CPT; q++) rb[q] = make_float4(r[q][0], r[q][1], r[q][2], r[q][3]);
-#pragma unroll
-    for (int v = 0; v < VPW; v++) {
-        const int t = warp + NW * v;
-        float sum = 0.f;
-#pragma unroll
-        for (int k = 0; k < LPV; k++) sum += x[v][k];
-        sum = warp_sum(sum);
-        if (lane == 0 && t < nval) out[t] = sum;
-    }
-    if (tid < nbc) bc_dst[tid] = bcv;
-    if (__syncthreads_or(!ok)) {
-        if (tid == 0) *s_ok = 0;
-        return false;
-    }
-    return true;
-}
-
 }  // namespace
 
 // Rows a row-pass batch takes (one warp per row): resident rows go 16 at a
@@ -253,8 +131,6 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
     const BdArgs &a = pm.a[mi];
     PkCtl *const ctl = pm.ctl[mi];
     const unsigned cnt_base = pm.cnt_base[mi];
-    const unsigned ep_base = pm.ep_base[mi];
-    const bool tagged = pm.tagged != 0;
     extern __shared__ __align__(128) float tiles[];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ float red[RP_THREADS / 32][PK_RMAX];
@@ -343,24 +219,15 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
         if (doX) {
             // all loads of this phase in flight together
             const int nbc = 2 + 2 * iip;
+            const float bcv = (tid < nbc) ? __ldcg(&a.bcB[tid]) : 0.f;
             float4 rb[CPT];
-            if (tagged) {
-                // the column pass of step i-1 handed these over with epoch ep_base + ii
-                if (!reduce_tagged<CPT>(a.cpart_t, G, nbc, s_red, a.bcB_t, s_bc, nbc, a.rowbuf_t, p0, i + 1, N, rb,
-                                        ep_base + (unsigned)ii, ctl, st, 400 + i, &s_ok)) {
-                    failed = true;
-                    break;
-                }
-            } else {
-                const float bcv = (tid < nbc) ? __ldcg(&a.bcB[tid]) : 0.f;
 #pragma unroll
-                for (int k = 0; k < CPT; k++) {
-                    int c = p0 + 4 * (tid + k * RP_THREADS);
-                    rb[k] = (c < ldw) ? __ldcg(reinterpret_cast<const float4 *>(a.rowbuf + c))
-                                      : make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-                reduce_records_fast(a.cpart, G, nbc, s_red, s_bc, bcv, nbc);
+            for (int k = 0; k < CPT; k++) {
+                int c = p0 + 4 * (tid + k * RP_THREADS);
+                rb[k] = (c < ldw) ? __ldcg(reinterpret_cast<const float4 *>(a.rowbuf + c))
+                                  : make_float4(0.f, 0.f, 0.f, 0.f);
             }
+            reduce_records_fast(a.cpart, G, nbc, s_red, s_bc, bcv, nbc);
             // every thread forms the same reflector from the same sums
             float beta, v0;
             make_reflector(s_bc[0], s_red[0], N - (i - 1) - 1, &beta, &r_taup, &v0);
@@ -647,7 +514,6 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
 
         // --------------------------------------------------- column pass
         const float tq = c_tau, invc_i = c_inv;
-        const unsigned epw = ep_base + (unsigned)ii + 1u;  // epoch of this step's hand-over
         for (int ch = b; ch < nchunk; ch += G) {
             const int j = i + 1 + ch * 32 + lane;
             const bool valid = j < N;
@@ -686,8 +552,7 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
                 aj = wij - Ynew - sb;
                 if (warp == 0) {
                     a.Yt[(long)ii * ldw + j] = Ynew;
-                    if (tagged) st_tag(&a.rowbuf_t[j], aj, epw);
-                    else a.rowbuf[j] = aj;
+                    a.rowbuf[j] = aj;
                 }
             }
             if (j == i + 1) {
@@ -696,23 +561,13 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
                 for (int e = 0; e < 2; e++) {
                     int q = 2 * warp + e;
                     if (q < ii) {
-                        if (tagged) {
-                            st_tag(&a.bcB_t[1 + q], Yq[e], epw);
-                            st_tag(&a.bcB_t[2 + ii + q], Wq[e], epw);
-                        } else {
-                            a.bcB[1 + q] = Yq[e];
-                            a.bcB[2 + ii + q] = Wq[e];
-                        }
+                        a.bcB[1 + q] = Yq[e];
+                        a.bcB[2 + ii + q] = Wq[e];
                     }
                 }
                 if (warp == 0) {
-                    if (tagged) {
-                        st_tag(&a.bcB_t[0], aj, epw);
-                        st_tag(&a.bcB_t[1 + ii], Ynew, epw);
-                    } else {
-                        a.bcB[0] = aj;
-                        a.bcB[1 + ii] = Ynew;
-                    }
+                    a.bcB[0] = aj;
+                    a.bcB[1 + ii] = Ynew;
                 }
             }
             float m = (valid && j >= i + 2) ? aj : 0.f;
@@ -731,12 +586,8 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
             __syncthreads();
         }
         stamp(i, 5);
-        if (tagged) {
-            for (int t = tid; t < PR; t += RP_THREADS) st_tag(&a.cpart_t[(long)t * PCAP + b], s_cpart[t], epw);
-        } else {
-            for (int t = tid; t < PR; t += RP_THREADS) a.cpart[(long)t * PCAP + b] = s_cpart[t];
-            if (!pk_barrier(ctl, cnt_base + (++nbar) * G, st, 400 + i, &s_ok)) { failed = true; break; }
-        }
+        for (int t = tid; t < PR; t += RP_THREADS) a.cpart[(long)t * PCAP + b] = s_cpart[t];
+        if (!pk_barrier(ctl, cnt_base + (++nbar) * G, st, 400 + i, &s_ok)) { failed = true; break; }
         stamp(i, 6);
     }
     // a step that ended early leaves prefetched rows in flight: they land
@@ -747,23 +598,11 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
 }
 
 // Grid barriers one launch for panel [p0, p1) passes (host and kernel agree):
-// barrier A at every step, barrier B at every step but a last column (none
-// when the column pass hands its results over by tagged values).
-static unsigned pk_barriers(int N, int p0, int p1, bool tagged)
+// barrier A at every step, barrier B at every step but a last column.
+static unsigned pk_barriers(int N, int p0, int p1)
 {
     const int nbp = p1 - p0;
-    return tagged ? (unsigned)nbp : (unsigned)(2 * nbp - (p1 == N ? 1 : 0));
-}
-
-// PACO_PK_TAGGED=0 keeps the second grid barrier per column step
-static bool pk_tagged()
-{
-    static int on = -1;
-    if (on < 0) {
-        const char *v = getenv("PACO_PK_TAGGED");
-        on = !(v && v[0] == '0');
-    }
-    return on != 0;
+    return (unsigned)(2 * nbp - (p1 == N ? 1 : 0));
 }
 
 // Host side: launches the persistent kernel for panel [p0, p1) of k matrices
@@ -772,7 +611,7 @@ static bool pk_tagged()
 // this launch makes.  Returns false when a cooperative launch of k * G CTAs
 // is not possible.
 bool bd_panel_pk_launch_multi(int k, const BdArgs *a, PkCtl *const *ctl, int p0, int p1, int G, unsigned *cnt,
-                              unsigned *ep, cudaStream_t s)
+                              cudaStream_t s)
 {
     if (k < 1 || k > PK_KMAX) return false;
     const int L = (int)(a[0].ldw - p0);
@@ -792,12 +631,10 @@ bool bd_panel_pk_launch_multi(int k, const BdArgs *a, PkCtl *const *ctl, int p0,
     PkMulti pm;
     memset(&pm, 0, sizeof(pm));
     pm.G = G;
-    pm.tagged = pk_tagged() ? 1 : 0;
     for (int j = 0; j < k; j++) {
         pm.a[j] = a[j];
         pm.ctl[j] = ctl[j];
         pm.cnt_base[j] = cnt[j];
-        pm.ep_base[j] = ep[j];
     }
     void *args[] = {&pm, &p0, &p1, &resident, &R};
     paco_count_launch();
@@ -805,17 +642,13 @@ bool bd_panel_pk_launch_multi(int k, const BdArgs *a, PkCtl *const *ctl, int p0,
         cudaGetLastError();
         return false;
     }
-    for (int j = 0; j < k; j++) {
-        cnt[j] += pk_barriers(a[j].N, p0, p1, pm.tagged != 0) * (unsigned)G;
-        ep[j] += (unsigned)(p1 - p0) + 1u;
-    }
+    for (int j = 0; j < k; j++) cnt[j] += pk_barriers(a[j].N, p0, p1) * (unsigned)G;
     return true;
 }
 
-bool bd_panel_pk_launch(const BdArgs &a, PkCtl *ctl, int p0, int p1, int G, unsigned *cnt, unsigned *ep,
-                        cudaStream_t s)
+bool bd_panel_pk_launch(const BdArgs &a, PkCtl *ctl, int p0, int p1, int G, unsigned *cnt, cudaStream_t s)
 {
-    return bd_panel_pk_launch_multi(1, &a, &ctl, p0, p1, G, cnt, ep, s);
+    return bd_panel_pk_launch_multi(1, &a, &ctl, p0, p1, G, cnt, s);
 }
 
 // Test hook: every CTA of a cooperative grid arrives at a grid barrier whose
