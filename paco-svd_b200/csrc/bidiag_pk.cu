@@ -126,6 +126,8 @@ template <int CPT, int RB>
 __global__ void __launch_bounds__(RP_THREADS, 1)
     bd_panel_pk(const __grid_constant__ PkMulti pm, int p0, int p1, int resident, int R)
 {
+    // rows of a batch kept in registers between the two uses (<= 64 floats)
+    constexpr bool REG = RB * CPT <= 16 && RB <= 16;
     // CTAs [j*G, (j+1)*G) run the panel of matrix j with their own barrier
     const int mi = blockIdx.x / pm.G;
     const BdArgs &a = pm.a[mi];
@@ -139,7 +141,13 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
     __shared__ float s_t1[NB], s_t2[NB], s_ai[NB], s_xi[NB];         // column reflector of step i
     __shared__ float s_part[PK_RMAX][PR];
     __shared__ float s_red[PR], s_bc[PR];
-    __shared__ float cy[RP_THREADS / 32][32], cA[RP_THREADS / 32][32], cB[RP_THREADS / 32][32];
+    // column pass: three [warp][lane] tiles; row pass (REG): the batch rows'
+    // panel columns s_pan[parity][row][lane] and dot partials
+    // red2[parity][warp][row] (the two passes never overlap)
+    __shared__ float cpool[3][RP_THREADS / 32][32];
+    float(*cy)[32] = cpool[0];
+    float(*cA)[32] = cpool[1];
+    float(*cB)[32] = cpool[2];
     __shared__ float s_cpart[PR];
     __shared__ int s_ok;
 
@@ -292,6 +300,104 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
         }
         pf_n = 0;
         float w_ss = 0.f, w_g1 = 0.f, w_g2 = 0.f;
+        if constexpr (REG) {
+            // Rows held in registers between the dot products and the A^T x
+            // share: one CTA barrier per batch.  Every warp forms every row's
+            // scalars (the same inputs and order in every warp); warp rr makes
+            // row rr's writes.  The stage is refilled right after the barrier.
+            for (int bb = 0; bb < nbatch; bb++) {
+                const int k0 = kfirst + bb * R, nr = min(R, nown - k0);
+                const int par = bb & 1, stage = bb & 1;
+                float *span = &cpool[par][0][0];  // [RB][32]
+                float *red2 = &cpool[2][0][0] + par * (RP_THREADS / 32) * 16;  // [warp][16]
+                const float *T;
+                if (resident) {
+                    T = tiles + (long)k0 * L;
+                } else {
+                    const unsigned long long tw = tracing ? gtimer() : 0ull;
+                    if (!mbar_wait_bounded(&bars[stage], stage ? phase1 : phase0, st, 200 + i)) failed = true;
+                    if (tracing) waited += gtimer() - tw;
+                    if (stage) phase1 ^= 1; else phase0 ^= 1;
+                    T = tiles + (long)stage * R * L;
+                }
+                float4 v[RB][CPT];
+#pragma unroll
+                for (int rr = 0; rr < RB; rr++) {
+                    float pd = 0.f;
+#pragma unroll
+                    for (int k = 0; k < CPT; k++) {
+                        const int c4 = tid + k * RP_THREADS;
+                        v[rr][k] = (rr < nr && 4 * c4 < L) ? *reinterpret_cast<const float4 *>(T + (long)rr * L + 4 * c4)
+                                                           : make_float4(0.f, 0.f, 0.f, 0.f);
+                        pd += v[rr][k].x * u4[k].x + v[rr][k].y * u4[k].y + v[rr][k].z * u4[k].z + v[rr][k].w * u4[k].w;
+                    }
+                    if (doX && rr < nr) {
+                        pd = warp_sum(pd);
+                        if (lane == 0) red2[warp * 16 + rr] = pd;
+                    }
+                }
+                if (warp < nr) span[warp * 32 + lane] = T[(long)warp * L + lane];
+                __syncthreads();
+                if (!resident && tid == 0 && bb + 2 < nbatch) {
+                    proxy_async_fence();
+                    issue_rows(kfirst, bb + 2, stage);
+                }
+#pragma unroll
+                for (int rr = 0; rr < RB; rr++) {
+                    if (rr >= nr) continue;
+                    const int r = own_row(k0 + rr);
+                    const float pan = span[rr * 32 + lane];
+                    float aq = (lane < ii) ? pan : 0.f;
+                    if (lane == ii - 1) aq *= invc;
+                    const float xq = (doX && lane < iip)
+                                         ? (xsm ? xsm[(k0 + rr) * NB + lane] : a.X[(long)r * NB + lane])
+                                         : 0.f;
+                    float Xn = 0.f;
+                    if (doX) {
+                        const float dot = warp_sum(lane < RP_THREADS / 32 ? red2[lane * 16 + rr] : 0.f);
+                        const float sx = ((lane <= iip) ? aq * s_t3[lane] : 0.f) + ((lane < iip) ? xq * s_t4[lane] : 0.f);
+                        Xn = taup_prev * (dot - warp_sum(sx));
+                        if (warp == rr && lane == 0) {
+                            a.X[(long)r * NB + iip] = Xn;
+                            if (xsm) xsm[(k0 + rr) * NB + iip] = Xn;
+                        }
+                    }
+                    if (warp == rr && lane == ii - 1) {
+                        a.W[(long)r * ldw + (i - 1)] = aq;
+                        if (resident) tiles[(long)(k0 + rr) * L + lane] = aq;
+                    }
+                    if (doCol) {
+                        const float xrq = (lane < ii - 1) ? xq : ((lane == ii - 1) ? Xn : 0.f);
+                        const float sc = (lane < ii) ? (aq * s_ycol[lane] + xrq * s_wcol[lane]) : 0.f;
+                        const float xr = __shfl_sync(0xffffffffu, pan, ii & 31) - warp_sum(sc);
+                        if (warp == rr) {
+                            if (lane == 0) {
+                                a.W[(long)r * ldw + i] = xr;
+                                if (resident) tiles[(long)(k0 + rr) * L + ii] = xr;
+                            }
+                            if (r == i) {
+                                // pivot and row-i panel entries for every CTA's column reflector
+                                if (lane == 0) a.bcA[0] = xr;
+                                if (lane < ii) {
+                                    a.bcA[1 + lane] = aq;
+                                    a.bcA[1 + ii + lane] = xrq;
+                                }
+                            } else if (r > i) {
+                                if (lane == 0) w_ss += xr * xr;
+                                if (lane < ii) { w_g1 += aq * xr; w_g2 += xrq * xr; }
+                            }
+                        }
+                        if (r > i) {
+#pragma unroll
+                            for (int k = 0; k < CPT; k++) {
+                                acc4[k].x += v[rr][k].x * xr; acc4[k].y += v[rr][k].y * xr;
+                                acc4[k].z += v[rr][k].z * xr; acc4[k].w += v[rr][k].w * xr;
+                            }
+                        }
+                    }
+                }
+            }
+        } else
         for (int bb = 0; bb < nbatch; bb++) {
             const int k0 = kfirst + bb * R, nr = min(R, nown - k0);
             const float *T;
@@ -620,11 +726,13 @@ bool bd_panel_pk_launch_multi(int k, const BdArgs *a, PkCtl *const *ctl, int p0,
     int resident = ((long)own * L * 4 <= budget) ? 1 : 0;
     int R = std::max(1, std::min(RMAX, (int)(budget / (2L * L * 4))));
     size_t smem = resident ? (size_t)own * L * 4 : (size_t)2 * R * L * 4;
-    if (resident) R = PK_RMAX;
-    if (own <= PK_XOWN) smem += (size_t)own * NB * 4;  // X entries of the owned rows
     const int chunks = ceil_div(L, 4 * RP_THREADS);
+    // resident rows go 16 per batch (8 with two float4 chunks a thread, so a
+    // batch stays in registers)
+    if (resident) R = (chunks == 2) ? RMAX : PK_RMAX;
+    if (own <= PK_XOWN) smem += (size_t)own * NB * 4;  // X entries of the owned rows
     void *fn;
-    if (resident) fn = chunks <= 1 ? (void *)bd_panel_pk<1, PK_RMAX> : chunks == 2 ? (void *)bd_panel_pk<2, PK_RMAX>
+    if (resident) fn = chunks <= 1 ? (void *)bd_panel_pk<1, PK_RMAX> : chunks == 2 ? (void *)bd_panel_pk<2, RMAX>
                                                                                  : (void *)bd_panel_pk<4, PK_RMAX>;
     else fn = chunks <= 1 ? (void *)bd_panel_pk<1, RMAX> : chunks == 2 ? (void *)bd_panel_pk<2, RMAX>
                                                                        : (void *)bd_panel_pk<4, RMAX>;
@@ -675,7 +783,6 @@ void bd_pk_init_attrs()
     if (done[dev]) return;
     int maxs = 200 * 1024 + PK_XOWN * NB * 4 + 1024;
     cudaFuncSetAttribute(bd_panel_pk<1, PK_RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
-    cudaFuncSetAttribute(bd_panel_pk<2, PK_RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
     cudaFuncSetAttribute(bd_panel_pk<4, PK_RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
     cudaFuncSetAttribute(bd_panel_pk<1, RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);
     cudaFuncSetAttribute(bd_panel_pk<2, RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs);

@@ -459,9 +459,11 @@ static int svd_direct_thin(int M, int N, float *A, float *U, float *Vt, float *s
 }
 
 // Test hook (not part of the public header): the QR-first path's R factor
-// (N x N, ld N, zeros below the diagonal) of A (M x N, M > N, N >= 1024);
-// ws holds paco_svd_workspace_size(M, N) bytes.  Synchronous.
-extern "C" int paco_debug_qr_r(int M, int N, const float *A, float *R, void *ws, size_t ws_bytes, void *stream)
+// (N x N, ld N, zeros below the diagonal) of A (M x N, M > N, N >= 1024) and,
+// when Qout is not null, Q (M x M) explicitly; ws holds
+// paco_svd_workspace_size(M, N) bytes.  Synchronous.
+extern "C" int paco_debug_qr_r(int M, int N, const float *A, float *R, float *Qout, void *ws, size_t ws_bytes,
+                               void *stream)
 {
     if (!shape_ok(M, N) || !qr_possible(M, N) || !qr_fits(M, N) || !A || !R || !ws ||
         ws_bytes < paco_svd_workspace_size(M, N))
@@ -479,6 +481,8 @@ extern "C" int paco_debug_qr_r(int M, int N, const float *A, float *R, void *ws,
     int rc = qr_factor(wq, M, N, (float *)(b + Q.tau), s);
     if (rc) return rc;
     qr_extract_r_launch(wq, N, R, s);
+    if (Qout) rc = qr_form_u(wq, M, N, (float *)(b + Q.tau), nullptr, Qout, s);  // Q (M x M) explicitly
+    if (rc) return rc;
     return paco_sync_status(ws, stream, nullptr);
 }
 

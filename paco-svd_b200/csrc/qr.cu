@@ -204,7 +204,7 @@ __global__ void qr_blockdiag(const float *__restrict__ UR, int N, int M, int uc,
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
         const long r = t / uc, c = t % uc;
         float v;
-        if (r < N && c < N) v = UR[r * N + c];
+        if (UR && r < N && c < N) v = UR[r * N + c];
         else v = (r == c) ? 1.f : 0.f;
         U[t] = v;
     }

@@ -18,5 +18,6 @@ int qr_factor(const BdWs &w, int M, int N, float *tau, cudaStream_t s);
 // R (N x N, ld N) <- the upper triangle of W[0:N, 0:N].
 void qr_extract_r_launch(const BdWs &w, int N, float *R, cudaStream_t s);
 // U (M x uc, ld uc) <- the first uc columns of Q blockdiag(UR, I) with Q from
-// qr_factor and UR N x N (ld N); uc = M (0 means M), or N for the thin U.
+// qr_factor and UR N x N (ld N; null: the identity, so U = Q); uc = M (0
+// means M), or N for the thin U.
 int qr_form_u(const BdWs &w, int M, int N, const float *tau, const float *UR, float *U, cudaStream_t s, int uc = 0);
