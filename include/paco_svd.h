@@ -76,6 +76,20 @@ int paco_tune_set(int M, int N, const int cfg[4]);
  * argument. */
 int paco_tune_qr(int M, int N, int mode);
 
+/* One field of the tuning entry for (M, N): which = 0 persistent panel
+ * kernel (0/1), 1 rows per CTA of a panel (4..256), 2 tcgen05 products (0/1),
+ * 3 last columns kept off the cluster kernel (0/1), 4 reflectors per
+ * compact-WY block when U and V are formed (64 or 128; 0 = 128), 5 columns per
+ * QR block (32 or 64; 0 = 64), 6 matrices per lockstep group of
+ * paco_svd_multi (1..8; 0 = 4), 7 the QR-first mode of paco_tune_qr.  value
+ * -1 queries.  Returns the value stored or queried, -1 for an invalid
+ * argument.  paco_autotune times fields 0-5 (and 7) for one shape;
+ * paco_autotune_multi times field 6 (2, 4, 8) on `count` synthetic matrices
+ * of the shape (out as paco_autotune's, out[0] = the group size chosen).
+ * paco_multi_group, when set, overrides field 6 for every shape. */
+int paco_tune_param(int M, int N, int which, int value);
+int paco_autotune_multi(int count, int M, int N, void *stream, double out[4]);
+
 /* Buffer sizes in bytes of main.cpp:33-43, in this order:
  * [0] U M*M, [1] A M*N, [2] Vt N*N, [3] d N, [4] e N-1, [5] tauq N,
  * [6] taup N-1, [7] qt 2*N*N, [8] wt 2*N*N, [9] tiling, [10] idx 16*N*u32,
@@ -192,8 +206,9 @@ int paco_svd_batched(int count, const int *M, const int *N, const float *const *
 size_t paco_svd_multi_workspace_size(int count, int M, int N);
 int paco_svd_multi(int count, int M, int N, const float *const *A, float *const *U, float *const *Vt,
                    float *const *sigma, int *status, void *workspace, size_t ws_bytes, void *stream);
-/* Matrices per lockstep group of paco_svd_multi (1..8; 0 = automatic, 4);
- * returns the previous setting.  Set it before computing workspace sizes. */
+/* Matrices per lockstep group of paco_svd_multi for every shape (1..8; 0 =
+ * the shape's tuning entry, 4 by default); returns the previous setting.
+ * Set it before computing workspace sizes. */
 int paco_multi_group(int k);
 
 /* Library version string. */

@@ -915,7 +915,9 @@ int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s0, cudaStream_t *side, 
         }
     }
 
-    // the formation of U and V: each matrix on its own side stream (k > 1)
+    // the formation of U and V (nbf reflectors per block update): each matrix
+    // on its own side stream (k > 1)
+    const int nbf = tune.wy == 64 ? 64 : NBF;
     if (k > 1) fork();
     for (int j = 0; j < k; j++) {
         const BdWs &x = w[j];
@@ -925,8 +927,8 @@ int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s0, cudaStream_t *side, 
         // NBF reflectors per block update)
         const int uc = J.thin ? N : M;  // columns of U formed
         paco_count_launch(), bd_set_eye<<<std::min(8192, ceil_div((long)M * uc, 256)), 256, 0, s>>>(J.u, M, uc);
-        for (int p0 = ((N - 1) / NBF) * NBF; p0 >= 0; p0 -= NBF) {
-            int nbp = std::min(N, p0 + NBF) - p0, Lp = M - p0;
+        for (int p0 = ((N - 1) / nbf) * nbf; p0 >= 0; p0 -= nbf) {
+            int nbp = std::min(N, p0 + nbf) - p0, Lp = M - p0;
             paco_count_launch(), bd_panel_vectors<<<std::min(4096, ceil_div((long)Lp * NBF, 256)), 256, 0, s>>>(
                 x.W, x.ldw, p0, nbp, Lp, 0, x.Vp);
             // columns < p0 of [I; 0] have no entries in rows >= p0: the block leaves them
@@ -934,8 +936,8 @@ int bd_run_multi(int k, const BdJob *jobs, cudaStream_t s0, cudaStream_t *side, 
         }
         // V = G_0 ... G_{N-2} (row reflectors), then Vt = V^T
         paco_count_launch(), bd_set_identity<<<std::min(8192, ceil_div((long)N * N, 256)), 256, 0, s>>>(x.Vtmp, N, N);
-        for (int p0 = ((N - 1) / NBF) * NBF; p0 >= 0; p0 -= NBF) {
-            int nbp = std::min(N - 1, p0 + NBF) - p0, Lp = N - p0 - 1;
+        for (int p0 = ((N - 1) / nbf) * nbf; p0 >= 0; p0 -= nbf) {
+            int nbp = std::min(N - 1, p0 + nbf) - p0, Lp = N - p0 - 1;
             if (nbp <= 0 || Lp <= 0) continue;
             paco_count_launch(), bd_panel_vectors<<<std::min(4096, ceil_div((long)Lp * NBF, 256)), 256, 0, s>>>(
                 x.W, x.ldw, p0, nbp, Lp, 1, x.Vp);

@@ -110,12 +110,13 @@ struct TuneEntry {
 std::mutex g_tune_mu;
 std::vector<TuneEntry> g_tune;
 unsigned g_tune_gen = 0;
-const PacoTune kTuneDefault = {1, bd::RMIN_PER_BLOCK, 1, 0};
+const PacoTune kTuneDefault = {1, bd::RMIN_PER_BLOCK, 1, 0, 0, 0, 0};
 
 bool tune_valid(const PacoTune &t)
 {
     return (t.persistent == 0 || t.persistent == 1) && (t.tc == 0 || t.tc == 1) && t.rows_per_cta >= 4 &&
-           t.rows_per_cta <= 256 && (t.no_tail == 0 || t.no_tail == 1);
+           t.rows_per_cta <= 256 && (t.no_tail == 0 || t.no_tail == 1) && (t.wy == 0 || t.wy == 64 || t.wy == 128) &&
+           (t.qb == 0 || t.qb == 32 || t.qb == 64) && t.mk >= 0 && t.mk <= PK_KMAX;
 }
 
 void tune_store(int M, int N, const PacoTune &cfg)
@@ -429,7 +430,8 @@ static int svd_direct_qr(int M, int N, const float *A, float *U, float *Vt, floa
     bd_init_attrs();
     paco_count_launch(), dev_status_begin<<<1, 64, 0, s>>>(st, 1);
     bd_copy_in_launch(A, wq.W, M, N, wq.ldw, st, s);
-    int rc = qr_factor(wq, M, N, tau, s);
+    const PacoTune tn = paco_tune_for(M, N);
+    int rc = qr_factor(wq, M, N, tau, s, tn.qb);
     if (rc) return rc;
     qr_extract_r_launch(wq, N, AR, s);
     rc = bd_run(N, N, AR, AR, UR, Vt, sigma, e, tq, tp, b + L.ws, s, device_sms());
@@ -438,7 +440,7 @@ static int svd_direct_qr(int M, int N, const float *A, float *U, float *Vt, floa
     rc = bdc_run(N, N, AR, UR, Vt, sigma, e, (float *)(b + L.qt), (float *)(b + L.wt), (uint32_t *)(b + L.idx),
                  b + L.ws, nullptr, s);
     if (rc) return rc;
-    return qr_form_u(wq, M, N, tau, UR, U, s, thin ? N : M);
+    return qr_form_u(wq, M, N, tau, UR, U, s, thin ? N : M, tn.wy);
 }
 
 // One-stage SVD with the thin U (M x N): stage 1 forms H_0 ... H_{N-1} [I; 0]
@@ -644,9 +646,10 @@ cudaStream_t *side_streams()
     return g_side[dev];
 }
 
-int multi_group(int count)
+int multi_group(int count, int M, int N)
 {
-    const int k = g_multi_k > 0 ? g_multi_k : 4;
+    const int tuned = paco_tune_for(M, N).mk;
+    const int k = g_multi_k > 0 ? g_multi_k : (tuned > 0 ? tuned : 4);
     return std::max(1, std::min({count, k, PK_KMAX}));
 }
 
@@ -663,7 +666,7 @@ MultiLayout multi_layout(int count, int M, int N)
     m.a_off = m.L.total;  // the M x N scratch that replaces A (A stays read only)
     m.per = (m.a_off + sizeof(float) * (size_t)M * N + 255) & ~(size_t)255;
     if (qr_possible(M, N)) m.per = std::max(m.per, qr_layout(M, N).total);  // QR-first reads A only
-    m.k = multi_group(count);
+    m.k = multi_group(count, M, N);
     m.total = m.per * m.k;
     return m;
 }
@@ -733,7 +736,7 @@ int svd_multi_qr(int count, int M, int N, const float *const *A, float *const *U
         for (int j = 0; j < k && !rc; j++) {
             char *b = ws + (size_t)j * ml.per;
             bd_copy_in_launch(A[g0 + j], wq[j].W, M, N, wq[j].ldw, sp.st[j], side[j]);
-            rc = qr_factor(wq[j], M, N, (float *)(b + Q.tau), side[j]);
+            rc = qr_factor(wq[j], M, N, (float *)(b + Q.tau), side[j], paco_tune_for(M, N).qb);
             qr_extract_r_launch(wq[j], N, (float *)(b + Q.ar), side[j]);
         }
         join(k);
@@ -746,7 +749,9 @@ int svd_multi_qr(int count, int M, int N, const float *const *A, float *const *U
             paco_count_launch(), dev_status_begin<<<1, 64, 0, side[j]>>>(sp.st[j], 2);
             rc = bdc_run(N, N, jobs[j].a_out, jobs[j].u, Vt[g0 + j], sigma[g0 + j], jobs[j].e, (float *)(b + L.qt),
                          (float *)(b + L.wt), (uint32_t *)(b + L.idx), b + L.ws, nullptr, side[j]);
-            if (!rc) rc = qr_form_u(wq[j], M, N, (float *)(b + Q.tau), jobs[j].u, U[g0 + j], side[j]);
+            if (!rc)
+                rc = qr_form_u(wq[j], M, N, (float *)(b + Q.tau), jobs[j].u, U[g0 + j], side[j], M,
+                               paco_tune_for(M, N).wy);
         }
         join(k);
         if (rc) return rc;
@@ -858,10 +863,90 @@ int paco_tune_get(int M, int N, int cfg[4])
 int paco_tune_set(int M, int N, const int cfg[4])
 {
     if (!cfg || !shape_ok(M, N)) return PACO_ERR_INVALID_ARG;
-    const PacoTune t = {cfg[0], cfg[1], cfg[2], cfg[3]};
+    PacoTune t = paco_tune_for(M, N);  // the tile-shape fields stay as they are
+    t.persistent = cfg[0]; t.rows_per_cta = cfg[1]; t.tc = cfg[2]; t.no_tail = cfg[3];
     if (!tune_valid(t)) return PACO_ERR_INVALID_ARG;
     tune_store(M, N, t);
     return PACO_OK;
+}
+
+int paco_tune_param(int M, int N, int which, int value)
+{
+    if (!shape_ok(M, N) || which < 0 || which > 7) return -1;
+    if (which == 7) return paco_tune_qr(M, N, value);
+    PacoTune t = paco_tune_for(M, N);
+    int *f[7] = {&t.persistent, &t.rows_per_cta, &t.tc, &t.no_tail, &t.wy, &t.qb, &t.mk};
+    if (value == -1) return *f[which];
+    *f[which] = value;
+    if (!tune_valid(t)) return -1;
+    tune_store(M, N, t);
+    return value;
+}
+
+int paco_autotune_multi(int count, int M, int N, void *stream, double out[4])
+{
+    if (count < 2 || !shape_ok(M, N)) return PACO_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int prev_global = g_multi_k;
+    g_multi_k = 0;  // the per-shape entry decides during the trials
+    PacoTune t0 = paco_tune_for(M, N);
+    size_t wsb = 0;
+    const int ks[] = {2, 4, 8};
+    for (int k : ks) {
+        PacoTune c = t0;
+        c.mk = k;
+        tune_store(M, N, c);
+        wsb = std::max(wsb, multi_layout(count, M, N).total);
+    }
+    std::vector<float *> A(count, nullptr), U(count, nullptr), Vt(count, nullptr), sg(count, nullptr);
+    char *ws = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t err = cudaSuccess;
+    for (int b = 0; b < count && !err; b++) {
+        err = cudaMalloc(&A[b], sizeof(float) * (size_t)M * N);
+        err = err ? err : cudaMalloc(&U[b], sizeof(float) * (size_t)M * M);
+        err = err ? err : cudaMalloc(&Vt[b], sizeof(float) * (size_t)N * N);
+        err = err ? err : cudaMalloc(&sg[b], sizeof(float) * N);
+    }
+    err = err ? err : cudaMalloc(&ws, wsb);
+    err = err ? err : cudaEventCreate(&e0);
+    err = err ? err : cudaEventCreate(&e1);
+    int rc = err ? PACO_ERR_CUDA : PACO_OK;
+    float best = 1e30f, first = 0.f;
+    int bk = t0.mk > 0 ? t0.mk : 4, tried = 0;
+    for (int b = 0; b < count && !rc; b++)
+        paco_count_launch(), tune_fill<<<std::min(4096, ceil_div((long)M * N, 256)), 256, 0, s>>>(A[b], (long)M * N,
+                                                                                                   777u + b);
+    for (int k : ks) {
+        if (rc || k > count) break;
+        PacoTune c = t0;
+        c.mk = k;
+        tune_store(M, N, c);
+        const MultiLayout ml = multi_layout(count, M, N);
+        float tk = 1e30f;
+        for (int rep = 0; rep < 2 && !rc; rep++) {
+            cudaEventRecord(e0, s);
+            int r = svd_multi_direct(count, M, N, A.data(), U.data(), Vt.data(), sg.data(), nullptr, ws, ml, s);
+            cudaEventRecord(e1, s);
+            if (r || cudaEventSynchronize(e1) != cudaSuccess) { rc = r ? r : PACO_ERR_CUDA; break; }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0) tk = ms;  // the first run warms up
+        }
+        tried++;
+        if (k == ks[0]) first = tk;
+        if (tk < best) { best = tk; bk = k; }
+    }
+    PacoTune c = t0;
+    c.mk = rc ? t0.mk : bk;
+    tune_store(M, N, c);
+    g_multi_k = prev_global;
+    if (out) { out[0] = bk; out[1] = best; out[2] = first; out[3] = tried; }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    for (int b = 0; b < count; b++) { cudaFree(A[b]); cudaFree(U[b]); cudaFree(Vt[b]); cudaFree(sg[b]); }
+    cudaFree(ws);
+    return rc;
 }
 
 int paco_autotune(int M, int N, void *stream, double out[4])
@@ -886,8 +971,10 @@ int paco_autotune(int M, int N, void *stream, double out[4])
     // SIMT engine for the large products, the two-kernel row/column passes,
     // the last columns on the panel kernel; for tall shapes the best of them
     // is then also timed with the QR-first choice flipped
-    const PacoTune cands[] = {{1, bd::RMIN_PER_BLOCK, 1, 0}, {1, 8, 1, 0}, {1, 32, 1, 0}, {1, bd::RMIN_PER_BLOCK, 0, 0},
-                              {0, bd::RMIN_PER_BLOCK, 1, 0}, {1, bd::RMIN_PER_BLOCK, 1, 1}};
+    PacoTune cands[] = {{1, bd::RMIN_PER_BLOCK, 1, 0}, {1, 8, 1, 0}, {1, 32, 1, 0}, {1, bd::RMIN_PER_BLOCK, 0, 0},
+                        {0, bd::RMIN_PER_BLOCK, 1, 0}, {1, bd::RMIN_PER_BLOCK, 1, 1}};
+    const int mk0 = paco_tune_for(M, N).mk;  // the multi-matrix group size is tuned separately
+    for (PacoTune &c : cands) c.mk = mk0;
     const int nc = (int)(sizeof(cands) / sizeof(cands[0]));
     float best = 1e30f, tdef = 0.f;
     int bi = 0, tried = 0;
@@ -925,6 +1012,26 @@ int paco_autotune(int M, int N, void *stream, double out[4])
             const float tq = time_one();
             if (!rc && tq < best) best = tq;
             else paco_tune_qr(M, N, mode);
+        }
+        // tile shapes of the blocked products: 64-reflector WY blocks, 32-column QR blocks
+        PacoTune t = paco_tune_for(M, N);
+        const int wy_sizes[] = {64};
+        for (int wy : wy_sizes) {
+            if (rc) break;
+            PacoTune c = t;
+            c.wy = wy;
+            tune_store(M, N, c);
+            const float tw = time_one();
+            if (!rc && tw < best) { best = tw; t = c; }
+            else tune_store(M, N, t);
+        }
+        if (!rc && qr_chosen(M, N)) {
+            PacoTune c = t;
+            c.qb = 32;
+            tune_store(M, N, c);
+            const float tb = time_one();
+            if (!rc && tb < best) { best = tb; t = c; }
+            else tune_store(M, N, t);
         }
     }
     if (out) { out[0] = bi; out[1] = best; out[2] = tdef; out[3] = tried; }

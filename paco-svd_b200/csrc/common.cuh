@@ -84,9 +84,13 @@ int paco_device();
 // column passes, rows per CTA of a panel (sets the grid: fewer CTAs meet at
 // each barrier, more CTAs stream more bandwidth), and whether the large
 // products use the tcgen05 GEMM, and whether the last columns stay on the
-// panel kernel instead of the cluster kernel (no_tail = 1).
+// panel kernel instead of the cluster kernel (no_tail = 1); the tile shapes
+// of the blocked products: reflectors per compact-WY block when U and V are
+// formed (wy: 64 or 128), columns per QR block (qb: 32 or 64), and matrices
+// per lockstep group of the multi-matrix form (mk: 1..8).  0 = the default.
 struct PacoTune {
     int persistent, rows_per_cta, tc, no_tail;
+    int wy, qb, mk;
 };
 PacoTune paco_tune_for(int M, int N);
 

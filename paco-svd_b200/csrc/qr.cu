@@ -276,12 +276,13 @@ bool qr_fits(int M, int N)
 
 // The columns of W (M x ldw, already holding A) become R (upper triangle) and
 // the Householder vectors (below the diagonal); tau[N] receives the scalars.
-int qr_factor(const BdWs &w, int M, int N, float *tau, cudaStream_t s)
+int qr_factor(const BdWs &w, int M, int N, float *tau, cudaStream_t s, int qb)
 {
     const QrCfg cfg = qr_cfg();
     if (!qr_fits(M, N)) return PACO_ERR_UNSUPPORTED;
-    for (int q0 = 0; q0 < N; q0 += QB) {
-        const int nb = std::min(QB, N - q0), rows = M - q0;
+    qb = (qb == 32) ? 32 : QB;
+    for (int q0 = 0; q0 < N; q0 += qb) {
+        const int nb = std::min(qb, N - q0), rows = M - q0;
         QrArgs a;
         a.W = w.W; a.ldw = w.ldw; a.M = M; a.q0 = q0; a.nb = nb;
         a.rpc = (rows + cfg.cs - 1) / cfg.cs;
@@ -320,12 +321,14 @@ void qr_extract_r_launch(const BdWs &w, int N, float *R, cudaStream_t s)
 
 // U (M x uc, ld uc; uc = M, or N for the thin U) <- the first uc columns of
 // Q blockdiag(UR, I), Q = H_0 ... H_{N-1} from qr_factor
-int qr_form_u(const BdWs &w, int M, int N, const float *tau, const float *UR, float *U, cudaStream_t s, int uc)
+int qr_form_u(const BdWs &w, int M, int N, const float *tau, const float *UR, float *U, cudaStream_t s, int uc,
+              int nbf)
 {
     if (uc <= 0) uc = M;
+    nbf = (nbf == 64) ? 64 : bd::NBF;
     paco_count_launch(), qr_blockdiag<<<std::min(8192, ceil_div((long)M * uc, 256)), 256, 0, s>>>(UR, N, M, uc, U);
-    for (int p0 = ((N - 1) / bd::NBF) * bd::NBF; p0 >= 0; p0 -= bd::NBF) {
-        const int nbp = std::min(N, p0 + bd::NBF) - p0, Lp = M - p0;
+    for (int p0 = ((N - 1) / nbf) * nbf; p0 >= 0; p0 -= nbf) {
+        const int nbp = std::min(N, p0 + nbf) - p0, Lp = M - p0;
         bd_column_vectors(w.W, w.ldw, p0, nbp, Lp, w.Vp, s);
         if (apply_block_reflector_ex(w, U, uc, p0, Lp, 0, uc, nbp, tau + p0, false, s) != cudaSuccess)
             return PACO_ERR_CUDA;

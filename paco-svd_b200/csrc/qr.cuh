@@ -14,10 +14,13 @@ bool qr_fits(int M, int N);
 // W of the stage-1 workspace w (M x ldw, holding A) <- R in its upper
 // triangle and the Householder vectors below the diagonal; tau[N] the
 // scalars.  Enqueued on s.
-int qr_factor(const BdWs &w, int M, int N, float *tau, cudaStream_t s);
+// qb: columns per block, 64 (QB, also for 0) or 32.
+int qr_factor(const BdWs &w, int M, int N, float *tau, cudaStream_t s, int qb = 0);
 // R (N x N, ld N) <- the upper triangle of W[0:N, 0:N].
 void qr_extract_r_launch(const BdWs &w, int N, float *R, cudaStream_t s);
 // U (M x uc, ld uc) <- the first uc columns of Q blockdiag(UR, I) with Q from
 // qr_factor and UR N x N (ld N; null: the identity, so U = Q); uc = M (0
 // means M), or N for the thin U.
-int qr_form_u(const BdWs &w, int M, int N, const float *tau, const float *UR, float *U, cudaStream_t s, int uc = 0);
+// nbf: reflectors per block update, 128 (NBF, also for 0) or 64.
+int qr_form_u(const BdWs &w, int M, int N, const float *tau, const float *UR, float *U, cudaStream_t s, int uc = 0,
+              int nbf = 0);

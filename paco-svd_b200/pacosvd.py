@@ -93,6 +93,10 @@ def lib():
         L.paco_svd_thin.restype = i
         L.paco_tune_qr.argtypes = [i, i, i]
         L.paco_tune_qr.restype = i
+        L.paco_tune_param.argtypes = [i, i, i, i]
+        L.paco_tune_param.restype = i
+        L.paco_autotune_multi.argtypes = [i, i, i, vp, ctypes.POINTER(ctypes.c_double)]
+        L.paco_autotune_multi.restype = i
         L.paco_multi_group.argtypes = [i]
         L.paco_multi_group.restype = i
         _lib = L
@@ -279,7 +283,27 @@ def autotune(M: int, N: int, stream=None) -> dict:
     _check(lib().paco_autotune(M, N, _stream(stream), out), "paco_autotune")
     k = int(out[0])
     return {"choice": k, "name": TUNE_CANDIDATES[k] if k < len(TUNE_CANDIDATES) else str(k),
-            "ms": out[1], "default_ms": out[2], "candidates": int(out[3]), "config": tune_get(M, N)}
+            "ms": out[1], "default_ms": out[2], "candidates": int(out[3]), "config": tune_get(M, N),
+            "fields": {f: tune_param(M, N, f) for f in TUNE_FIELDS}}
+
+
+TUNE_FIELDS = ["persistent", "rows_per_cta", "tc", "no_tail", "wy", "qb", "mk", "qr"]
+
+
+def tune_param(M: int, N: int, name: str, value: int = -1) -> int:
+    """One field of the tuning entry of (M, N) (TUNE_FIELDS); value -1 queries."""
+    r = int(lib().paco_tune_param(M, N, TUNE_FIELDS.index(name), int(value)))
+    if r < 0 and value != -1:
+        raise PacoError(PACO_ERR_INVALID_ARG, f"paco_tune_param {name}={value}")
+    return r
+
+
+def autotune_multi(count: int, M: int, N: int, stream=None) -> dict:
+    """Times lockstep groups of 2, 4 and 8 matrices of the multi-matrix form
+    on `count` synthetic M x N matrices and keeps the fastest for the shape."""
+    out = (ctypes.c_double * 4)()
+    _check(lib().paco_autotune_multi(count, M, N, _stream(stream), out), "paco_autotune_multi")
+    return {"group": int(out[0]), "ms": out[1], "ms_group2": out[2], "candidates": int(out[3])}
 
 
 def tune_get(M: int, N: int):
