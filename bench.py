@@ -518,10 +518,16 @@ def run_multi(args, wl, rank, world, local, dist):
     lib = P.lib()
     lib.paco_launch_count.restype = ctypes.c_ulonglong
     lib.paco_profile_read.argtypes = [ctypes.POINTER(ctypes.c_double)]
+    # the tiling autotuner: the single-matrix configuration of the shape, then
+    # the lockstep group size (before the workspace is sized)
+    tune = tune_m = None
+    if not args.no_autotune:
+        tune = P.autotune(M, N)
+        if not args.multi_group:
+            tune_m = P.autotune_multi(count, M, N)
     if args.multi_group:
         P.multi_group(args.multi_group)
-    group = P.multi_group(0)
-    P.multi_group(group)
+    group = args.multi_group or P.tune_param(M, N, "mk") or 4
     m = P.Multi(count, M, N)
     sig_exact = []
     for b in range(count):
@@ -596,15 +602,18 @@ def run_multi(args, wl, rank, world, local, dist):
     singles = {}
     if rank == 0:
         W = P.Workspace(M, N)
+        tuned_cfg, tuned_qr = P.tune_get(M, N), P.tune_qr(M, N)
         for name, cfg in (("plain_fp32_single", [1, 16, 0, 0]), ("precision_single", None)):
             # plain: the reference's method (one-stage bidiagonalization, no QR
-            # first) with SIMT FP32 products; precision: the defaults
+            # first) with SIMT FP32 products; precision: the tuned configuration
+            # the multi-matrix form runs with
             if cfg is not None:
                 P.tune_set(M, N, cfg)
                 P.tune_qr(M, N, 0)
             else:
-                P.tune_set(M, N, [1, 16, 1, 0])
-                P.tune_qr(M, N, 2)
+                P.tune_set(M, N, tuned_cfg)
+                P.tune_qr(M, N, tuned_qr)
+            qr_in_use = P.tune_qr(M, N, -2) == 1
             times = []
             with torch.cuda.stream(stream):
                 for k in range(3 + 3):
@@ -625,8 +634,11 @@ def run_multi(args, wl, rank, world, local, dist):
                              "form": ("one paco_svd call per matrix, the one-stage method with SIMT FP32 "
                                       "products (tuning entry tc = 0, QR-first off)"
                                       if cfg is not None else
-                                      "one paco_svd call per matrix, QR-first, 3xTF32 tcgen05 products")}
-        P.tune_set(M, N, [1, 16, 1, 0])
+                                      "one paco_svd call per matrix, the tuned configuration ("
+                                      + ("QR-first, " if qr_in_use else "one-stage, ")
+                                      + "3xTF32 tcgen05 products)")}
+        P.tune_set(M, N, tuned_cfg)
+        P.tune_qr(M, N, tuned_qr)
         del W
 
     e2e = None
@@ -673,7 +685,9 @@ def run_multi(args, wl, rank, world, local, dist):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": multi_config(args.workload, wl),
             "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-            "form": f"paco_svd_multi, lockstep groups of {group or 4}, 3xTF32 tcgen05 products",
+            "form": f"paco_svd_multi, lockstep groups of {group}, 3xTF32 tcgen05 products",
+            "autotune": ({"single": {"choice": tune["name"], "ms": tune["ms"], "fields": tune["fields"]},
+                          "multi": tune_m} if tune else None),
             "latency": {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                         "definition": "a result is delivered when its call returns: the call's duration"},
             "accuracy": acc, "clocks": clk,
