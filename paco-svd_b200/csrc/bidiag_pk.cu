@@ -145,6 +145,7 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
     // panel columns s_pan[parity][row][lane] and dot partials
     // red2[parity][warp][row] (the two passes never overlap)
     __shared__ float cpool[3][RP_THREADS / 32][32];
+    __shared__ float xs2[2][16];  // the batch rows' updated column entries, by batch parity
     float(*cy)[32] = cpool[0];
     float(*cA)[32] = cpool[1];
     float(*cB)[32] = cpool[2];
@@ -302,9 +303,10 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
         float w_ss = 0.f, w_g1 = 0.f, w_g2 = 0.f;
         if constexpr (REG) {
             // Rows held in registers between the dot products and the A^T x
-            // share: one CTA barrier per batch.  Every warp forms every row's
-            // scalars (the same inputs and order in every warp); warp rr makes
-            // row rr's writes.  The stage is refilled right after the barrier.
+            // share (one read of the stage), two CTA barriers per batch, and
+            // the stage refilled right after the first: the rows' panel
+            // columns go to shared memory first for the per-row scalars,
+            // which warp rr forms for row rr.
             for (int bb = 0; bb < nbatch; bb++) {
                 const int k0 = kfirst + bb * R, nr = min(R, nown - k0);
                 const int par = bb & 1, stage = bb & 1;
@@ -342,52 +344,58 @@ __global__ void __launch_bounds__(RP_THREADS, 1)
                     proxy_async_fence();
                     issue_rows(kfirst, bb + 2, stage);
                 }
-#pragma unroll
-                for (int rr = 0; rr < RB; rr++) {
-                    if (rr >= nr) continue;
-                    const int r = own_row(k0 + rr);
+                if (warp < nr) {
+                    const int rr = warp, r = own_row(k0 + rr);
                     const float pan = span[rr * 32 + lane];
                     float aq = (lane < ii) ? pan : 0.f;
-                    if (lane == ii - 1) aq *= invc;
+                    if (lane == ii - 1) {
+                        aq *= invc;
+                        a.W[(long)r * ldw + (i - 1)] = aq;
+                        if (resident) tiles[(long)(k0 + rr) * L + lane] = aq;
+                    }
                     const float xq = (doX && lane < iip)
                                          ? (xsm ? xsm[(k0 + rr) * NB + lane] : a.X[(long)r * NB + lane])
                                          : 0.f;
                     float Xn = 0.f;
                     if (doX) {
-                        const float dot = warp_sum(lane < RP_THREADS / 32 ? red2[lane * 16 + rr] : 0.f);
+                        float dot = 0.f;
+#pragma unroll
+                        for (int w2 = 0; w2 < RP_THREADS / 32; w2++) dot += red2[w2 * 16 + rr];
                         const float sx = ((lane <= iip) ? aq * s_t3[lane] : 0.f) + ((lane < iip) ? xq * s_t4[lane] : 0.f);
                         Xn = taup_prev * (dot - warp_sum(sx));
-                        if (warp == rr && lane == 0) {
+                        if (lane == 0) {
                             a.X[(long)r * NB + iip] = Xn;
                             if (xsm) xsm[(k0 + rr) * NB + iip] = Xn;
                         }
-                    }
-                    if (warp == rr && lane == ii - 1) {
-                        a.W[(long)r * ldw + (i - 1)] = aq;
-                        if (resident) tiles[(long)(k0 + rr) * L + lane] = aq;
                     }
                     if (doCol) {
                         const float xrq = (lane < ii - 1) ? xq : ((lane == ii - 1) ? Xn : 0.f);
                         const float sc = (lane < ii) ? (aq * s_ycol[lane] + xrq * s_wcol[lane]) : 0.f;
                         const float xr = __shfl_sync(0xffffffffu, pan, ii & 31) - warp_sum(sc);
-                        if (warp == rr) {
-                            if (lane == 0) {
-                                a.W[(long)r * ldw + i] = xr;
-                                if (resident) tiles[(long)(k0 + rr) * L + ii] = xr;
-                            }
-                            if (r == i) {
-                                // pivot and row-i panel entries for every CTA's column reflector
-                                if (lane == 0) a.bcA[0] = xr;
-                                if (lane < ii) {
-                                    a.bcA[1 + lane] = aq;
-                                    a.bcA[1 + ii + lane] = xrq;
-                                }
-                            } else if (r > i) {
-                                if (lane == 0) w_ss += xr * xr;
-                                if (lane < ii) { w_g1 += aq * xr; w_g2 += xrq * xr; }
-                            }
+                        if (lane == 0) {
+                            a.W[(long)r * ldw + i] = xr;
+                            if (resident) tiles[(long)(k0 + rr) * L + ii] = xr;
+                            xs2[par][rr] = xr;
                         }
-                        if (r > i) {
+                        if (r == i) {
+                            // pivot and row-i panel entries for every CTA's column reflector
+                            if (lane == 0) a.bcA[0] = xr;
+                            if (lane < ii) {
+                                a.bcA[1 + lane] = aq;
+                                a.bcA[1 + ii + lane] = xrq;
+                            }
+                        } else if (r > i) {
+                            if (lane == 0) w_ss += xr * xr;
+                            if (lane < ii) { w_g1 += aq * xr; w_g2 += xrq * xr; }
+                        }
+                    }
+                }
+                __syncthreads();
+                if (doCol) {
+#pragma unroll
+                    for (int rr = 0; rr < RB; rr++) {
+                        if (rr < nr && own_row(k0 + rr) > i) {
+                            const float xr = xs2[par][rr];
 #pragma unroll
                             for (int k = 0; k < CPT; k++) {
                                 acc4[k].x += v[rr][k].x * xr; acc4[k].y += v[rr][k].y * xr;

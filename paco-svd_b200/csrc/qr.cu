@@ -26,6 +26,7 @@
 namespace {
 
 constexpr int QT = 256, QW = QT / 32;  // threads and warps per CTA
+constexpr int QCS_MAX = 16;            // largest cluster
 
 struct QrArgs {
     float *W;
@@ -113,9 +114,14 @@ __global__ void __launch_bounds__(QT, 1) qr_block_k(QrArgs a)
     for (int j = 0; j < nb; j++) {
         const int pr = a.q0 + j;  // pivot row
         q_cluster_sync();         // every CTA's sums of column j are published
-        float sig = 0.f;
-        for (int c = 0; c < CS; c++) sig += q_ld(q_dsmem(&s_sig, c));
+        // every CTA's partial sum, all remote loads in flight before the first add
+        float part[QCS_MAX];
+#pragma unroll
+        for (int c = 0; c < QCS_MAX; c++) part[c] = (c < CS) ? q_ld(q_dsmem(&s_sig, c)) : 0.f;
         const float x0 = q_ld(q_dsmem(&s_x0, (pr - a.q0) / a.rpc));
+        float sig = 0.f;
+#pragma unroll
+        for (int c = 0; c < QCS_MAX; c++) sig += part[c];
         float beta, tau, v0;
         make_reflector(x0, sig, a.M - pr, &beta, &tau, &v0);
         const float inv = 1.f / v0;
@@ -152,8 +158,12 @@ __global__ void __launch_bounds__(QT, 1) qr_block_k(QrArgs a)
         q_cluster_sync();  // every CTA's partial v^T A is published
         if (kn > 0) {
             if (tid < kn) {
+                float wp[QCS_MAX];
+#pragma unroll
+                for (int c = 0; c < QCS_MAX; c++) wp[c] = (c < CS) ? q_ld(q_dsmem(&s_w[tid], c)) : 0.f;
                 float t = 0.f;
-                for (int c = 0; c < CS; c++) t += q_ld(q_dsmem(&s_w[tid], c));
+#pragma unroll
+                for (int c = 0; c < QCS_MAX; c++) t += wp[c];
                 s_wsum[tid] = t * tau;
             }
             __syncthreads();
