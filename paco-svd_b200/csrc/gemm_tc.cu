@@ -36,6 +36,8 @@ constexpr int TM = 128, TN = 128, TK = 32;  // tile of C; k per image (128 bytes
 constexpr int IMG = TM * TK;                // floats per tile image (16 KB)
 constexpr int STAGES = 2;
 constexpr int MAX_SPLITS = 8;
+constexpr int KCHAIN = 4;              // k images (of 32) per accumulation chain of a skinny product
+constexpr int MAX_CHAIN_SPLITS = 128;
 constexpr uint32_t IDESC = (1u << 4)             // D format F32
                            | (2u << 7)           // A format TF32
                            | (2u << 10)          // B format TF32 (both K-major: bits 15, 16 clear)
@@ -105,6 +107,17 @@ TcGeom tc_geom(int M, int N, int K)
     // enough CTAs to cover the SMs, at least 4 images of k per split
     const int tiles = g.MT * g.NT;
     g.splits = std::max(1, std::min({MAX_SPLITS, ceil_div(148, tiles), g.KT / 4}));
+    // The tensor cores round each accumulation into TMEM toward zero, so a
+    // long k chain loses about one ulp of the running sum per MMA.  Skinny
+    // products (one or two row tiles, e.g. V^T Q with k = the matrix height)
+    // are split into k chains of at most KCHAIN images whose FP32 partial sums
+    // are added with round-to-nearest, as long as the partials stay small.
+    if (g.MT <= 2) {
+        const int want = ceil_div(g.KT, KCHAIN);
+        const long budget = 32L << 20;  // floats of partial sums
+        const int cap = (int)std::max(1L, std::min((long)MAX_CHAIN_SPLITS, budget / std::max(1L, (long)M * N)));
+        g.splits = std::max(g.splits, std::min(want, cap));
+    }
     return g;
 }
 
