@@ -85,7 +85,8 @@ int paco_tune_qr(int M, int N, int mode);
  * -1 queries.  Returns the value stored or queried, -1 for an invalid
  * argument.  paco_autotune times fields 0-5 (and 7) for one shape;
  * paco_autotune_multi times field 6 (2, 4, 8) on `count` synthetic matrices
- * of the shape (out as paco_autotune's, out[0] = the group size chosen).
+ * of the shape, then for tall shapes the other QR-first choice with that
+ * group size (out as paco_autotune's, out[0] = the group size chosen).
  * paco_multi_group, when set, overrides field 6 for every shape. */
 int paco_tune_param(int M, int N, int which, int value);
 int paco_autotune_multi(int count, int M, int N, void *stream, double out[4]);

@@ -940,6 +940,29 @@ int paco_autotune_multi(int count, int M, int N, void *stream, double out[4])
     PacoTune c = t0;
     c.mk = rc ? t0.mk : bk;
     tune_store(M, N, c);
+    // the QR-first choice of the single-matrix tuning may not suit k matrices
+    // in lockstep (their R factors stream less): time the other choice too
+    if (!rc && qr_possible(M, N) && qr_fits(M, N)) {
+        const int mode = qr_mode_for(M, N);
+        const bool on = qr_chosen(M, N);
+        paco_tune_qr(M, N, on ? 0 : 1);
+        const MultiLayout ml = multi_layout(count, M, N);
+        float tq = 1e30f;
+        if (ml.total <= wsb) {
+            for (int rep = 0; rep < 2 && !rc; rep++) {
+                cudaEventRecord(e0, s);
+                int r = svd_multi_direct(count, M, N, A.data(), U.data(), Vt.data(), sg.data(), nullptr, ws, ml, s);
+                cudaEventRecord(e1, s);
+                if (r || cudaEventSynchronize(e1) != cudaSuccess) { rc = r ? r : PACO_ERR_CUDA; break; }
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (rep > 0) tq = ms;
+            }
+            tried++;
+        }
+        if (!rc && tq < best) best = tq;
+        else paco_tune_qr(M, N, mode);
+    }
     g_multi_k = prev_global;
     if (out) { out[0] = bk; out[1] = best; out[2] = first; out[3] = tried; }
     if (e0) cudaEventDestroy(e0);

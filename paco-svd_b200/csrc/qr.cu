@@ -25,7 +25,7 @@
 
 namespace {
 
-constexpr int QT = 256, QW = QT / 32;  // threads and warps per CTA
+constexpr int QT = 512, QW = QT / 32;  // threads and warps per CTA
 constexpr int QCS_MAX = 16;            // largest cluster
 
 struct QrArgs {
