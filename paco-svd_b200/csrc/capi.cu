@@ -765,6 +765,10 @@ int svd_multi_direct(int count, int M, int N, const float *const *A, float *cons
 {
     cudaStream_t *side = side_streams();
     if (!side) return PACO_ERR_CUDA;
+    // kernel attributes before the first launch (the QR path's products come
+    // before stage 1, which would set them otherwise)
+    bd_init_attrs();
+    bdc_init_attrs();
     cudaEvent_t *fe = bd_fork_events();
     const SvdLayout &L = ml.L;
     if (qr_chosen(M, N)) return svd_multi_qr(count, M, N, A, U, Vt, sigma, status, ws, ml, s, side);

@@ -12,9 +12,10 @@
 //              182-218: mu = +sqrt, Parlett v0, tau = 2 v0^2/(sigma + v0^2),
 //              implicit v[0] = 1) and applies it to the block's remaining
 //              columns.  The CTAs' partial sums (the column norm, then
-//              v^T A for the remaining columns) are read by every CTA through
-//              distributed shared memory and added in rank order, so each
-//              CTA forms the same reflector; two cluster barriers per column.
+//              v^T A for the remaining columns) are pushed into every CTA's
+//              shared memory through distributed shared memory and added in
+//              rank order, so each CTA forms the same reflector; two cluster
+//              barriers per column.
 // trailing     A[q0:, q1:N] <- (I - V T^T V^T) A[q0:, q1:N] through the
 //              block-reflector products of stage 1 (Gram on the SIMT engine,
 //              T, then V^T A, T^T G1, A -= V G2 on the tensor cores).
@@ -47,13 +48,6 @@ __device__ __forceinline__ uint32_t q_dsmem(const void *local, int rank)
     return r;
 }
 
-__device__ __forceinline__ float q_ld(uint32_t addr)
-{
-    float v;
-    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(addr));
-    return v;
-}
-
 __device__ __forceinline__ unsigned q_rank()
 {
     unsigned r;
@@ -82,14 +76,23 @@ __device__ __forceinline__ float q_block_sum(float v, float *red)
     return t;
 }
 
+__device__ __forceinline__ void q_st(uint32_t addr, float v)
+{
+    asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(addr), "f"(v) : "memory");
+}
+
+// Every CTA pushes its partial sums into a slot of its own in every CTA of
+// the cluster (remote stores), so after the cluster barrier each CTA adds the
+// slots from its own shared memory, in rank order.
 __global__ void __launch_bounds__(QT, 1) qr_block_k(QrArgs a)
 {
-    extern __shared__ float qrows[];  // rpc x (QB + 1): this CTA's rows of the block
-    __shared__ float s_sig, s_x0;     // this CTA's partial |x[1:]|^2 and (owner) pivot
-    __shared__ float s_w[QB];         // this CTA's partial v^T A[:, k]
-    __shared__ float wpart[QW][QB];   // per-warp partials
+    extern __shared__ float qrows[];          // rpc x (QB + 1): this CTA's rows of the block
+    __shared__ float s_sig_all[QCS_MAX];      // partial |x[1:]|^2 of the current column, by CTA
+    __shared__ float s_x0_all;                // its pivot, from the owner
+    __shared__ float s_w_all[QCS_MAX][QB];    // partial v^T A[:, k], by CTA
+    __shared__ float wpart[QW][QB];           // per-warp partials
     __shared__ float red[QW];
-    __shared__ float s_wsum[QB];      // v^T A[:, k] of the current column (all CTAs)
+    __shared__ float s_wsum[QB];              // tau v^T A[:, k] of the current column
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int rank = (int)q_rank(), CS = (int)q_nrank();
     const int LD = QB + 1, nb = a.nb;
@@ -99,71 +102,61 @@ __global__ void __launch_bounds__(QT, 1) qr_block_k(QrArgs a)
         const int i = t / nb, k = t % nb;
         qrows[i * LD + k] = a.W[(long)(r0 + i) * a.ldw + a.q0 + k];
     }
-    __syncthreads();
-    // partial sums of column 0 (rows below its pivot)
+    q_cluster_sync();  // every CTA of the cluster runs before the first remote store
+    // publishes this CTA's sum for the column whose pivot row is pr (and the
+    // pivot itself from its owner)
+    auto push_sig = [&](float t, int pr, int col) {
+        if (tid < CS) {
+            q_st(q_dsmem(&s_sig_all[rank], tid), t);
+            if (pr >= r0 && pr < r0 + nr) q_st(q_dsmem(&s_x0_all, tid), qrows[(pr - r0) * LD + col]);
+        }
+    };
     {
         float acc = 0.f;
         for (int i = tid; i < nr; i += QT)
             if (r0 + i > a.q0) acc += qrows[i * LD] * qrows[i * LD];
-        const float t = q_block_sum(acc, red);
-        if (tid == 0) {
-            s_sig = t;
-            if (a.q0 >= r0 && a.q0 < r0 + nr) s_x0 = qrows[(a.q0 - r0) * LD];
-        }
+        push_sig(q_block_sum(acc, red), a.q0, 0);
     }
     for (int j = 0; j < nb; j++) {
         const int pr = a.q0 + j;  // pivot row
-        q_cluster_sync();         // every CTA's sums of column j are published
-        // every CTA's partial sum, all remote loads in flight before the first add
-        float part[QCS_MAX];
-#pragma unroll
-        for (int c = 0; c < QCS_MAX; c++) part[c] = (c < CS) ? q_ld(q_dsmem(&s_sig, c)) : 0.f;
-        const float x0 = q_ld(q_dsmem(&s_x0, (pr - a.q0) / a.rpc));
+        q_cluster_sync();         // every CTA's sums of column j are in place
         float sig = 0.f;
 #pragma unroll
-        for (int c = 0; c < QCS_MAX; c++) sig += part[c];
+        for (int c = 0; c < QCS_MAX; c++) sig += (c < CS) ? s_sig_all[c] : 0.f;
         float beta, tau, v0;
-        make_reflector(x0, sig, a.M - pr, &beta, &tau, &v0);
+        make_reflector(s_x0_all, sig, a.M - pr, &beta, &tau, &v0);
         const float inv = 1.f / v0;
-        // v_r = x_r / v0 below the pivot (stored), beta on the diagonal
-        for (int i = tid; i < nr; i += QT) {
-            const int r = r0 + i;
-            if (r > pr) qrows[i * LD + j] *= inv;
-        }
-        __syncthreads();
-        // partial w_k = sum_r v_r A[r, k] over the remaining columns (v_pr = 1)
+        // partial w_k = sum_r v_r A[r, k] over the remaining columns, with
+        // v_r = x_r / v0 below the pivot (stored in place by lane 0 of the
+        // row's warp) and v_pr = 1
         const int kn = nb - j - 1;
         float acc0 = 0.f, acc1 = 0.f;
-        if (kn > 0) {
-            for (int i = warp; i < nr; i += QW) {
-                const int r = r0 + i;
-                if (r < pr) continue;
-                const float v = (r == pr) ? 1.f : qrows[i * LD + j];
-                const int k0 = j + 1 + lane, k1 = j + 33 + lane;
-                if (k0 < nb) acc0 += v * qrows[i * LD + k0];
-                if (k1 < nb) acc1 += v * qrows[i * LD + k1];
-            }
-            wpart[warp][lane] = acc0;
-            wpart[warp][lane + 32] = acc1;
+        for (int i = warp; i < nr; i += QW) {
+            const int r = r0 + i;
+            if (r < pr) continue;
+            const float v = (r == pr) ? 1.f : qrows[i * LD + j] * inv;
+            const int k0 = j + 1 + lane, k1 = j + 33 + lane;
+            if (k0 < nb) acc0 += v * qrows[i * LD + k0];
+            if (k1 < nb) acc1 += v * qrows[i * LD + k1];
+            __syncwarp();
+            if (lane == 0) qrows[i * LD + j] = (r == pr) ? beta : v;
         }
+        wpart[warp][lane] = acc0;
+        wpart[warp][lane + 32] = acc1;
         __syncthreads();
         if (tid < kn) {
             float t = 0.f;
 #pragma unroll
             for (int w = 0; w < QW; w++) t += wpart[w][tid];
-            s_w[tid] = t;
+            for (int c = 0; c < CS; c++) q_st(q_dsmem(&s_w_all[rank][tid], c), t);
         }
-        if (tid == 0 && pr >= r0 && pr < r0 + nr) qrows[(pr - r0) * LD + j] = beta;
         if (tid == 0 && rank == 0) a.tau[pr] = tau;
-        q_cluster_sync();  // every CTA's partial v^T A is published
+        q_cluster_sync();  // every CTA's partial v^T A is in place
         if (kn > 0) {
             if (tid < kn) {
-                float wp[QCS_MAX];
-#pragma unroll
-                for (int c = 0; c < QCS_MAX; c++) wp[c] = (c < CS) ? q_ld(q_dsmem(&s_w[tid], c)) : 0.f;
                 float t = 0.f;
 #pragma unroll
-                for (int c = 0; c < QCS_MAX; c++) t += wp[c];
+                for (int c = 0; c < QCS_MAX; c++) t += (c < CS) ? s_w_all[c][tid] : 0.f;
                 s_wsum[tid] = t * tau;
             }
             __syncthreads();
@@ -182,11 +175,7 @@ __global__ void __launch_bounds__(QT, 1) qr_block_k(QrArgs a)
                 }
                 if (k1 < nb) qrows[i * LD + k1] -= v * s_wsum[lane + 32];
             }
-            const float t = q_block_sum(acc, red);
-            if (tid == 0) {
-                s_sig = t;
-                if (pr + 1 >= r0 && pr + 1 < r0 + nr) s_x0 = qrows[(pr + 1 - r0) * LD + j + 1];
-            }
+            push_sig(q_block_sum(acc, red), pr + 1, j + 1);
         }
     }
     __syncthreads();
@@ -194,7 +183,7 @@ __global__ void __launch_bounds__(QT, 1) qr_block_k(QrArgs a)
         const int i = t / nb, k = t % nb;
         a.W[(long)(r0 + i) * a.ldw + a.q0 + k] = qrows[i * LD + k];
     }
-    q_cluster_sync();  // no CTA leaves while another may still read its shared memory
+    q_cluster_sync();  // no CTA leaves while another may still write into its shared memory
 }
 
 // R (N x N, ld N) <- the upper triangle of W[0:N, 0:N]
