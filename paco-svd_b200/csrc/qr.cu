@@ -228,7 +228,7 @@ QrCfg qr_cfg()
         cudaGetLastError();
         return cfg;
     }
-    const int smem = optin - 8192;  // room for the static shared memory
+    const int smem = optin - 16384;  // room for the static shared memory
     if (cudaFuncSetAttribute(qr_block_k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
         cudaFuncSetAttribute(qr_block_k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
         cudaGetLastError();
