@@ -172,9 +172,16 @@ __global__ void __launch_bounds__(256) tc_pack(GemmOp X, int transposed, int R, 
 
 // ------------------------------------------------------------------ GEMM
 
+// Direct B: when Bd.p is set, B is not pre-packed: it is a plain row-major
+// operand (B(k, n) = Bd.p[k * Bd.rs + n]) that all 128 threads read from
+// global memory one 32 x 128 tile at a time (the next tile's loads in flight
+// while the current tile's MMAs run), split into TF32 hi and lo parts and
+// store into the stage's images in the swizzled K-major layout tc_pack writes.
+// A stays pre-packed (bulk copies).  Kdim is K (rows of B beyond it read 0).
 __global__ void __launch_bounds__(128, 1)
     tc_gemm(int M, int N, int KT, int kper, float alpha, const float *Ahi, const float *Alo, const float *Bhi,
-            const float *Blo, float beta, float *C, long ldc, float *part, int ctma, const int *lim, DevStatus *st)
+            const float *Blo, float beta, float *C, long ldc, float *part, int ctma, const int *lim, DevStatus *st,
+            GemmOp Bd, int Kdim)
 {
     if (lim) M = min(M, *lim);  // rows at or beyond the limit are left as they are
     extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
@@ -224,13 +231,95 @@ __global__ void __launch_bounds__(128, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
 
-    if (tid == 0) {
+    if (tid == 0 && cload) {
         // the C tile streams in while the products run
-        if (cload) {
-            mbar_expect_tx(&cbar, (uint32_t)(nrows * ncols * 4));
-            for (int r = 0; r < nrows; r++)
-                tma_load_1d(Csm + r * TN, Cd + (long)(m0 + r) * ld + n0, (uint32_t)(ncols * 4), &cbar);
+        mbar_expect_tx(&cbar, (uint32_t)(nrows * ncols * 4));
+        for (int r = 0; r < nrows; r++)
+            tma_load_1d(Csm + r * TN, Cd + (long)(m0 + r) * ld + n0, (uint32_t)(ncols * 4), &cbar);
+    }
+    if (Bd.p) {
+        // thread (warp w, lane l): k chunks c = w, w + 4 (4 k each) of image
+        // rows n = l + 32 j, j < 4
+        const long abase = (long)mt * KT * IMG;
+        float rb[2][4][4];
+        auto load_b = [&](int j) {
+            const int kbase = (kb0 + j) * TK;
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++)
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const int gk = kbase + 4 * (warp + 4 * cc) + i;
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const int gn = n0 + lane + 32 * q;
+                        rb[cc][i][q] = (gk < Kdim && gn < N) ? __ldg(Bd.p + (long)gk * Bd.rs + gn) : 0.f;
+                    }
+                }
+        };
+        if (nk > 0) load_b(0);
+        bool ok = true;
+        int issued = 0, consumed = 0;
+        for (int kb = 0; kb < nk; kb++) {
+            const int s = kb % STAGES;
+            // the stage's previous MMAs are done before it is refilled
+            if (tid == 0 && kb >= STAGES && ok && !mbar_wait_bounded(&empty[s], ((kb / STAGES) - 1) & 1, st, 505))
+                ok = false;
+            if (__syncthreads_or(tid == 0 && !ok)) break;
+            float *dst = stage + (long)s * 4 * IMG;
+            if (tid == 0) {
+                mbar_expect_tx(&full[s], 2u * IMG * 4u);
+                tma_load_1d(dst + 0 * IMG, Ahi + abase + (long)(kb0 + kb) * IMG, IMG * 4u, &full[s]);
+                tma_load_1d(dst + 1 * IMG, Alo + abase + (long)(kb0 + kb) * IMG, IMG * 4u, &full[s]);
+                issued = kb + 1;
+            }
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++) {
+                const int c = warp + 4 * cc;
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const int r = lane + 32 * q;
+                    float4 h, l;
+                    h.x = tf32_round(rb[cc][0][q]); l.x = tf32_round(rb[cc][0][q] - h.x);
+                    h.y = tf32_round(rb[cc][1][q]); l.y = tf32_round(rb[cc][1][q] - h.y);
+                    h.z = tf32_round(rb[cc][2][q]); l.z = tf32_round(rb[cc][2][q] - h.z);
+                    h.w = tf32_round(rb[cc][3][q]); l.w = tf32_round(rb[cc][3][q] - h.w);
+                    const int off = r * TK + ((c ^ (r & 7)) << 2);
+                    *reinterpret_cast<float4 *>(dst + 2 * IMG + off) = h;
+                    *reinterpret_cast<float4 *>(dst + 3 * IMG + off) = l;
+                }
+            }
+            if (kb + 1 < nk) load_b(kb + 1);
+            proxy_async_fence();  // the images written here, visible to the tensor cores
+            __syncthreads();
+            if (tid == 0 && ok) {
+                if (!mbar_wait_bounded(&full[s], (kb / STAGES) & 1, st, 506)) {
+                    ok = false;
+                } else {
+                    consumed = kb + 1;
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t base = smem_u32(dst);
+                    const uint64_t ahi = smem_desc(base), alo = smem_desc(base + IMG * 4);
+                    const uint64_t bhi = smem_desc(base + 2 * IMG * 4), blo = smem_desc(base + 3 * IMG * 4);
+#pragma unroll
+                    for (int j = 0; j < TK / 8; j++) {
+                        const uint64_t dk = (uint64_t)(j * 32 >> 4);
+                        mma_tf32(tmem, alo + dk, bhi + dk, (kb | j) ? 1u : 0u);
+                        mma_tf32(tmem, ahi + dk, blo + dk, 1u);
+                        mma_tf32(tmem, ahi + dk, bhi + dk, 1u);
+                    }
+                    mma_commit(&empty[s]);
+                }
+            }
         }
+        if (tid == 0) {
+            if (!ok) {
+                s_fail = 1;
+                for (int j = consumed; j < issued; j++)
+                    mbar_wait_bounded(&full[j % STAGES], (j / STAGES) & 1, st, 507, 1000000000LL);
+            }
+            mma_commit(&done);
+        }
+    } else if (tid == 0) {
         const long abase = (long)mt * KT * IMG, bbase = (long)nt * KT * IMG;
         auto produce = [&](int j) {  // k-block j of this split into stage j % STAGES
             float *dst = stage + (long)(j % STAGES) * 4 * IMG;
@@ -628,6 +717,11 @@ static bool encode_c_map(CUtensorMap *tm, float *C, int M, int N, long ldc)
 
 // PACO_TC_PERSISTENT=0 keeps every product on the one-tile-per-CTA kernel
 static int g_tc_persistent = -1;
+// PACO_TC_DIRECT_B=0 packs B in a separate pass for the one-tile kernel too
+static const bool g_tc_direct_b = [] {
+    const char *e = getenv("PACO_TC_DIRECT_B");
+    return !(e && e[0] == '0');
+}();
 
 static bool tc_persistent()
 {
@@ -718,13 +812,16 @@ cudaError_t gemm_tc_run(int M, int N, int K, float alpha, GemmOp A, GemmOp B, fl
     float *Bhi = Alo + (size_t)g.MT * g.KT * IMG, *Blo = Bhi + (size_t)g.NT * g.KT * IMG;
     float *part = g.splits > 1 ? Blo + (size_t)g.NT * g.KT * IMG : nullptr;
     const int kper = ceil_div(g.KT, g.splits);
+    const bool persistent = !part && tc_persistent();
+    // the one-tile kernel reads a plain row-major B itself (no packing pass)
+    const bool bdirect = !persistent && !lim && g_tc_direct_b && B.cs == 1 && !B.gather && !B.p2;
     paco_count_launch(), tc_pack<<<g.MT * g.KT, 256, 0, s>>>(A, 0, M, K, g.KT, Ahi, Alo, lim);
-    paco_count_launch(), tc_pack<<<g.NT * g.KT, 256, 0, s>>>(B, 1, N, K, g.KT, Bhi, Blo, lim);
+    if (!bdirect) paco_count_launch(), tc_pack<<<g.NT * g.KT, 256, 0, s>>>(B, 1, N, K, g.KT, Bhi, Blo, lim);
     // bulk-copy epilogue when every row segment of the destination is 16-byte aligned
     const float *dst = part ? part : C;
     const long dld = part ? (long)N : ldc;
     const int ctma = ((((uintptr_t)dst) & 15) == 0 && (dld % 4) == 0 && (N % 4) == 0) ? 1 : 0;
-    if (!part && tc_persistent()) {
+    if (persistent) {
         const int ntiles = g.MT * g.NT;
         const int grid = std::min(ntiles, tc_sms());
         CUtensorMap tm;
@@ -734,8 +831,10 @@ cudaError_t gemm_tc_run(int M, int N, int K, float alpha, GemmOp A, GemmOp B, fl
                                  M, N, g.KT, g.NT, ntiles, alpha, Ahi, Alo, Bhi, Blo, beta, C, ldc, use_tm, tm, lim, st);
         return cudaGetLastError();
     }
+    GemmOp Bd = gop(nullptr, 0, 0);
+    if (bdirect) Bd = B;
     paco_count_launch(), tc_gemm<<<dim3(g.NT, g.MT, g.splits), 128, tc_smem_bytes(), s>>>(
-                             M, N, g.KT, kper, alpha, Ahi, Alo, Bhi, Blo, beta, C, ldc, part, ctma, lim, st);
+                             M, N, g.KT, kper, alpha, Ahi, Alo, Bhi, Blo, beta, C, ldc, part, ctma, lim, st, Bd, K);
     if (part) {
         if (lim) return cudaErrorInvalidValue;  // a limited product is never split (see gemm_tc_scratch_floats)
         return gemm_splitk_reduce_run(M, N, g.splits, alpha, part, beta, C, ldc, s);
