@@ -94,6 +94,19 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32])
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32])
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]),
+        "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]),
+        "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]),
+        "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
+        : "memory");
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
 struct TcGeom {
     int MT, NT, KT, splits;
 };
@@ -112,6 +125,8 @@ TcGeom tc_geom(int M, int N, int K)
     // products (one or two row tiles, e.g. V^T Q with k = the matrix height)
     // are split into k chains of at most KCHAIN images whose FP32 partial sums
     // are added with round-to-nearest, as long as the partials stay small.
+    // (Unsplit products on the persistent kernel chain their k range the same
+    // way inside the kernel, KCP images per chain.)
     if (g.MT <= 2) {
         const int want = ceil_div(g.KT, KCHAIN);
         const long budget = 32L << 20;  // floats of partial sums
@@ -439,9 +454,13 @@ __global__ void __launch_bounds__(128, 1)
 
 // Persistent, warp-specialized form of tc_gemm for products without split-K:
 // CTA b takes tiles b, b + gridDim.x, ... (6 warps).  Warp 0 issues the copies
-// (operand stages; the C tile when beta != 0), warp 1 issues the MMAs into one
-// of two TMEM accumulators (tile parity), warps 2-5 run the epilogue of tile t
-// while the MMAs of tile t+1 proceed.
+// (operand stages; the C tile when beta != 0), warp 1 issues the MMAs, warps
+// 2-5 run the epilogue.  A tile's k range runs in chains of KCP images, chain
+// g into TMEM accumulator g & 1: with one chain per tile the epilogue writes
+// tile t out of its accumulator while the MMAs of tile t+1 fill the other;
+// with several, the epilogue adds each finished chain into FP32 sums (TMEM
+// columns 2TN..3TN-1) while the next chain accumulates, and writes the tile
+// out of the sums.
 // With a tensor map for C (C rows 16-byte aligned, no row limit) the C tile
 // moves in two halves of 64 columns, each with one 2-D TMA load and one TMA
 // store: the load of a half of the next tile starts as soon as the store of
@@ -455,6 +474,7 @@ __global__ void __launch_bounds__(128, 1)
 // at their next check or time out, copies in flight and issued MMAs are
 // waited for (bounded) and the tensor memory is freed.
 constexpr int PT_THREADS = 192;
+constexpr int KCP = 4;  // k images per accumulation chain of the persistent kernel
 constexpr int CH = TN / 2;  // columns of a C half
 
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *tm, int x, int y, uint64_t *bar)
@@ -492,7 +512,7 @@ __global__ void __launch_bounds__(PT_THREADS, 1)
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
-                     "r"(2 * TN)
+                     "r"(4 * TN)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -558,31 +578,37 @@ __global__ void __launch_bounds__(PT_THREADS, 1)
             for (int h = 0; h < 2; h++) mbar_wait_bounded(&cfull[h], (cl - 1) & 1, st, 613, 1000000000LL);
     } else if (warp == 1 && lane == 0) {
         // ------------------------------------------------ MMA issuer
-        int it = 0;
+        // each tile's k range in chains of KCP images, one TMEM accumulator
+        // per chain, alternating (the epilogue folds a finished chain into
+        // its FP32 sums while the next one accumulates)
+        int it = 0, g = 0;
         for (int lt = 0; lt < ntl && !s_abort; lt++) {
-            const int ab = lt & 1;
-            if (lt >= 2 && !mbar_wait_bounded(&acce[ab], ((lt >> 1) - 1) & 1, st, 620)) { s_abort = 1; break; }
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t acc = tmem + (uint32_t)(ab * TN);
             bool ok = true;
-            for (int kb = 0; kb < KT; kb++, it++) {
-                const int sidx = it % STAGES;
-                if (!mbar_wait_bounded(&full[sidx], (it / STAGES) & 1, st, 621)) { ok = false; break; }
+            for (int c0 = 0; c0 < KT && ok; c0 += KCP, g++) {
+                const int ab = g & 1;
+                if (g >= 2 && !mbar_wait_bounded(&acce[ab], ((g >> 1) - 1) & 1, st, 620)) { ok = false; break; }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t base = smem_u32(stage + (long)sidx * 4 * IMG);
-                const uint64_t ahi = smem_desc(base), alo = smem_desc(base + IMG * 4);
-                const uint64_t bhi = smem_desc(base + 2 * IMG * 4), blo = smem_desc(base + 3 * IMG * 4);
+                const uint32_t acc = tmem + (uint32_t)(ab * TN);
+                const int c1 = min(KT, c0 + KCP);
+                for (int kb = c0; kb < c1; kb++, it++) {
+                    const int sidx = it % STAGES;
+                    if (!mbar_wait_bounded(&full[sidx], (it / STAGES) & 1, st, 621)) { ok = false; break; }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t base = smem_u32(stage + (long)sidx * 4 * IMG);
+                    const uint64_t ahi = smem_desc(base), alo = smem_desc(base + IMG * 4);
+                    const uint64_t bhi = smem_desc(base + 2 * IMG * 4), blo = smem_desc(base + 3 * IMG * 4);
 #pragma unroll
-                for (int j = 0; j < TK / 8; j++) {
-                    const uint64_t dk = (uint64_t)(j * 32 >> 4);
-                    mma_tf32(acc, alo + dk, bhi + dk, (kb | j) ? 1u : 0u);
-                    mma_tf32(acc, ahi + dk, blo + dk, 1u);
-                    mma_tf32(acc, ahi + dk, bhi + dk, 1u);
+                    for (int j = 0; j < TK / 8; j++) {
+                        const uint64_t dk = (uint64_t)(j * 32 >> 4);
+                        mma_tf32(acc, alo + dk, bhi + dk, ((kb - c0) | j) ? 1u : 0u);
+                        mma_tf32(acc, ahi + dk, blo + dk, 1u);
+                        mma_tf32(acc, ahi + dk, bhi + dk, 1u);
+                    }
+                    mma_commit(&empty[sidx]);
                 }
-                mma_commit(&empty[sidx]);
+                if (ok) mma_commit(&accf[ab]);
             }
             if (!ok) { s_abort = 1; break; }
-            mma_commit(&accf[ab]);
         }
         mma_commit(&done);  // every MMA issued above has completed when this arrives
         mbar_wait_bounded(&done, 0, st, 622);
@@ -591,16 +617,50 @@ __global__ void __launch_bounds__(PT_THREADS, 1)
         const int q = warp & 3;  // TMEM lane quarter of this warp: rows 32q..32q+31
         const int ew = warp - 2;
         float(*sb)[33] = reinterpret_cast<float(*)[33]>(sbuf + ew * 32 * 33);
+        const int nch = (KT + KCP - 1) / KCP;
+        // with more than one chain, the chains of a tile are summed in FP32
+        // (round-to-nearest) into TMEM columns 2TN..3TN-1, which only the
+        // epilogue touches; a single chain is read straight from its accumulator
+        const bool chained = nch > 1;
+        const uint32_t lq = (uint32_t)(q * 32) << 16;
+        const uint32_t tsum = tmem + (uint32_t)(2 * TN) + lq;
+        int g = 0;
         for (int lt = 0; lt < ntl; lt++) {
-            const int ab = lt & 1;
-            const bool ok = mbar_wait_bounded(&accf[ab], (lt >> 1) & 1, st, 630);
-            if (bar_or(1, 128, !ok || s_abort)) { s_abort = 1; break; }  // the same decision in every warp
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            bool abort = false;
+            uint32_t tout = tsum;
+            int ab = 0;
+            for (int c = 0; c < nch; c++, g++) {
+                ab = g & 1;
+                const bool ok = mbar_wait_bounded(&accf[ab], (g >> 1) & 1, st, 630);
+                if (bar_or(1, 128, !ok || s_abort)) { abort = true; break; }  // the same decision in every warp
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t tacc = tmem + (uint32_t)(ab * TN) + lq;
+                if (!chained) {  // released after the write-out below
+                    tout = tacc;
+                    g++;
+                    break;
+                }
+#pragma unroll 1
+                for (int cb = 0; cb < TN; cb += 32) {
+                    uint32_t v[32], w[32];
+                    tmem_ld32(tacc + (uint32_t)cb, v);
+                    if (c > 0) {
+                        tmem_ld32(tsum + (uint32_t)cb, w);
+#pragma unroll
+                        for (int k = 0; k < 32; k++) v[k] = __float_as_uint(__uint_as_float(v[k]) + __uint_as_float(w[k]));
+                    }
+                    tmem_st32(tsum + (uint32_t)cb, v);
+                }
+                // the accumulator is read out: the MMAs of chain g + 2 may use it
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                bar_or(1, 128, false);
+                if (ew == 0 && lane == 0) mbar_arrive(&acce[ab]);
+            }
+            if (abort) { s_abort = 1; break; }
             const int t = blockIdx.x + lt * gridDim.x, mt = t / NTt, nt = t % NTt;
             const int m0 = mt * TM, n0 = nt * TN;
             const int nrows = min(TM, M - m0), ncols = min(TN, N - n0);
-            const uint32_t taddr = tmem + (uint32_t)(ab * TN) + ((uint32_t)(q * 32) << 16);
-            bool abort = false;
+#pragma unroll
             for (int h = 0; h < 2; h++) {
                 float *Ch = Cbuf + h * TM * CH;
                 if (use_tm) {
@@ -611,7 +671,7 @@ __global__ void __launch_bounds__(PT_THREADS, 1)
 #pragma unroll 1
                 for (int c0 = h * CH; c0 < (h + 1) * CH; c0 += 32) {
                     uint32_t v[32];
-                    tmem_ld32(taddr + (uint32_t)c0, v);
+                    tmem_ld32(tout + (uint32_t)c0, v);
 #pragma unroll
                     for (int k = 0; k < 32; k++) sb[lane][k] = __uint_as_float(v[k]);
                     __syncwarp();
@@ -631,16 +691,16 @@ __global__ void __launch_bounds__(PT_THREADS, 1)
                         for (int rr = 0; rr < 32; rr++) {
                             const int rl = q * 32 + rr;
                             if (rl >= nrows) break;
-                            float *c = C + (long)(m0 + rl) * ldc + n0 + cl;
+                            float *cp = C + (long)(m0 + rl) * ldc + n0 + cl;
                             float x = alpha * sb[rr][lane];
-                            if (beta != 0.f) x = fmaf(beta, *c, x);
-                            *c = x;
+                            if (beta != 0.f) x = fmaf(beta, *cp, x);
+                            *cp = x;
                         }
                     }
                     __syncwarp();
                 }
-                if (h == 1) {
-                    // the accumulator is read out: the MMAs of tile lt+2 may use it
+                if (h == 1 && !chained) {
+                    // the accumulator is read out: the MMAs of chain g + 1 may use it
                     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                     bar_or(1, 128, false);
                     if (ew == 0 && lane == 0) mbar_arrive(&acce[ab]);
@@ -666,7 +726,7 @@ __global__ void __launch_bounds__(PT_THREADS, 1)
     if (warp == 0) {
         __syncwarp();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TN) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(4 * TN) : "memory");
     }
 }
 

@@ -90,9 +90,10 @@ def test_tensor_core_product_is_deterministic():
     assert torch.equal(outs[0], outs[1])
 
 
-@pytest.mark.parametrize("M,N,K", [(2048, 2048, 64), (1000, 1100, 64), (517, 517, 517)])
+@pytest.mark.parametrize("M,N,K", [(2048, 2048, 64), (1000, 1100, 64), (600, 700, 128)])
 def test_persistent_and_per_tile_kernels_agree_bitwise(M, N, K):
-    # same products, same accumulation order within a tile: identical bits
+    # k <= 4 images is one accumulation chain in both kernels: same products,
+    # same accumulation order within a tile, identical bits
     import torch
     g = torch.Generator().manual_seed(M + N + K)
     A = torch.randn(M, K, generator=g).cuda()
@@ -104,3 +105,28 @@ def test_persistent_and_per_tile_kernels_agree_bitwise(M, N, K):
         run_gemm(A, B, C, -1.0, 1.0, mode)
         outs.append(C.cpu())
     assert torch.equal(outs[0], outs[1])
+
+
+def test_persistent_kernel_sums_long_k_in_chains():
+    # 2048 x 2048 (256 tiles: no split-K, the persistent kernel), k = 4096.
+    # The tensor cores round every accumulation into TMEM toward zero; one
+    # chain over the whole k range (the one-tile kernel) carries that bias
+    # through 1536 MMAs, the persistent kernel folds chains of 4 images into
+    # FP32 sums with round-to-nearest.  Its error stays within 1e-6 of the
+    # |A||B| scale and well below the single chain's.
+    import torch
+    M = N = 2048
+    K = 4096
+    g = torch.Generator().manual_seed(77)
+    A64 = torch.randn(M, K, generator=g, dtype=torch.float64).float().double()
+    B64 = torch.randn(K, N, generator=g, dtype=torch.float64).float().double()
+    ref = A64 @ B64
+    scale = (A64.abs() @ B64.abs()).max().item()
+    err = {}
+    for mode in (1, 2):
+        C = torch.zeros(M, N, device="cuda")
+        run_gemm(A64.float().cuda(), B64.float().cuda(), C, 1.0, 0.0, mode)
+        d = C.double().cpu() - ref
+        err[mode] = (d.abs().max().item(), d.pow(2).mean().sqrt().item())
+    assert err[1][0] <= 1e-6 * scale, (err, scale)
+    assert err[1][1] <= 0.25 * err[2][1], err
