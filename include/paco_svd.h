@@ -81,9 +81,12 @@ int paco_tune_qr(int M, int N, int mode);
  * 3 last columns kept off the cluster kernel (0/1), 4 reflectors per
  * compact-WY block when U and V are formed (64 or 128; 0 = 128), 5 columns per
  * QR block (32 or 64; 0 = 64), 6 matrices per lockstep group of
- * paco_svd_multi (1..8; 0 = 4), 7 the QR-first mode of paco_tune_qr.  value
- * -1 queries.  Returns the value stored or queried, -1 for an invalid
- * argument.  paco_autotune times fields 0-5 (and 7) for one shape;
+ * paco_svd_multi (1..8; 0 = 4), 7 the QR-first mode of paco_tune_qr, 8 the
+ * two-stage reduction (dense -> band -> bidiagonal by bulge chasing) with
+ * band width 32 or 64, 0 off (the default; used for N >= 1024 when its
+ * chasing kernel holds the band, and then before QR-first).  value -1
+ * queries.  Returns the value stored or queried, -1 for an invalid
+ * argument.  paco_autotune times fields 0-5, 7 and 8 for one shape;
  * paco_autotune_multi times field 6 (2, 4, 8) on `count` synthetic matrices
  * of the shape, then for tall shapes the other QR-first choice with that
  * group size (out as paco_autotune's, out[0] = the group size chosen).

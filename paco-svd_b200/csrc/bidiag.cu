@@ -560,6 +560,29 @@ cudaError_t apply_block_reflector_ex(const BdWs &w, float *Q, long ldq, long ro,
                     w.tcs_floats, w.st, s);
 }
 
+cudaError_t apply_block_reflector_right(const BdWs &w, float *X, long ldx, long ro, int Lr, long co, int Lc, int nbp,
+                                        const float *tau, cudaStream_t s)
+{
+    const int gsplits = (int)std::max(1L, std::min({(long)ceil_div(Lc, 64), 64L, (long)SPLITS * ldx / NBF}));
+    cudaError_t err = gemm_run(nbp, nbp, Lc, 1.f, gop(w.Vp, 1, NBF), gop(w.Vp, NBF, 1), 0.f, w.gram, NBF, gsplits,
+                               w.gscr, s);
+    if (err) return err;
+    paco_count_launch(), bd_build_t<<<NBF / 8, 256, (size_t)NBF * NBF * sizeof(float), s>>>(w.gram, nbp, tau, w.T);
+    float *Xs = X + ro * ldx + co;
+    // G1 = X_sub Vp  (Lr x nbp, k = Lc)
+    const int splits = std::max(1, std::min(SPLITS, ceil_div(Lc, 512)));
+    err = gemm_any(Lr, nbp, Lc, 1.f, gop(Xs, ldx, 1), gop(w.Vp, NBF, 1), 0.f, w.G1, nbp, splits, w.gscr, w.tcs,
+                   w.tcs_floats, w.st, s);
+    if (err) return err;
+    // G2 = G1 T  (Lr x nbp)
+    err = gemm_any(Lr, nbp, nbp, 1.f, gop(w.G1, nbp, 1), gop(w.T, NBF, 1), 0.f, w.G2, nbp, 1, nullptr, w.tcs,
+                   w.tcs_floats, w.st, s);
+    if (err) return err;
+    // X_sub -= G2 Vp^T
+    return gemm_any(Lr, Lc, nbp, -1.f, gop(w.G2, nbp, 1), gop(w.Vp, 1, NBF), 1.f, Xs, ldx, 1, nullptr, w.tcs,
+                    w.tcs_floats, w.st, s);
+}
+
 // Q_sub <- (I - Vp T Vp^T) Q_sub for Q_sub = Q[off:off+Lp, off:off+Lp] (ld ldq)
 static cudaError_t apply_block_reflector(const BdWs &w, float *Q, long ldq, long off, int Lp, int nbp,
                                          const float *tau, cudaStream_t s)

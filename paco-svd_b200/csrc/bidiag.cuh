@@ -185,6 +185,10 @@ size_t bd_workspace_bytes(int M, int N);
 // transT, for the nbp reflectors in w.Vp (T built from their Gram matrix).
 cudaError_t apply_block_reflector_ex(const BdWs &w, float *Q, long ldq, long ro, int Lr, long co, int Lc, int nbp,
                                      const float *tau, bool transT, cudaStream_t s);
+// X[ro:ro+Lr, co:co+Lc] <- X[...] (I - Vp T Vp^T), the nbp reflectors in w.Vp
+// (rows of Vp = the Lc columns), T their forward triangular factor.
+cudaError_t apply_block_reflector_right(const BdWs &w, float *X, long ldx, long ro, int Lr, long co, int Lc, int nbp,
+                                        const float *tau, cudaStream_t s);
 // w.Vp-style explicit block of the column reflectors [p0, p0 + nbp) stored in W.
 void bd_column_vectors(const float *W, long ldw, int p0, int nbp, int Lp, float *Vp, cudaStream_t s);
 // W (M x ldw, zero padded) <- a (M x N); non-finite entries are reported and replaced by 0.

@@ -8,6 +8,7 @@
 #include "bdc.cuh"
 #include "bidiag.cuh"
 #include "qr.cuh"
+#include "twostage.cuh"
 
 namespace {
 
@@ -79,6 +80,35 @@ QrLayout qr_layout(int M, int N)
 // Shapes that may take the QR-first path (their workspace size covers it).
 bool qr_possible(int M, int N) { return M > N && N >= 1024; }
 
+// Two-stage path: the one-stage layout of (M, N) (its stage-1 workspace holds
+// the band reduction, and is then reused by divide and conquer), the band and
+// the chasing reflectors of both sides, sized for the widest band (64).
+struct TsLayout {
+    SvdLayout L;
+    size_t band, rl, rr, total;
+};
+
+TsLayout ts_layout(int M, int N)
+{
+    TsLayout T;
+    T.L = svd_layout(M, N);
+    size_t off = T.L.total;
+    auto take = [&](size_t bytes) {
+        off = (off + 255) & ~(size_t)255;
+        size_t p = off;
+        off += bytes;
+        return p;
+    };
+    T.band = take(sizeof(float) * ts::band_floats(N, 64));
+    T.rl = take(sizeof(float) * ts::refl_floats(N, 64));
+    T.rr = take(sizeof(float) * ts::refl_floats(N, 64));
+    T.total = (off + 255) & ~(size_t)255;
+    return T;
+}
+
+// Shapes that may take the two-stage path (their workspace size covers it).
+bool ts_possible(int M, int N) { return M >= N && N >= 1024; }
+
 } // namespace
 
 static unsigned long long g_launches = 0;
@@ -110,13 +140,14 @@ struct TuneEntry {
 std::mutex g_tune_mu;
 std::vector<TuneEntry> g_tune;
 unsigned g_tune_gen = 0;
-const PacoTune kTuneDefault = {1, bd::RMIN_PER_BLOCK, 1, 0, 0, 0, 0};
+const PacoTune kTuneDefault = {1, bd::RMIN_PER_BLOCK, 1, 0, 0, 0, 0, 0};
 
 bool tune_valid(const PacoTune &t)
 {
     return (t.persistent == 0 || t.persistent == 1) && (t.tc == 0 || t.tc == 1) && t.rows_per_cta >= 4 &&
            t.rows_per_cta <= 256 && (t.no_tail == 0 || t.no_tail == 1) && (t.wy == 0 || t.wy == 64 || t.wy == 128) &&
-           (t.qb == 0 || t.qb == 32 || t.qb == 64) && t.mk >= 0 && t.mk <= PK_KMAX;
+           (t.qb == 0 || t.qb == 32 || t.qb == 64) && t.mk >= 0 && t.mk <= PK_KMAX &&
+           (t.ts == 0 || t.ts == 32 || t.ts == 64);
 }
 
 void tune_store(int M, int N, const PacoTune &cfg)
@@ -164,6 +195,15 @@ PacoTune paco_tune_for(int M, int N)
     for (const TuneEntry &e : g_tune)
         if (e.M == M && e.N == N) return e.cfg;
     return kTuneDefault;
+}
+
+// Two-stage reduction chosen for (M, N): the tuning entry's band width (0
+// off, the default), a shape its workspace covers, and a band the chasing
+// kernel holds.
+static int ts_chosen(int M, int N)
+{
+    const int b = paco_tune_for(M, N).ts;
+    return (b && ts_possible(M, N) && ts_fits(N, b)) ? b : 0;
 }
 
 // fills A with reproducible values uniform on [-1, 1) (a hash of the index)
@@ -393,8 +433,10 @@ int paco_sync_status(void *workspace, void *stream, int *info)
 size_t paco_svd_workspace_size(int M, int N)
 {
     if (!shape_ok(M, N)) return 0;
-    const size_t one = svd_layout(M, N).total;
-    return qr_possible(M, N) ? std::max(one, qr_layout(M, N).total) : one;
+    size_t one = svd_layout(M, N).total;
+    if (qr_possible(M, N)) one = std::max(one, qr_layout(M, N).total);
+    if (ts_possible(M, N)) one = std::max(one, ts_layout(M, N).total);
+    return one;
 }
 
 int paco_tune_qr(int M, int N, int mode)
@@ -443,6 +485,38 @@ static int svd_direct_qr(int M, int N, const float *A, float *U, float *Vt, floa
     return qr_form_u(wq, M, N, tau, UR, U, s, thin ? N : M, tn.wy);
 }
 
+// Two-stage SVD: A -> band (bandwidth b) -> bidiagonal by bulge chasing,
+// U = Q1 (formed) times the left chasing reflectors, Vt = the right chasing
+// reflectors times P1^T, then divide and conquer updates both.  A is
+// destroyed (scratch), as on the one-stage path.
+static int svd_direct_ts(int M, int N, float *A, float *U, float *Vt, float *sigma, char *b, const TsLayout &T,
+                         int bw, void *stream, bool thin)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    const SvdLayout &L = T.L;
+    float *e = (float *)(b + L.e), *tq = (float *)(b + L.tauq), *tp = (float *)(b + L.taup);
+    float *rl = (float *)(b + T.rl), *rr = (float *)(b + T.rr);
+    BdWs w;
+    bd_carve(b + L.ws, M, N, &w);
+    DevStatus *st = w.st;
+    const PacoTune tn = paco_tune_for(M, N);
+    if (!tn.tc) w.tcs = nullptr;
+    bd_init_attrs();
+    paco_count_launch(), dev_status_begin<<<1, 64, 0, s>>>(st, 1);
+    bd_copy_in_launch(A, w.W, M, N, w.ldw, st, s);
+    int rc = ts_band_reduce(w, M, N, bw, tq, tp, s);
+    if (!rc) rc = ts_chase(w, N, bw, (float *)(b + T.band), rl, rr, sigma, e, s);
+    const long lu = thin ? N : M;
+    if (!rc) rc = qr_form_u(w, M, N, tq, nullptr, U, s, (int)lu, tn.wy);
+    if (!rc) rc = ts_form_p1t(w, N, bw, tp, A, Vt, s);
+    if (!rc) rc = ts_apply(U, lu, N, M, 1, bw, rl, st, s);
+    if (!rc) rc = ts_apply(Vt, N, N, N, 0, bw, rr, st, s);
+    if (rc) return rc;
+    paco_count_launch(), dev_status_begin<<<1, 64, 0, s>>>(st, 2);
+    return bdc_run(M, N, A, U, Vt, sigma, e, (float *)(b + L.qt), (float *)(b + L.wt), (uint32_t *)(b + L.idx),
+                   b + L.ws, nullptr, s, lu);
+}
+
 // One-stage SVD with the thin U (M x N): stage 1 forms H_0 ... H_{N-1} [I; 0]
 // only, and stage 2 updates those N columns.
 static int svd_direct_thin(int M, int N, float *A, float *U, float *Vt, float *sigma, char *b, const SvdLayout &L,
@@ -488,6 +562,33 @@ extern "C" int paco_debug_qr_r(int M, int N, const float *A, float *R, float *Qo
     return paco_sync_status(ws, stream, nullptr);
 }
 
+// Test hook (not part of the public header): stages 1 and 2 of the two-stage
+// reduction of A (M x N, N >= 1024) with band width b: band (N x 3b, row i =
+// columns i - b .. i + 2b - 1 of the band matrix; may be null) and the
+// bidiagonal d (N), e (N - 1).  ws holds paco_svd_workspace_size(M, N) bytes.
+// Synchronous.
+extern "C" int paco_debug_ts(int M, int N, int b, const float *A, float *band, float *d, float *e, void *ws,
+                             size_t ws_bytes, void *stream)
+{
+    if (!shape_ok(M, N) || !ts_possible(M, N) || !ts_fits(N, b) || !A || !d || !e || !ws ||
+        ws_bytes < paco_svd_workspace_size(M, N))
+        return PACO_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    char *p = (char *)ws;
+    const TsLayout T = ts_layout(M, N);
+    BdWs w;
+    bd_carve(p + T.L.ws, M, N, &w);
+    bd_init_attrs();
+    cudaMemsetAsync(w.st, 0, sizeof(DevStatus), s);
+    bd_copy_in_launch(A, w.W, M, N, w.ldw, w.st, s);
+    int rc = ts_band_reduce(w, M, N, b, (float *)(p + T.L.tauq), (float *)(p + T.L.taup), s);
+    float *bandp = (float *)(p + T.band);
+    if (!rc) rc = ts_chase(w, N, b, bandp, (float *)(p + T.rl), (float *)(p + T.rr), d, e, s);
+    if (rc) return rc;
+    if (band) cudaMemcpyAsync(band, bandp, sizeof(float) * ts::band_floats(N, b), cudaMemcpyDeviceToDevice, s);
+    return paco_sync_status(p + T.L.ws, stream, nullptr);
+}
+
 static int svd_direct(int M, int N, float *A, float *U, float *Vt, float *sigma, char *b, const SvdLayout &L,
                       void *stream)
 {
@@ -498,12 +599,14 @@ static int svd_direct(int M, int N, float *A, float *U, float *Vt, float *sigma,
                   b + L.ws, nullptr, stream);
 }
 
-// The single-matrix SVD in the configuration of (M, N): QR-first for tall
-// matrices when chosen, otherwise the one-stage pipeline.  b holds
+// The single-matrix SVD in the configuration of (M, N): the two-stage
+// reduction when its tuning entry asks for it, QR-first for tall matrices when
+// chosen, otherwise the one-stage pipeline.  b holds
 // paco_svd_workspace_size(M, N) bytes.
 static int svd_any(int M, int N, float *A, float *U, float *Vt, float *sigma, char *b, void *stream,
                    bool thin = false)
 {
+    if (const int bw = ts_chosen(M, N)) return svd_direct_ts(M, N, A, U, Vt, sigma, b, ts_layout(M, N), bw, stream, thin);
     if (qr_chosen(M, N)) return svd_direct_qr(M, N, A, U, Vt, sigma, b, qr_layout(M, N), stream, thin);
     if (thin) return svd_direct_thin(M, N, A, U, Vt, sigma, b, svd_layout(M, N), stream);
     return svd_direct(M, N, A, U, Vt, sigma, b, svd_layout(M, N), stream);
@@ -876,10 +979,10 @@ int paco_tune_set(int M, int N, const int cfg[4])
 
 int paco_tune_param(int M, int N, int which, int value)
 {
-    if (!shape_ok(M, N) || which < 0 || which > 7) return -1;
+    if (!shape_ok(M, N) || which < 0 || which > 8) return -1;
     if (which == 7) return paco_tune_qr(M, N, value);
     PacoTune t = paco_tune_for(M, N);
-    int *f[7] = {&t.persistent, &t.rows_per_cta, &t.tc, &t.no_tail, &t.wy, &t.qb, &t.mk};
+    int *f[9] = {&t.persistent, &t.rows_per_cta, &t.tc, &t.no_tail, &t.wy, &t.qb, &t.mk, nullptr, &t.ts};
     if (value == -1) return *f[which];
     *f[which] = value;
     if (!tune_valid(t)) return -1;
@@ -997,7 +1100,9 @@ int paco_autotune(int M, int N, void *stream, double out[4])
     // candidates: the defaults first, then fewer / more rows per CTA, the
     // SIMT engine for the large products, the two-kernel row/column passes,
     // the last columns on the panel kernel; for tall shapes the best of them
-    // is then also timed with the QR-first choice flipped
+    // is then also timed with the QR-first choice flipped, then with 64-
+    // reflector WY blocks, the two-stage reduction (bands 32 and 64) and
+    // 32-column QR blocks
     PacoTune cands[] = {{1, bd::RMIN_PER_BLOCK, 1, 0}, {1, 8, 1, 0}, {1, 32, 1, 0}, {1, bd::RMIN_PER_BLOCK, 0, 0},
                         {0, bd::RMIN_PER_BLOCK, 1, 0}, {1, bd::RMIN_PER_BLOCK, 1, 1}};
     const int mk0 = paco_tune_for(M, N).mk;  // the multi-matrix group size is tuned separately
@@ -1052,7 +1157,17 @@ int paco_autotune(int M, int N, void *stream, double out[4])
             if (!rc && tw < best) { best = tw; t = c; }
             else tune_store(M, N, t);
         }
-        if (!rc && qr_chosen(M, N)) {
+        // the two-stage reduction, band 32 and 64
+        for (int bwid : {32, 64}) {
+            if (rc || !ts_possible(M, N) || !ts_fits(N, bwid)) continue;
+            PacoTune c = t;
+            c.ts = bwid;
+            tune_store(M, N, c);
+            const float tt = time_one();
+            if (!rc && tt < best) { best = tt; t = c; }
+            else tune_store(M, N, t);
+        }
+        if (!rc && !t.ts && qr_chosen(M, N)) {
             PacoTune c = t;
             c.qb = 32;
             tune_store(M, N, c);

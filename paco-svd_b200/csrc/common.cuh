@@ -91,6 +91,7 @@ int paco_device();
 struct PacoTune {
     int persistent, rows_per_cta, tc, no_tail;
     int wy, qb, mk;
+    int ts;  // two-stage reduction: band width 32 or 64, 0 off
 };
 PacoTune paco_tune_for(int M, int N);
 

@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(QT, 1) qr_block_k(QrArgs a)
             for (int w = 0; w < QW; w++) t += wpart[w][tid];
             for (int c = 0; c < CS; c++) q_st(q_dsmem(&s_w_all[rank][tid], c), t);
         }
-        if (tid == 0 && rank == 0) a.tau[pr] = tau;
+        if (tid == 0 && rank == 0) a.tau[j] = tau;  // tau of the block's column j
         q_cluster_sync();  // every CTA's partial v^T A is in place
         if (kn > 0) {
             if (tid < kn) {
@@ -273,36 +273,52 @@ bool qr_fits(int M, int N)
     return cfg.cs > 0 && N >= 1 && M >= N && qr_smem_bytes(M, cfg.cs) <= (size_t)cfg.max_smem;
 }
 
+// QR of the block of nb <= QB columns at q0 of W, rows [q0, M), in place
+// (R on and above the diagonal, the reflectors below); tau[0, nb) its scalars.
+int qr_panel(float *W, long ldw, int M, int q0, int nb, float *tau, cudaStream_t s, bool small)
+{
+    const QrCfg cfg = qr_cfg();
+    const int rows = M - q0;
+    if (cfg.cs <= 0 || nb < 1 || nb > QB || rows < 1 || qr_smem_bytes(rows, cfg.cs) > (size_t)cfg.max_smem)
+        return PACO_ERR_UNSUPPORTED;
+    // small: the smallest cluster (down to one CTA) that keeps at most 256
+    // rows per CTA; fewer CTAs make the two cluster barriers per column cheaper
+    int cs = cfg.cs;
+    while (small && cs > 1 && rows <= (cs / 2) * 256) cs /= 2;
+    QrArgs a;
+    a.W = W; a.ldw = ldw; a.M = M; a.q0 = q0; a.nb = nb;
+    a.rpc = (rows + cs - 1) / cs;
+    a.tau = tau;
+    cudaLaunchConfig_t lc = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    lc.gridDim = dim3(cs);
+    lc.blockDim = dim3(QT);
+    lc.dynamicSmemBytes = qr_smem_bytes(rows, cs);
+    lc.stream = s;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    paco_count_launch();
+    if (cudaLaunchKernelEx(&lc, qr_block_k, a) != cudaSuccess) {
+        cudaGetLastError();
+        return PACO_ERR_CUDA;
+    }
+    return PACO_OK;
+}
+
 // The columns of W (M x ldw, already holding A) become R (upper triangle) and
 // the Householder vectors (below the diagonal); tau[N] receives the scalars.
 int qr_factor(const BdWs &w, int M, int N, float *tau, cudaStream_t s, int qb)
 {
-    const QrCfg cfg = qr_cfg();
     if (!qr_fits(M, N)) return PACO_ERR_UNSUPPORTED;
     qb = (qb == 32) ? 32 : QB;
     for (int q0 = 0; q0 < N; q0 += qb) {
         const int nb = std::min(qb, N - q0), rows = M - q0;
-        QrArgs a;
-        a.W = w.W; a.ldw = w.ldw; a.M = M; a.q0 = q0; a.nb = nb;
-        a.rpc = (rows + cfg.cs - 1) / cfg.cs;
-        a.tau = tau;
-        cudaLaunchConfig_t lc = {};
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeClusterDimension;
-        at[0].val.clusterDim.x = cfg.cs;
-        at[0].val.clusterDim.y = 1;
-        at[0].val.clusterDim.z = 1;
-        lc.gridDim = dim3(cfg.cs);
-        lc.blockDim = dim3(QT);
-        lc.dynamicSmemBytes = qr_smem_bytes(rows, cfg.cs);
-        lc.stream = s;
-        lc.attrs = at;
-        lc.numAttrs = 1;
-        paco_count_launch();
-        if (cudaLaunchKernelEx(&lc, qr_block_k, a) != cudaSuccess) {
-            cudaGetLastError();
-            return PACO_ERR_CUDA;
-        }
+        const int rc = qr_panel(w.W, w.ldw, M, q0, nb, tau + q0, s);
+        if (rc) return rc;
         const int q1 = q0 + nb;
         if (q1 < N) {
             bd_column_vectors(w.W, w.ldw, q0, nb, rows, w.Vp, s);

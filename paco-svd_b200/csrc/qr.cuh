@@ -16,6 +16,11 @@ bool qr_fits(int M, int N);
 // scalars.  Enqueued on s.
 // qb: columns per block, 64 (QB, also for 0) or 32.
 int qr_factor(const BdWs &w, int M, int N, float *tau, cudaStream_t s, int qb = 0);
+// QR of one block of nb <= QB columns at column q0 of W (ld ldw), rows
+// [q0, M): R on and above the diagonal, the reflectors below it, their
+// scalars in tau[0, nb).  PACO_ERR_UNSUPPORTED when the rows do not fit.
+// small: a cluster of fewer CTAs (down to one) for panels of few rows.
+int qr_panel(float *W, long ldw, int M, int q0, int nb, float *tau, cudaStream_t s, bool small = false);
 // R (N x N, ld N) <- the upper triangle of W[0:N, 0:N].
 void qr_extract_r_launch(const BdWs &w, int N, float *R, cudaStream_t s);
 // U (M x uc, ld uc) <- the first uc columns of Q blockdiag(UR, I) with Q from

@@ -1,0 +1,498 @@
+// Two-stage reduction to bidiagonal form.  The reference names it as future
+// work ("use aic to apply householder transformation", README.md:23); its
+// one-stage kernel is upper_bidiagonalization.cpp.
+//
+// Stage 1, dense -> upper band of bandwidth b (ts_band_reduce): for each
+// panel of b columns, the QR of the column panel (the QR block kernel of
+// qr.cu on one thread-block cluster) and its block reflector applied to the
+// trailing columns, then the LQ of the row panel W[k:k+b, k+b:N] (the panel
+// transposed, factored by the same kernel, transposed back) and its block
+// reflector applied from the right to the rows below.  Every step is a
+// panel factorization or a block-reflector product; no column-by-column
+// pass streams the trailing matrix.
+//
+// Stage 2, band -> bidiagonal by bulge chasing (ts_chase_k): sweep s
+// annihilates row s beyond the superdiagonal with a right reflector on
+// columns [s+1, s+b], which fills the b x b block below the diagonal; a left
+// reflector on rows [s+1, s+b] clears its first column and fills row s+1
+// beyond the band; step j of the sweep repeats this b columns further on
+// (right reflector on columns c0 = s+1+jb .. c0+b-1 from row c0-b, left
+// reflector on rows c0 .. c0+b-1 from column c0), until the matrix ends.
+// Task (s, j) touches rows [c0-b, c0+b) only, and needs (s, j-1) and
+// (s-1, j+2) done, so super-step t runs task j = t - 3s of every sweep s at
+// once: the concurrent tasks are 3b - 1 rows apart and never share a row.
+// The band lives in the shared memory of one 16-CTA cluster (contiguous
+// row ranges, row r stored at columns r - b .. r + 2b - 1), each task runs
+// on one warp of the CTA owning its row c0 through distributed shared
+// memory, and the super-steps are separated by cluster barriers.
+//
+// Back-transformation: U = Q1 blockdiag(Q2 U_B, I), V = P1 P2 V_B with Q1, P1
+// from stage 1 (formed explicitly by the compact-WY products of qr.cu) and
+// Q2, P2 the products of the chasing reflectors.  ts_apply_k applies the
+// chasing reflectors of every sweep, in sweep order, to U[:, :N] from the
+// right and to Vt from the left; it splits the matrix into chunks of 8 (or
+// 4) independent columns (rows of U) held in shared memory, and stages the
+// reflectors of each sweep by cp.async while the previous sweep is applied.
+#include <cooperative_groups.h>
+
+#include "qr.cuh"
+#include "tma.cuh"
+#include "twostage.cuh"
+
+namespace {
+namespace cg = cooperative_groups;
+
+constexpr int CT = 256, CWARPS = CT / 32;  // chasing kernel: threads, warps per CTA
+constexpr int AT = 256;                    // back-transformation kernel threads
+
+// dst[c * ldd + r] = src[r * lds + c] for r < rows, c < cols
+__global__ void ts_transpose(const float *__restrict__ src, long lds, int rows, int cols, float *__restrict__ dst,
+                             long ldd)
+{
+    __shared__ float tile[32][33];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+        const int r = r0 + y, c = c0 + threadIdx.x;
+        if (r < rows && c < cols) tile[y][threadIdx.x] = src[(long)r * lds + c];
+    }
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+        const int c = c0 + y, r = r0 + threadIdx.x;
+        if (r < rows && c < cols) dst[(long)c * ldd + r] = tile[threadIdx.x][y];
+    }
+}
+
+void transpose_launch(const float *src, long lds, int rows, int cols, float *dst, long ldd, cudaStream_t s)
+{
+    if (rows <= 0 || cols <= 0) return;
+    paco_count_launch(), ts_transpose<<<dim3(ceil_div(cols, 32), ceil_div(rows, 32)), dim3(32, 8), 0, s>>>(
+                             src, lds, rows, cols, dst, ldd);
+}
+
+// band[i * 3b + o] <- B[i, i + o - b] for the band (o - b in [0, b]), 0 elsewhere
+__global__ void ts_band_from_w(const float *__restrict__ W, long ldw, int N, int b, float *__restrict__ band)
+{
+    const long total = (long)N * 3 * b;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / (3 * b)), o = (int)(t % (3 * b));
+        const int c = i + o - b;
+        band[t] = (o >= b && o <= 2 * b && c < N) ? W[(long)i * ldw + c] : 0.f;
+    }
+}
+
+// Vt <- blockdiag(I_b, F^T), F ((N - b) x (N - b), ld N - b)
+__global__ void ts_p1t(const float *__restrict__ F, int N, int b, float *__restrict__ Vt)
+{
+    const long total = (long)N * N;
+    const int n = N - b;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / N), j = (int)(t % N);
+        Vt[t] = (i < b || j < b) ? (i == j ? 1.f : 0.f) : F[(long)(j - b) * n + (i - b)];
+    }
+}
+
+struct ChaseArgs {
+    const float *band;  // N x 3b (global copy of B)
+    float *refl_l, *refl_r, *d, *e;
+    int N, rpc, jmax, T;
+};
+
+__device__ __forceinline__ void cluster_fence() { asm volatile("fence.acq_rel.cluster;" ::: "memory"); }
+
+// One chasing task (sweep s, step j) on one warp.  rows_of[o] is the generic
+// address of CTA o's band rows; element (r, c) of the band is entry
+// c - r + B of row r's storage.
+template <int B>
+__device__ void chase_task(const ChaseArgs &a, int s, int j, float *vb, float **rowp, float *const *rows_of,
+                           int rpc)
+{
+    constexpr int NL = B / 32, OFF = B, LDB = 3 * B;
+    const int lane = threadIdx.x & 31, N = a.N;
+    // address of element (r, c)
+    auto at = [&](int r, int c) -> float * {
+        const int o = r / rpc;
+        return rows_of[o] + (long)(r - o * rpc) * LDB + (c - r + OFF);
+    };
+    const int c0 = s + 1 + j * B;
+    const int c1 = min(c0 + B - 1, N - 1), L = c1 - c0 + 1;
+    const int rp = (j == 0) ? s : c0 - B;
+    // ---- right reflector on columns [c0, c1] from row rp
+    float *prow = at(rp, c0);  // prow[l] = (rp, c0 + l)
+    float x[NL];
+#pragma unroll
+    for (int k = 0; k < NL; k++) {
+        const int l = lane + 32 * k;
+        x[k] = (l < L) ? prow[l] : 0.f;
+    }
+    float sg = 0.f;
+#pragma unroll
+    for (int k = 0; k < NL; k++)
+        if (lane + 32 * k >= 1) sg += x[k] * x[k];
+    sg = warp_sum(sg);
+    const float x0 = __shfl_sync(0xffffffffu, x[0], 0);
+    float beta, tau, v0;
+    make_reflector(x0, sg, L, &beta, &tau, &v0);
+    float inv = 1.f / v0;
+    float *rr = a.refl_r + ((long)s * a.jmax + j) * B;
+#pragma unroll
+    for (int k = 0; k < NL; k++) {
+        const int l = lane + 32 * k;
+        const float v = (l == 0) ? 1.f : (l < L ? x[k] * inv : 0.f);
+        vb[l] = v;
+        rr[l] = (l == 0) ? tau : v;
+        if (l < L) prow[l] = (l == 0) ? beta : 0.f;
+    }
+    cluster_fence();
+    __syncwarp();
+    if (tau != 0.f) {
+        for (int r = rp + 1 + lane; r <= c1; r += 32) {
+            float *p = at(r, c0);
+            float w = 0.f;
+#pragma unroll 8
+            for (int l = 0; l < L; l++) w += p[l] * vb[l];
+            w *= tau;
+#pragma unroll 8
+            for (int l = 0; l < L; l++) p[l] -= w * vb[l];
+        }
+    }
+    // ---- left reflector on rows [c0, c1] from column c0
+#pragma unroll
+    for (int k = 0; k < NL; k++) {
+        const int l = lane + 32 * k;
+        if (l < L) rowp[l] = at(c0 + l, c0);  // rowp[l][c - c0] = (c0 + l, c)
+    }
+    cluster_fence();
+    __syncwarp();
+    float y[NL];
+#pragma unroll
+    for (int k = 0; k < NL; k++) {
+        const int l = lane + 32 * k;
+        y[k] = (l < L) ? rowp[l][0] : 0.f;
+    }
+    sg = 0.f;
+#pragma unroll
+    for (int k = 0; k < NL; k++)
+        if (lane + 32 * k >= 1) sg += y[k] * y[k];
+    sg = warp_sum(sg);
+    const float y0 = __shfl_sync(0xffffffffu, y[0], 0);
+    make_reflector(y0, sg, L, &beta, &tau, &v0);
+    inv = 1.f / v0;
+    float *rl = a.refl_l + ((long)s * a.jmax + j) * B;
+    __syncwarp();  // every lane is done with vb
+#pragma unroll
+    for (int k = 0; k < NL; k++) {
+        const int l = lane + 32 * k;
+        const float v = (l == 0) ? 1.f : (l < L ? y[k] * inv : 0.f);
+        vb[l] = v;
+        rl[l] = (l == 0) ? tau : v;
+        if (l < L) rowp[l][0] = (l == 0) ? beta : 0.f;
+    }
+    cluster_fence();
+    __syncwarp();
+    if (tau != 0.f) {
+        const int e1 = min(c0 + 2 * B - 1, N - 1);
+        for (int c = c0 + 1 + lane; c <= e1; c += 32) {
+            float w = 0.f;
+#pragma unroll 8
+            for (int l = 0; l < L; l++) w += vb[l] * rowp[l][c - c0];
+            w *= tau;
+#pragma unroll 8
+            for (int l = 0; l < L; l++) rowp[l][c - c0] -= w * vb[l];
+        }
+    }
+    cluster_fence();
+    __syncwarp();  // vb and rowp are free for the warp's next task
+}
+
+template <int B>
+__global__ void __launch_bounds__(CT, 1) ts_chase_k(ChaseArgs a)
+{
+    extern __shared__ float sb[];  // this CTA's rows of the band, 3B floats each
+    __shared__ float vbuf[CWARPS][B];
+    __shared__ float *rowp[CWARPS][B];
+    __shared__ float *rows_of[16];
+    constexpr int LDB = 3 * B;
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank(), CS = (int)cl.num_blocks();
+    const int N = a.N, rpc = a.rpc;
+    const int r0 = rank * rpc, r1 = min(N, r0 + rpc);
+    const int warp = threadIdx.x >> 5;
+    for (long t = threadIdx.x; t < (long)max(0, r1 - r0) * LDB; t += CT) sb[t] = a.band[(long)r0 * LDB + t];
+    if (threadIdx.x < CS) rows_of[threadIdx.x] = cl.map_shared_rank(sb, (int)threadIdx.x);
+    cl.sync();
+    const long den = 3L * B - 1;
+    for (int t = 0; t < a.T; t++) {
+        // sweeps whose step j = t - 3s starts at c0 = 1 + tB - s(3B - 1) in [r0, r1)
+        const long num = 1L + (long)t * B;
+        long s_hi = min((long)t / 3, (long)N - 2);
+        s_hi = (num - r0 >= 0) ? min(s_hi, (num - r0) / den) : -1;
+        const long s_lo = (num - r1 >= 0) ? (num - r1) / den + 1 : 0;
+        for (long s = s_lo + warp; s <= s_hi; s += CWARPS)
+            chase_task<B>(a, (int)s, (int)(t - 3 * s), vbuf[warp], rowp[warp], rows_of, rpc);
+        cl.sync();
+    }
+    for (int r = r0 + (int)threadIdx.x; r < r1; r += CT) {
+        a.d[r] = sb[(long)(r - r0) * LDB + B];
+        if (r < N - 1) a.e[r] = sb[(long)(r - r0) * LDB + B + 1];
+    }
+}
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+// Applies the chasing reflectors of every sweep, in sweep order, to CW
+// columns of X held in shared memory (row r at r + r/32: the rows of the
+// reflectors a warp covers at once fall into different banks).
+template <int CW>
+__global__ void __launch_bounds__(AT, 1) ts_apply_k(float *X, long ld, int N, int ncols, int trans, int b, int jmax,
+                                                   const float *__restrict__ refl)
+{
+    extern __shared__ __align__(16) float sm[];
+    const int rows_p = N + N / 32 + 1;
+    float *Xs = sm;
+    float *Rb = Xs + (long)rows_p * CW;  // two stages of jmax * b floats
+    const long rb = (long)jmax * b;
+    const int cbase = blockIdx.x * CW, ncw = min(CW, ncols - cbase);
+    auto ri = [](int r) { return r + (r >> 5); };
+    if (trans) {
+        for (long t = threadIdx.x; t < (long)ncw * N; t += AT) {
+            const int c = (int)(t / N), r = (int)(t % N);
+            Xs[ri(r) * CW + c] = X[(long)(cbase + c) * ld + r];
+        }
+    } else {
+        for (long t = threadIdx.x; t < (long)N * CW; t += AT) {
+            const int r = (int)(t / CW), c = (int)(t % CW);
+            if (c < ncw) Xs[ri(r) * CW + c] = X[(long)r * ld + cbase + c];
+        }
+    }
+    auto stage = [&](int s, float *dst) {
+        const int nf = ((N - 2 - s + b) / b) * b;
+        const float *src = refl + (long)s * rb;
+        for (int i = threadIdx.x * 4; i < nf; i += AT * 4) cp_async16(dst + i, src + i);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    stage(0, Rb);
+    for (int s = 0; s <= N - 2; s++) {
+        const float *R = Rb + (s & 1) * rb;
+        if (s + 1 <= N - 2)
+            stage(s + 1, Rb + ((s + 1) & 1) * rb);
+        else
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        __syncthreads();
+        const int J = (N - 2 - s + b) / b;
+        for (int p = threadIdx.x; p < J * CW; p += AT) {
+            const int j = p / CW, c = p % CW;
+            const float *v = R + j * b;
+            const float tau = v[0];
+            if (c >= ncw || tau == 0.f) continue;
+            const int c0 = s + 1 + j * b, L = min(b, N - c0);
+            float w = Xs[ri(c0) * CW + c];
+            for (int l = 1; l < L; l++) w += v[l] * Xs[ri(c0 + l) * CW + c];
+            w *= tau;
+            Xs[ri(c0) * CW + c] -= w;
+            for (int l = 1; l < L; l++) Xs[ri(c0 + l) * CW + c] -= w * v[l];
+        }
+        __syncthreads();  // the stage of sweep s is free for sweep s + 2
+    }
+    if (trans) {
+        for (long t = threadIdx.x; t < (long)ncw * N; t += AT) {
+            const int c = (int)(t / N), r = (int)(t % N);
+            X[(long)(cbase + c) * ld + r] = Xs[ri(r) * CW + c];
+        }
+    } else {
+        for (long t = threadIdx.x; t < (long)N * CW; t += AT) {
+            const int r = (int)(t / CW), c = (int)(t % CW);
+            if (c < ncw) X[(long)r * ld + cbase + c] = Xs[ri(r) * CW + c];
+        }
+    }
+}
+
+struct TsCfg {
+    int cs = 0;        // cluster size of the chasing kernel (0: unavailable)
+    int max_smem = 0;  // dynamic shared memory per CTA
+};
+
+size_t chase_smem(int N, int b, int cs) { return sizeof(float) * (size_t)((N + cs - 1) / cs) * 3 * b; }
+
+TsCfg ts_cfg_probe()
+{
+    TsCfg cfg;
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return cfg;
+    }
+    const int smem = optin - 8192;  // room for the static shared memory
+    bool ok = true;
+    for (auto f : {(const void *)ts_chase_k<32>, (const void *)ts_chase_k<64>}) {
+        ok = ok && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
+             cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess;
+    }
+    for (auto f : {(const void *)ts_apply_k<8>, (const void *)ts_apply_k<4>})
+        ok = ok && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        return cfg;
+    }
+    for (int cs : {16, 8}) {
+        cudaLaunchConfig_t lc = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = cs;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        lc.gridDim = dim3(cs);
+        lc.blockDim = dim3(CT);
+        lc.dynamicSmemBytes = smem;
+        lc.attrs = at;
+        lc.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, (const void *)ts_chase_k<64>, &lc) == cudaSuccess && n >= 1) {
+            cfg.cs = cs;
+            cfg.max_smem = smem;
+            break;
+        }
+        cudaGetLastError();
+    }
+    return cfg;
+}
+
+TsCfg g_ts_cfg[PACO_MAX_DEVICES];
+bool g_ts_done[PACO_MAX_DEVICES];
+
+TsCfg ts_cfg()
+{
+    const int dev = paco_device();
+    if (!g_ts_done[dev]) {
+        g_ts_cfg[dev] = ts_cfg_probe();
+        g_ts_done[dev] = true;
+    }
+    return g_ts_cfg[dev];
+}
+
+int apply_cw(int N) { return N <= 4608 ? 8 : 4; }
+
+size_t apply_smem(int N, int b, int cw)
+{
+    return sizeof(float) * ((size_t)(N + N / 32 + 1) * cw + 2 * (size_t)ts::jmax(N, b) * b);
+}
+
+}  // namespace
+
+void ts_init() { (void)ts_cfg(); }
+
+bool ts_fits(int N, int b)
+{
+    const TsCfg c = ts_cfg();
+    if (c.cs <= 0 || (b != 32 && b != 64) || N <= b || c.cs > 16) return false;
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return chase_smem(N, b, c.cs) <= (size_t)c.max_smem && apply_smem(N, b, apply_cw(N)) <= (size_t)optin &&
+           qr_fits(N, b);
+}
+
+int ts_band_reduce(const BdWs &w, int M, int N, int b, float *tauq, float *taup, cudaStream_t s)
+{
+    cudaMemsetAsync(taup, 0, sizeof(float) * N, s);
+    float *P = w.Vtmp;  // the transposed row panel, L x b
+    for (int k = 0; k < N; k += b) {
+        const int kb = std::min(b, N - k), k1 = k + kb;
+        int rc = qr_panel(w.W, w.ldw, M, k, kb, tauq + k, s, true);
+        if (rc) return rc;
+        if (k1 < N) {
+            bd_column_vectors(w.W, w.ldw, k, kb, M - k, w.Vp, s);
+            if (apply_block_reflector_ex(w, w.W, w.ldw, k, M - k, k1, N - k1, kb, tauq + k, true, s) != cudaSuccess)
+                return PACO_ERR_CUDA;
+        }
+        const int L = N - k - b;  // columns right of the band of the row panel
+        if (L <= 0) continue;
+        const int nr = std::min(kb, L);  // rows of the panel with a reflector
+        float *Wr = w.W + (long)k * w.ldw + k + b;
+        transpose_launch(Wr, w.ldw, kb, L, P, b, s);
+        // all kb columns of P: with L < kb the reflectors of the first L rows
+        // still apply to the panel's other rows (their own taus come out 0)
+        rc = qr_panel(P, b, L, 0, kb, taup + k, s, true);
+        if (rc) return rc;
+        transpose_launch(P, b, L, kb, Wr, w.ldw, s);
+        if (k1 < M) {
+            bd_column_vectors(P, b, 0, nr, L, w.Vp, s);
+            if (apply_block_reflector_right(w, w.W, w.ldw, k1, M - k1, k + b, L, nr, taup + k, s) != cudaSuccess)
+                return PACO_ERR_CUDA;
+        }
+    }
+    return cudaGetLastError() == cudaSuccess ? PACO_OK : PACO_ERR_CUDA;
+}
+
+int ts_chase(const BdWs &w, int N, int b, float *band, float *refl_l, float *refl_r, float *d, float *e,
+             cudaStream_t s)
+{
+    const TsCfg cfg = ts_cfg();
+    if (!ts_fits(N, b)) return PACO_ERR_UNSUPPORTED;
+    paco_count_launch(), ts_band_from_w<<<std::min(4096, ceil_div((long)N * 3 * b, 256)), 256, 0, s>>>(
+                             w.W, w.ldw, N, b, band);
+    ChaseArgs a;
+    a.band = band;
+    a.refl_l = refl_l;
+    a.refl_r = refl_r;
+    a.d = d;
+    a.e = e;
+    a.N = N;
+    a.rpc = ceil_div(N, cfg.cs);
+    a.jmax = ts::jmax(N, b);
+    a.T = 3 * (N - 2) + 1;
+    cudaLaunchConfig_t lc = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cfg.cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    lc.gridDim = dim3(cfg.cs);
+    lc.blockDim = dim3(CT);
+    lc.dynamicSmemBytes = chase_smem(N, b, cfg.cs);
+    lc.stream = s;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    paco_count_launch();
+    const cudaError_t err =
+        b == 32 ? cudaLaunchKernelEx(&lc, ts_chase_k<32>, a) : cudaLaunchKernelEx(&lc, ts_chase_k<64>, a);
+    if (err != cudaSuccess) {
+        cudaGetLastError();
+        return PACO_ERR_CUDA;
+    }
+    return PACO_OK;
+}
+
+int ts_form_p1t(const BdWs &w, int N, int b, const float *taup, float *Q, float *Vt, cudaStream_t s)
+{
+    const int n = N - b;
+    // column r of Wt holds the LQ reflector of row r (unit entry at row r)
+    transpose_launch(w.W + b, w.ldw, n, n, w.Vtmp, n, s);
+    BdWs wt = w;
+    wt.W = w.Vtmp;
+    wt.ldw = n;
+    const int rc = qr_form_u(wt, n, n, taup, nullptr, Q, s, n, 0);
+    if (rc) return rc;
+    paco_count_launch(), ts_p1t<<<std::min(8192, ceil_div((long)N * N, 256)), 256, 0, s>>>(Q, N, b, Vt);
+    return cudaGetLastError() == cudaSuccess ? PACO_OK : PACO_ERR_CUDA;
+}
+
+int ts_apply(float *X, long ld, int N, int ncols, int trans, int b, const float *refl, DevStatus *st, cudaStream_t s)
+{
+    (void)st;
+    if (N < 2 || ncols <= 0) return PACO_OK;
+    const int cw = apply_cw(N);
+    const int jm = ts::jmax(N, b);
+    const size_t smem = apply_smem(N, b, cw);
+    const int grid = ceil_div(ncols, cw);
+    paco_count_launch();
+    if (cw == 8)
+        ts_apply_k<8><<<grid, AT, smem, s>>>(X, ld, N, ncols, trans, b, jm, refl);
+    else
+        ts_apply_k<4><<<grid, AT, smem, s>>>(X, ld, N, ncols, trans, b, jm, refl);
+    return cudaGetLastError() == cudaSuccess ? PACO_OK : PACO_ERR_CUDA;
+}

@@ -287,7 +287,7 @@ def autotune(M: int, N: int, stream=None) -> dict:
             "fields": {f: tune_param(M, N, f) for f in TUNE_FIELDS}}
 
 
-TUNE_FIELDS = ["persistent", "rows_per_cta", "tc", "no_tail", "wy", "qb", "mk", "qr"]
+TUNE_FIELDS = ["persistent", "rows_per_cta", "tc", "no_tail", "wy", "qb", "mk", "qr", "ts"]
 
 
 def tune_param(M: int, N: int, name: str, value: int = -1) -> int:

@@ -4,7 +4,8 @@ Runs W warm-up SVDs of an M x N N(0,1) matrix (seed 0) through the one-shot
 workspace path, then exactly one more, with CUDA-graph capture off so that a
 profiler sees every kernel launch on its own (`ncu -s <skip> -c <count>`
 counts them).  Prints the status and the number of library launches of the
-last SVD.  --qr sets the QR-first mode for the shape (0 off, 1 on, 2 automatic)."""
+last SVD.  --qr sets the QR-first mode for the shape (0 off, 1 on, 2 automatic),
+--ts the two-stage band width (32 or 64; 0 off)."""
 import argparse
 import ctypes
 import os
@@ -24,9 +25,12 @@ def main():
     ap.add_argument("N", type=int)
     ap.add_argument("--warm", type=int, default=1)
     ap.add_argument("--qr", type=int, default=None)
+    ap.add_argument("--ts", type=int, default=None)
     a = ap.parse_args()
     if a.qr is not None:
         P.tune_qr(a.M, a.N, a.qr)
+    if a.ts is not None:
+        P.tune_param(a.M, a.N, "ts", a.ts)
     torch.manual_seed(0)
     A = torch.randn(a.M, a.N, device="cuda")
     W = P.Workspace(a.M, a.N)

@@ -161,13 +161,14 @@ def test_tuning_fields_validate_and_round_trip():
     assert P.tune_param(M, N, "wy") == 0 and P.tune_param(M, N, "qb") == 0
     assert P.tune_param(M, N, "wy", 64) == 64 and P.tune_param(M, N, "wy") == 64
     assert P.tune_param(M, N, "qb", 32) == 32 and P.tune_param(M, N, "mk", 8) == 8
-    for name, bad in (("wy", 96), ("qb", 48), ("mk", 9), ("rows_per_cta", 2), ("tc", 2)):
+    assert P.tune_param(M, N, "ts") == 0 and P.tune_param(M, N, "ts", 64) == 64
+    for name, bad in (("wy", 96), ("qb", 48), ("mk", 9), ("rows_per_cta", 2), ("tc", 2), ("ts", 48)):
         with pytest.raises(P.PacoError):
             P.tune_param(M, N, name, bad)
     # paco_tune_set rewrites the first four fields and keeps the tile shapes
     P.tune_set(M, N, [1, 8, 1, 0])
     assert P.tune_get(M, N) == [1, 8, 1, 0] and P.tune_param(M, N, "wy") == 64
     assert P.lib().paco_tune_param(M, N, 9, 0) == -1 and P.lib().paco_tune_param(0, 0, 0, -1) == -1
-    for f, v in (("wy", 0), ("qb", 0), ("mk", 0)):
+    for f, v in (("wy", 0), ("qb", 0), ("mk", 0), ("ts", 0)):
         P.tune_param(M, N, f, v)
     P.tune_set(M, N, [1, 16, 1, 0])

@@ -56,7 +56,7 @@ def test_autotune_tall_shape_and_multi_group():
     M, N = 2400, 1100
     r = P.autotune(M, N)
     assert r["ms"] <= r["default_ms"] * 1.0001 and r["candidates"] >= 8
-    assert r["fields"]["wy"] in (0, 64) and r["fields"]["qb"] in (0, 32)
+    assert r["fields"]["wy"] in (0, 64) and r["fields"]["qb"] in (0, 32) and r["fields"]["ts"] in (0, 32, 64)
     m = P.autotune_multi(4, M, N)
     assert m["group"] in (2, 4) and m["candidates"] == 3 and P.tune_param(M, N, "mk") == m["group"]
     A = [np.random.default_rng(50 + k).standard_normal((M, N)).astype(np.float32) for k in range(3)]
@@ -64,7 +64,7 @@ def test_autotune_tall_shape_and_multi_group():
     assert st == [0, 0, 0]
     for a, s1, u1, v1 in zip(A, s, U, Vt):
         check(a, s1, u1, v1)
-    for f in ("wy", "qb", "mk"):
+    for f in ("wy", "qb", "mk", "ts"):
         P.tune_param(M, N, f, 0)
     P.tune_qr(M, N, 2)
     P.tune_set(M, N, [1, 16, 1, 0])
