@@ -145,14 +145,19 @@ __device__ void chase_task(const ChaseArgs &a, int s, int j, float *vb, float **
     cluster_fence();
     __syncwarp();
     if (tau != 0.f) {
+        // one row per lane, its L entries in registers (vb is 0 beyond L)
         for (int r = rp + 1 + lane; r <= c1; r += 32) {
             float *p = at(r, c0);
+            float seg[B];
+#pragma unroll
+            for (int l = 0; l < B; l++) seg[l] = (l < L) ? p[l] : 0.f;
             float w = 0.f;
-#pragma unroll 8
-            for (int l = 0; l < L; l++) w += p[l] * vb[l];
+#pragma unroll
+            for (int l = 0; l < B; l++) w += seg[l] * vb[l];
             w *= tau;
-#pragma unroll 8
-            for (int l = 0; l < L; l++) p[l] -= w * vb[l];
+#pragma unroll
+            for (int l = 0; l < B; l++)
+                if (l < L) p[l] = seg[l] - w * vb[l];
         }
     }
     // ---- left reflector on rows [c0, c1] from column c0
@@ -191,13 +196,18 @@ __device__ void chase_task(const ChaseArgs &a, int s, int j, float *vb, float **
     __syncwarp();
     if (tau != 0.f) {
         const int e1 = min(c0 + 2 * B - 1, N - 1);
+        // one column per lane, its L entries in registers
         for (int c = c0 + 1 + lane; c <= e1; c += 32) {
+            float seg[B];
+#pragma unroll
+            for (int l = 0; l < B; l++) seg[l] = (l < L) ? rowp[l][c - c0] : 0.f;
             float w = 0.f;
-#pragma unroll 8
-            for (int l = 0; l < L; l++) w += vb[l] * rowp[l][c - c0];
+#pragma unroll
+            for (int l = 0; l < B; l++) w += vb[l] * seg[l];
             w *= tau;
-#pragma unroll 8
-            for (int l = 0; l < L; l++) rowp[l][c - c0] -= w * vb[l];
+#pragma unroll
+            for (int l = 0; l < B; l++)
+                if (l < L) rowp[l][c - c0] = seg[l] - w * vb[l];
         }
     }
     cluster_fence();
