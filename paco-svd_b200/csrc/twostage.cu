@@ -142,8 +142,7 @@ __device__ void chase_task(const ChaseArgs &a, int s, int j, float *vb, float **
         rr[l] = (l == 0) ? tau : v;
         if (l < L) prow[l] = (l == 0) ? beta : 0.f;
     }
-    cluster_fence();
-    __syncwarp();
+    __syncwarp();  // vb
     if (tau != 0.f) {
         // one row per lane, its L entries in registers (vb is 0 beyond L)
         for (int r = rp + 1 + lane; r <= c1; r += 32) {
@@ -166,7 +165,12 @@ __device__ void chase_task(const ChaseArgs &a, int s, int j, float *vb, float **
         const int l = lane + 32 * k;
         if (l < L) rowp[l] = at(c0 + l, c0);  // rowp[l][c - c0] = (c0 + l, c)
     }
-    cluster_fence();
+    // the row updates of other lanes are read from here on: ordered at the
+    // scope of the CTA, or of the cluster when the rows reach another CTA
+    if (rp / rpc == c1 / rpc)
+        __threadfence_block();
+    else
+        cluster_fence();
     __syncwarp();
     float y[NL];
 #pragma unroll
@@ -192,8 +196,7 @@ __device__ void chase_task(const ChaseArgs &a, int s, int j, float *vb, float **
         rl[l] = (l == 0) ? tau : v;
         if (l < L) rowp[l][0] = (l == 0) ? beta : 0.f;
     }
-    cluster_fence();
-    __syncwarp();
+    __syncwarp();  // vb (the column pass reads columns right of c0 only)
     if (tau != 0.f) {
         const int e1 = min(c0 + 2 * B - 1, N - 1);
         // one column per lane, its L entries in registers
@@ -210,8 +213,7 @@ __device__ void chase_task(const ChaseArgs &a, int s, int j, float *vb, float **
                 if (l < L) rowp[l][c - c0] = seg[l] - w * vb[l];
         }
     }
-    cluster_fence();
-    __syncwarp();  // vb and rowp are free for the warp's next task
+    __syncwarp();  // vb and rowp are free for the warp's next task (its rows are disjoint)
 }
 
 template <int B>
@@ -228,7 +230,8 @@ __global__ void __launch_bounds__(CT, 1) ts_chase_k(ChaseArgs a)
     const int r0 = rank * rpc, r1 = min(N, r0 + rpc);
     const int warp = threadIdx.x >> 5;
     for (long t = threadIdx.x; t < (long)max(0, r1 - r0) * LDB; t += CT) sb[t] = a.band[(long)r0 * LDB + t];
-    if (threadIdx.x < CS) rows_of[threadIdx.x] = cl.map_shared_rank(sb, (int)threadIdx.x);
+    // own rows through the CTA's shared window, the others' through the cluster's
+    if (threadIdx.x < CS) rows_of[threadIdx.x] = ((int)threadIdx.x == rank) ? sb : cl.map_shared_rank(sb, (int)threadIdx.x);
     cl.sync();
     const long den = 3L * B - 1;
     for (int t = 0; t < a.T; t++) {
@@ -253,59 +256,99 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src)
 }
 
 // Applies the chasing reflectors of every sweep, in sweep order, to CW
-// columns of X held in shared memory (row r at r + r/32: the rows of the
-// reflectors a warp covers at once fall into different banks).
-template <int CW>
-__global__ void __launch_bounds__(AT, 1) ts_apply_k(float *X, long ld, int N, int ncols, int trans, int b, int jmax,
+// columns of X held in shared memory (row r at r + r/32, so the rows that
+// the reflectors of one warp start at fall into different banks).  Thread t
+// takes reflectors j = t / G, t / G + AT / G, ... of each sweep on the 4
+// columns 4 (t % G) .. 4 (t % G) + 3 (G = CW / 4): the dot products and the
+// update run on float4 rows, with the 32 rows of a B = 32 reflector kept in
+// registers between the two.  The reflectors of sweep s + 1 are staged by
+// cp.async (row stride B + 4 floats) while sweep s is applied.
+template <int CW, int B, int NS>
+__global__ void __launch_bounds__(AT, 1) ts_apply_k(float *X, long ld, int N, int ncols, int trans, int jmax,
                                                    const float *__restrict__ refl)
 {
+    constexpr int G = CW / 4, RS = B + 4;
+    constexpr bool KEEP = (B == 32);  // the reflector's rows stay in registers
     extern __shared__ __align__(16) float sm[];
     const int rows_p = N + N / 32 + 1;
     float *Xs = sm;
-    float *Rb = Xs + (long)rows_p * CW;  // two stages of jmax * b floats
-    const long rb = (long)jmax * b;
+    float *Rb = Xs + (long)rows_p * CW;  // NS stages of jmax reflectors, RS floats each
+    const long rb = (long)jmax * RS;
     const int cbase = blockIdx.x * CW, ncw = min(CW, ncols - cbase);
     auto ri = [](int r) { return r + (r >> 5); };
     if (trans) {
-        for (long t = threadIdx.x; t < (long)ncw * N; t += AT) {
+        for (long t = threadIdx.x; t < (long)CW * N; t += AT) {
             const int c = (int)(t / N), r = (int)(t % N);
-            Xs[ri(r) * CW + c] = X[(long)(cbase + c) * ld + r];
+            Xs[ri(r) * CW + c] = (c < ncw) ? X[(long)(cbase + c) * ld + r] : 0.f;
         }
     } else {
         for (long t = threadIdx.x; t < (long)N * CW; t += AT) {
             const int r = (int)(t / CW), c = (int)(t % CW);
-            if (c < ncw) Xs[ri(r) * CW + c] = X[(long)r * ld + cbase + c];
+            Xs[ri(r) * CW + c] = (c < ncw) ? X[(long)r * ld + cbase + c] : 0.f;
         }
     }
     auto stage = [&](int s, float *dst) {
-        const int nf = ((N - 2 - s + b) / b) * b;
-        const float *src = refl + (long)s * rb;
-        for (int i = threadIdx.x * 4; i < nf; i += AT * 4) cp_async16(dst + i, src + i);
+        const int J = (N - 2 - s + B) / B;
+        const float *src = refl + (long)s * jmax * B;
+        for (int i = threadIdx.x; i < J * (B / 4); i += AT) {
+            const int j = i / (B / 4), q = i % (B / 4);
+            cp_async16(dst + j * RS + 4 * q, src + (long)j * B + 4 * q);
+        }
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
-    stage(0, Rb);
-    for (int s = 0; s <= N - 2; s++) {
-        const float *R = Rb + (s & 1) * rb;
-        if (s + 1 <= N - 2)
-            stage(s + 1, Rb + ((s + 1) & 1) * rb);
+    const int g = threadIdx.x % G;
+    // the reflectors of sweeps s .. s + NS - 2 are in flight while sweep s is
+    // applied (one commit group per sweep, empty ones past the last sweep)
+    for (int q = 0; q < NS - 1; q++) {
+        if (q <= N - 2)
+            stage(q, Rb + q * rb);
         else
             asm volatile("cp.async.commit_group;" ::: "memory");
-        asm volatile("cp.async.wait_group 1;" ::: "memory");
+    }
+    for (int s = 0; s <= N - 2; s++) {
+        const float *R = Rb + (s % NS) * rb;
+        const int sn = s + NS - 1;
+        if (sn <= N - 2)
+            stage(sn, Rb + (sn % NS) * rb);
+        else
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group %0;" ::"n"(NS - 1) : "memory");
         __syncthreads();
-        const int J = (N - 2 - s + b) / b;
-        for (int p = threadIdx.x; p < J * CW; p += AT) {
-            const int j = p / CW, c = p % CW;
-            const float *v = R + j * b;
+        const int J = (N - 2 - s + B) / B;
+        for (int j = threadIdx.x / G; j < J; j += AT / G) {
+            const float *v = R + j * RS;
             const float tau = v[0];
-            if (c >= ncw || tau == 0.f) continue;
-            const int c0 = s + 1 + j * b, L = min(b, N - c0);
-            float w = Xs[ri(c0) * CW + c];
-            for (int l = 1; l < L; l++) w += v[l] * Xs[ri(c0 + l) * CW + c];
-            w *= tau;
-            Xs[ri(c0) * CW + c] -= w;
-            for (int l = 1; l < L; l++) Xs[ri(c0 + l) * CW + c] -= w * v[l];
+            if (tau == 0.f) continue;
+            const int c0 = s + 1 + j * B, L = min(B, N - c0);
+            float4 *x0 = reinterpret_cast<float4 *>(Xs + ri(c0) * CW + 4 * g);
+            float4 seg[KEEP ? B : 1];
+            float4 w = *x0;
+            if (KEEP) seg[0] = w;
+#pragma unroll
+            for (int l = 1; l < B; l++) {
+                if (l < L) {
+                    const float4 xv = *reinterpret_cast<const float4 *>(Xs + ri(c0 + l) * CW + 4 * g);
+                    if (KEEP) seg[l] = xv;
+                    const float vl = v[l];
+                    w.x += vl * xv.x; w.y += vl * xv.y; w.z += vl * xv.z; w.w += vl * xv.w;
+                }
+            }
+            w.x *= tau; w.y *= tau; w.z *= tau; w.w *= tau;
+            {
+                const float4 xv = KEEP ? seg[0] : *x0;
+                *x0 = make_float4(xv.x - w.x, xv.y - w.y, xv.z - w.z, xv.w - w.w);
+            }
+#pragma unroll
+            for (int l = 1; l < B; l++) {
+                if (l < L) {
+                    float4 *xp = reinterpret_cast<float4 *>(Xs + ri(c0 + l) * CW + 4 * g);
+                    const float4 xv = KEEP ? seg[l] : *xp;
+                    const float vl = v[l];
+                    *xp = make_float4(xv.x - vl * w.x, xv.y - vl * w.y, xv.z - vl * w.z, xv.w - vl * w.w);
+                }
+            }
         }
-        __syncthreads();  // the stage of sweep s is free for sweep s + 2
+        __syncthreads();  // the stage of sweep s is free for sweep s + NS
     }
     if (trans) {
         for (long t = threadIdx.x; t < (long)ncw * N; t += AT) {
@@ -342,7 +385,10 @@ TsCfg ts_cfg_probe()
         ok = ok && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
              cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess;
     }
-    for (auto f : {(const void *)ts_apply_k<8>, (const void *)ts_apply_k<4>})
+    for (auto f : {(const void *)ts_apply_k<8, 32, 4>, (const void *)ts_apply_k<4, 32, 4>,
+                   (const void *)ts_apply_k<8, 64, 4>, (const void *)ts_apply_k<4, 64, 4>,
+                   (const void *)ts_apply_k<8, 32, 2>, (const void *)ts_apply_k<4, 32, 2>,
+                   (const void *)ts_apply_k<8, 64, 2>, (const void *)ts_apply_k<4, 64, 2>})
         ok = ok && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
@@ -386,10 +432,21 @@ TsCfg ts_cfg()
 
 int apply_cw(int N) { return N <= 4608 ? 8 : 4; }
 
-size_t apply_smem(int N, int b, int cw)
+size_t apply_smem(int N, int b, int cw, int ns)
 {
-    return sizeof(float) * ((size_t)(N + N / 32 + 1) * cw + 2 * (size_t)ts::jmax(N, b) * b);
+    return sizeof(float) * ((size_t)(N + N / 32 + 1) * cw + (size_t)ns * ts::jmax(N, b) * (b + 4));
 }
+
+int optin_smem()
+{
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return optin;
+}
+
+// reflector stages of the back-transformation: 4 when they fit, else 2
+int apply_stages(int N, int b) { return apply_smem(N, b, apply_cw(N), 4) <= (size_t)optin_smem() ? 4 : 2; }
 
 }  // namespace
 
@@ -402,7 +459,7 @@ bool ts_fits(int N, int b)
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    return chase_smem(N, b, c.cs) <= (size_t)c.max_smem && apply_smem(N, b, apply_cw(N)) <= (size_t)optin &&
+    return chase_smem(N, b, c.cs) <= (size_t)c.max_smem && apply_smem(N, b, apply_cw(N), 2) <= (size_t)optin &&
            qr_fits(N, b);
 }
 
@@ -497,12 +554,14 @@ int ts_apply(float *X, long ld, int N, int ncols, int trans, int b, const float 
     if (N < 2 || ncols <= 0) return PACO_OK;
     const int cw = apply_cw(N);
     const int jm = ts::jmax(N, b);
-    const size_t smem = apply_smem(N, b, cw);
     const int grid = ceil_div(ncols, cw);
     paco_count_launch();
-    if (cw == 8)
-        ts_apply_k<8><<<grid, AT, smem, s>>>(X, ld, N, ncols, trans, b, jm, refl);
-    else
-        ts_apply_k<4><<<grid, AT, smem, s>>>(X, ld, N, ncols, trans, b, jm, refl);
+    using K = void (*)(float *, long, int, int, int, int, const float *);
+    const int ns = apply_stages(N, b);
+    K k = ns == 4 ? (cw == 8 ? (b == 32 ? ts_apply_k<8, 32, 4> : ts_apply_k<8, 64, 4>)
+                             : (b == 32 ? ts_apply_k<4, 32, 4> : ts_apply_k<4, 64, 4>))
+                  : (cw == 8 ? (b == 32 ? ts_apply_k<8, 32, 2> : ts_apply_k<8, 64, 2>)
+                             : (b == 32 ? ts_apply_k<4, 32, 2> : ts_apply_k<4, 64, 2>));
+    k<<<grid, AT, apply_smem(N, b, cw, ns), s>>>(X, ld, N, ncols, trans, jm, refl);
     return cudaGetLastError() == cudaSuccess ? PACO_OK : PACO_ERR_CUDA;
 }
