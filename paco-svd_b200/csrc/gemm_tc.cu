@@ -144,11 +144,10 @@ TcGeom tc_geom(int M, int N, int K)
 // when `transposed`); writes hi and lo images, image (rt, kt) at
 // (rt * KT + kt) * IMG floats.  One CTA of 256 threads per image.
 // With lim, k >= *lim (and, for A, rows >= *lim) read as 0.
-__global__ void __launch_bounds__(256) tc_pack(GemmOp X, int transposed, int R, int K, int KT, float *hi,
-                                               float *lo, const int *lim)
+__device__ __forceinline__ void tc_pack_image(GemmOp X, int transposed, int R, int K, int KT, float *hi, float *lo,
+                                              const int *lim, int img)
 {
     __shared__ float tile[TM][TK + 1];
-    const int img = blockIdx.x;
     const int rt = img / KT, kt = img % KT;
     const int t = threadIdx.x;
     if (lim) {
@@ -183,6 +182,18 @@ __global__ void __launch_bounds__(256) tc_pack(GemmOp X, int transposed, int R, 
         reinterpret_cast<float4 *>(hi + base)[chunk] = h;
         reinterpret_cast<float4 *>(lo + base)[chunk] = l;
     }
+}
+
+// Both operands of a product in one launch: CTAs [0, nA) pack the images of
+// A (R = M), the others those of B (transposed, R = N), one image each.
+__global__ void __launch_bounds__(256) tc_pack(GemmOp A, int M, float *Ahi, float *Alo, int nA, GemmOp B, int N,
+                                               float *Bhi, float *Blo, int K, int KT, const int *lim)
+{
+    const int img = blockIdx.x;
+    if (img < nA)
+        tc_pack_image(A, 0, M, K, KT, Ahi, Alo, lim, img);
+    else
+        tc_pack_image(B, 1, N, K, KT, Bhi, Blo, lim, img - nA);
 }
 
 // ------------------------------------------------------------------ GEMM
@@ -875,8 +886,8 @@ cudaError_t gemm_tc_run(int M, int N, int K, float alpha, GemmOp A, GemmOp B, fl
     const bool persistent = !part && tc_persistent();
     // the one-tile kernel reads a plain row-major B itself (no packing pass)
     const bool bdirect = !persistent && !lim && g_tc_direct_b && B.cs == 1 && !B.gather && !B.p2;
-    paco_count_launch(), tc_pack<<<g.MT * g.KT, 256, 0, s>>>(A, 0, M, K, g.KT, Ahi, Alo, lim);
-    if (!bdirect) paco_count_launch(), tc_pack<<<g.NT * g.KT, 256, 0, s>>>(B, 1, N, K, g.KT, Bhi, Blo, lim);
+    const int nA = g.MT * g.KT, nB = bdirect ? 0 : g.NT * g.KT;
+    paco_count_launch(), tc_pack<<<nA + nB, 256, 0, s>>>(A, M, Ahi, Alo, nA, B, N, Bhi, Blo, K, g.KT, lim);
     // bulk-copy epilogue when every row segment of the destination is 16-byte aligned
     const float *dst = part ? part : C;
     const long dld = part ? (long)N : ldc;

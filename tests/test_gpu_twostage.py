@@ -64,7 +64,7 @@ def test_band_and_bidiagonal_keep_the_singular_values(M, N, b):
 
 
 @pytest.mark.parametrize("M,N,b", [(1024, 1024, 32), (1024, 1024, 64), (1100, 1030, 32), (2048, 1024, 64),
-                                   (1536, 1536, 32)])
+                                   (1536, 1536, 32), (4096, 4096, 32)])
 def test_two_stage_svd_matches_lapack(M, N, b):
     A = np.random.default_rng(M * 3 + N + b).standard_normal((M, N)).astype(np.float32)
     try:
