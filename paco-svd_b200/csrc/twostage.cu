@@ -42,7 +42,7 @@
 namespace {
 namespace cg = cooperative_groups;
 
-constexpr int CT = 256, CWARPS = CT / 32;  // chasing kernel: threads, warps per CTA
+constexpr int CT = 512, CTEAM = 128, NTEAM = CT / CTEAM;  // chasing kernel: threads, threads per task, teams
 constexpr int AT = 256;                    // back-transformation kernel threads
 
 // dst[c * ldd + r] = src[r * lds + c] for r < rows, c < cols
@@ -99,16 +99,33 @@ struct ChaseArgs {
 
 __device__ __forceinline__ void cluster_fence() { asm volatile("fence.acq_rel.cluster;" ::: "memory"); }
 
-// One chasing task (sweep s, step j) on one warp.  rows_of[o] is the generic
-// address of CTA o's band rows; element (r, c) of the band is entry
-// c - r + B of row r's storage.
+// Per-team shared state of a chasing task.
 template <int B>
-__device__ void chase_task(const ChaseArgs &a, int s, int j, float *vb, float **rowp, float *const *rows_of,
+struct ChaseTeam {
+    float vb[B];     // the current reflector, v[0] = 1, zero beyond its length
+    float *rowp[B];  // rowp[l] = address of band element (c0 + l, c0)
+    float tau;
+};
+
+__device__ __forceinline__ void team_sync(int team)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(team + 1), "r"(CTEAM) : "memory");
+}
+
+// One chasing task (sweep s, step j) on a team of CTEAM threads (4 warps).
+// rows_of[o] is the generic address of CTA o's band rows; element (r, c) of
+// the band is entry c - r + B of row r's storage.  The team's first warp forms
+// the two reflectors; the updates split each row (then each column) into
+// B/16 segments of 16 entries, one thread per segment, the segment sums of a
+// row added by shuffles between neighbouring lanes.
+template <int B>
+__device__ void chase_task(const ChaseArgs &a, int s, int j, int team, ChaseTeam<B> &ts, float *const *rows_of,
                            int rpc)
 {
-    constexpr int NL = B / 32, OFF = B, LDB = 3 * B;
-    const int lane = threadIdx.x & 31, N = a.N;
-    // address of element (r, c)
+    constexpr int NL = B / 32, OFF = B, LDB = 3 * B, GS = B / 16, SEG = 16;
+    constexpr int STRIDE = CTEAM / GS;  // rows (columns) one pass of the team covers
+    const int tid = threadIdx.x % CTEAM, lane = threadIdx.x & 31, N = a.N;
+    const bool lead = tid < 32;  // the team's first warp
     auto at = [&](int r, int c) -> float * {
         const int o = r / rpc;
         return rows_of[o] + (long)(r - o * rpc) * LDB + (c - r + OFF);
@@ -116,122 +133,145 @@ __device__ void chase_task(const ChaseArgs &a, int s, int j, float *vb, float **
     const int c0 = s + 1 + j * B;
     const int c1 = min(c0 + B - 1, N - 1), L = c1 - c0 + 1;
     const int rp = (j == 0) ? s : c0 - B;
-    // ---- right reflector on columns [c0, c1] from row rp
-    float *prow = at(rp, c0);  // prow[l] = (rp, c0 + l)
-    float x[NL];
+    const bool remote = (rp / rpc != c1 / rpc);  // rows of another CTA are touched
+    const int g = tid % GS, gi = tid / GS;       // segment, row (column) slot
+    // ---- right reflector on columns [c0, c1] from row rp (first warp)
+    if (lead) {
+        float *prow = at(rp, c0);
+        float x[NL];
 #pragma unroll
-    for (int k = 0; k < NL; k++) {
-        const int l = lane + 32 * k;
-        x[k] = (l < L) ? prow[l] : 0.f;
+        for (int k = 0; k < NL; k++) {
+            const int l = lane + 32 * k;
+            x[k] = (l < L) ? prow[l] : 0.f;
+        }
+        float sg = 0.f;
+#pragma unroll
+        for (int k = 0; k < NL; k++)
+            if (lane + 32 * k >= 1) sg += x[k] * x[k];
+        sg = warp_sum(sg);
+        const float x0 = __shfl_sync(0xffffffffu, x[0], 0);
+        float beta, tau, v0;
+        make_reflector(x0, sg, L, &beta, &tau, &v0);
+        const float inv = 1.f / v0;
+        float *rr = a.refl_r + ((long)s * a.jmax + j) * B;
+#pragma unroll
+        for (int k = 0; k < NL; k++) {
+            const int l = lane + 32 * k;
+            const float v = (l == 0) ? 1.f : (l < L ? x[k] * inv : 0.f);
+            ts.vb[l] = v;
+            rr[l] = (l == 0) ? tau : v;
+            if (l < L) prow[l] = (l == 0) ? beta : 0.f;
+        }
+        if (lane == 0) ts.tau = tau;
     }
-    float sg = 0.f;
-#pragma unroll
-    for (int k = 0; k < NL; k++)
-        if (lane + 32 * k >= 1) sg += x[k] * x[k];
-    sg = warp_sum(sg);
-    const float x0 = __shfl_sync(0xffffffffu, x[0], 0);
-    float beta, tau, v0;
-    make_reflector(x0, sg, L, &beta, &tau, &v0);
-    float inv = 1.f / v0;
-    float *rr = a.refl_r + ((long)s * a.jmax + j) * B;
-#pragma unroll
-    for (int k = 0; k < NL; k++) {
-        const int l = lane + 32 * k;
-        const float v = (l == 0) ? 1.f : (l < L ? x[k] * inv : 0.f);
-        vb[l] = v;
-        rr[l] = (l == 0) ? tau : v;
-        if (l < L) prow[l] = (l == 0) ? beta : 0.f;
-    }
-    __syncwarp();  // vb
+    team_sync(team);
+    float tau = ts.tau;
     if (tau != 0.f) {
-        // one row per lane, its L entries in registers (vb is 0 beyond L)
-        for (int r = rp + 1 + lane; r <= c1; r += 32) {
-            float *p = at(r, c0);
-            float seg[B];
-#pragma unroll
-            for (int l = 0; l < B; l++) seg[l] = (l < L) ? p[l] : 0.f;
+        // rows rp+1 .. c1, GS threads per row
+        for (int base = 0; base < 2 * B - 1; base += STRIDE) {
+            const int r = rp + 1 + base + gi;
+            const bool act = r <= c1;
+            float *p = act ? at(r, c0) + SEG * g : nullptr;
+            float seg[SEG];
             float w = 0.f;
 #pragma unroll
-            for (int l = 0; l < B; l++) w += seg[l] * vb[l];
-            w *= tau;
+            for (int l = 0; l < SEG; l++) {
+                const int lc = SEG * g + l;
+                seg[l] = (act && lc < L) ? p[l] : 0.f;
+                w += seg[l] * ts.vb[lc];
+            }
 #pragma unroll
-            for (int l = 0; l < B; l++)
-                if (l < L) p[l] = seg[l] - w * vb[l];
+            for (int o = 1; o < GS; o <<= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+            w *= tau;
+            if (act) {
+#pragma unroll
+                for (int l = 0; l < SEG; l++)
+                    if (SEG * g + l < L) p[l] = seg[l] - w * ts.vb[SEG * g + l];
+            }
         }
     }
-    // ---- left reflector on rows [c0, c1] from column c0
+    // the row updates are read from here on, by other threads
+    if (remote) cluster_fence();
+    team_sync(team);
+    // ---- left reflector on rows [c0, c1] from column c0 (first warp)
+    if (lead) {
+        float *rp_[NL];
 #pragma unroll
-    for (int k = 0; k < NL; k++) {
-        const int l = lane + 32 * k;
-        if (l < L) rowp[l] = at(c0 + l, c0);  // rowp[l][c - c0] = (c0 + l, c)
+        for (int k = 0; k < NL; k++) {
+            const int l = lane + 32 * k;
+            rp_[k] = (l < L) ? at(c0 + l, c0) : nullptr;
+            if (l < L) ts.rowp[l] = rp_[k];
+        }
+        float y[NL];
+#pragma unroll
+        for (int k = 0; k < NL; k++) y[k] = rp_[k] ? *rp_[k] : 0.f;
+        float sg = 0.f;
+#pragma unroll
+        for (int k = 0; k < NL; k++)
+            if (lane + 32 * k >= 1) sg += y[k] * y[k];
+        sg = warp_sum(sg);
+        const float y0 = __shfl_sync(0xffffffffu, y[0], 0);
+        float beta, tl, v0;
+        make_reflector(y0, sg, L, &beta, &tl, &v0);
+        const float inv = 1.f / v0;
+        float *rl = a.refl_l + ((long)s * a.jmax + j) * B;
+#pragma unroll
+        for (int k = 0; k < NL; k++) {
+            const int l = lane + 32 * k;
+            const float v = (l == 0) ? 1.f : (l < L ? y[k] * inv : 0.f);
+            ts.vb[l] = v;
+            rl[l] = (l == 0) ? tl : v;
+            if (l < L) *rp_[k] = (l == 0) ? beta : 0.f;
+        }
+        if (lane == 0) ts.tau = tl;
     }
-    // the row updates of other lanes are read from here on: ordered at the
-    // scope of the CTA, or of the cluster when the rows reach another CTA
-    if (rp / rpc == c1 / rpc)
-        __threadfence_block();
-    else
-        cluster_fence();
-    __syncwarp();
-    float y[NL];
-#pragma unroll
-    for (int k = 0; k < NL; k++) {
-        const int l = lane + 32 * k;
-        y[k] = (l < L) ? rowp[l][0] : 0.f;
-    }
-    sg = 0.f;
-#pragma unroll
-    for (int k = 0; k < NL; k++)
-        if (lane + 32 * k >= 1) sg += y[k] * y[k];
-    sg = warp_sum(sg);
-    const float y0 = __shfl_sync(0xffffffffu, y[0], 0);
-    make_reflector(y0, sg, L, &beta, &tau, &v0);
-    inv = 1.f / v0;
-    float *rl = a.refl_l + ((long)s * a.jmax + j) * B;
-    __syncwarp();  // every lane is done with vb
-#pragma unroll
-    for (int k = 0; k < NL; k++) {
-        const int l = lane + 32 * k;
-        const float v = (l == 0) ? 1.f : (l < L ? y[k] * inv : 0.f);
-        vb[l] = v;
-        rl[l] = (l == 0) ? tau : v;
-        if (l < L) rowp[l][0] = (l == 0) ? beta : 0.f;
-    }
-    __syncwarp();  // vb (the column pass reads columns right of c0 only)
+    team_sync(team);
+    tau = ts.tau;
     if (tau != 0.f) {
+        // columns c0+1 .. e1 of rows [c0, c1], GS threads per column
         const int e1 = min(c0 + 2 * B - 1, N - 1);
-        // one column per lane, its L entries in registers
-        for (int c = c0 + 1 + lane; c <= e1; c += 32) {
-            float seg[B];
-#pragma unroll
-            for (int l = 0; l < B; l++) seg[l] = (l < L) ? rowp[l][c - c0] : 0.f;
+        for (int base = 0; base < 2 * B - 1; base += STRIDE) {
+            const int c = c0 + 1 + base + gi;
+            const bool act = c <= e1;
+            float seg[SEG];
             float w = 0.f;
 #pragma unroll
-            for (int l = 0; l < B; l++) w += vb[l] * seg[l];
-            w *= tau;
+            for (int l = 0; l < SEG; l++) {
+                const int lr = SEG * g + l;
+                seg[l] = (act && lr < L) ? ts.rowp[lr][c - c0] : 0.f;
+                w += ts.vb[lr] * seg[l];
+            }
 #pragma unroll
-            for (int l = 0; l < B; l++)
-                if (l < L) rowp[l][c - c0] = seg[l] - w * vb[l];
+            for (int o = 1; o < GS; o <<= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+            w *= tau;
+            if (act) {
+#pragma unroll
+                for (int l = 0; l < SEG; l++) {
+                    const int lr = SEG * g + l;
+                    if (lr < L) ts.rowp[lr][c - c0] = seg[l] - w * ts.vb[lr];
+                }
+            }
         }
     }
-    __syncwarp();  // vb and rowp are free for the warp's next task (its rows are disjoint)
+    team_sync(team);  // vb and rowp are free for the team's next task (its rows are disjoint)
 }
 
 template <int B>
 __global__ void __launch_bounds__(CT, 1) ts_chase_k(ChaseArgs a)
 {
     extern __shared__ float sb[];  // this CTA's rows of the band, 3B floats each
-    __shared__ float vbuf[CWARPS][B];
-    __shared__ float *rowp[CWARPS][B];
+    __shared__ ChaseTeam<B> teams[NTEAM];
     __shared__ float *rows_of[16];
     constexpr int LDB = 3 * B;
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank(), CS = (int)cl.num_blocks();
     const int N = a.N, rpc = a.rpc;
     const int r0 = rank * rpc, r1 = min(N, r0 + rpc);
-    const int warp = threadIdx.x >> 5;
+    const int team = threadIdx.x / CTEAM;
     for (long t = threadIdx.x; t < (long)max(0, r1 - r0) * LDB; t += CT) sb[t] = a.band[(long)r0 * LDB + t];
     // own rows through the CTA's shared window, the others' through the cluster's
-    if (threadIdx.x < CS) rows_of[threadIdx.x] = ((int)threadIdx.x == rank) ? sb : cl.map_shared_rank(sb, (int)threadIdx.x);
+    if (threadIdx.x < CS)
+        rows_of[threadIdx.x] = ((int)threadIdx.x == rank) ? sb : cl.map_shared_rank(sb, (int)threadIdx.x);
     cl.sync();
     const long den = 3L * B - 1;
     for (int t = 0; t < a.T; t++) {
@@ -240,8 +280,8 @@ __global__ void __launch_bounds__(CT, 1) ts_chase_k(ChaseArgs a)
         long s_hi = min((long)t / 3, (long)N - 2);
         s_hi = (num - r0 >= 0) ? min(s_hi, (num - r0) / den) : -1;
         const long s_lo = (num - r1 >= 0) ? (num - r1) / den + 1 : 0;
-        for (long s = s_lo + warp; s <= s_hi; s += CWARPS)
-            chase_task<B>(a, (int)s, (int)(t - 3 * s), vbuf[warp], rowp[warp], rows_of, rpc);
+        for (long s = s_lo + team; s <= s_hi; s += NTEAM)
+            chase_task<B>(a, (int)s, (int)(t - 3 * s), team, teams[team], rows_of, rpc);
         cl.sync();
     }
     for (int r = r0 + (int)threadIdx.x; r < r1; r += CT) {
