@@ -297,18 +297,17 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src)
 
 // Applies the chasing reflectors of every sweep, in sweep order, to CW
 // columns of X held in shared memory (row r at r + r/32, so the rows that
-// the reflectors of one warp start at fall into different banks).  Thread t
-// takes reflectors j = t / G, t / G + AT / G, ... of each sweep on the 4
-// columns 4 (t % G) .. 4 (t % G) + 3 (G = CW / 4): the dot products and the
-// update run on float4 rows, with the 32 rows of a B = 32 reflector kept in
-// registers between the two.  The reflectors of sweep s + 1 are staged by
-// cp.async (row stride B + 4 floats) while sweep s is applied.
+// the reflectors of one warp start at fall into different banks).  A
+// reflector's work on 4 columns (a float4 column group, G = CW / 4 of them)
+// is split over P = B / 8 neighbouring lanes, 8 rows each kept in registers
+// between the dot product (summed over the P lanes by shuffles) and the
+// update; the reflectors of the sweeps ahead are staged by cp.async (row
+// stride B + 4 floats) while sweep s is applied.
 template <int CW, int B, int NS>
 __global__ void __launch_bounds__(AT, 1) ts_apply_k(float *X, long ld, int N, int ncols, int trans, int jmax,
                                                    const float *__restrict__ refl)
 {
-    constexpr int G = CW / 4, RS = B + 4;
-    constexpr bool KEEP = (B == 32);  // the reflector's rows stay in registers
+    constexpr int G = CW / 4, RS = B + 4, P = B / 8, JSTEP = AT / (P * G);
     extern __shared__ __align__(16) float sm[];
     const int rows_p = N + N / 32 + 1;
     float *Xs = sm;
@@ -336,7 +335,7 @@ __global__ void __launch_bounds__(AT, 1) ts_apply_k(float *X, long ld, int N, in
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
-    const int g = threadIdx.x % G;
+    const int q = threadIdx.x % P, g = (threadIdx.x / P) % G, js = threadIdx.x / (P * G);
     // the reflectors of sweeps s .. s + NS - 2 are in flight while sweep s is
     // applied (one commit group per sweep, empty ones past the last sweep)
     for (int q = 0; q < NS - 1; q++) {
@@ -355,36 +354,44 @@ __global__ void __launch_bounds__(AT, 1) ts_apply_k(float *X, long ld, int N, in
         asm volatile("cp.async.wait_group %0;" ::"n"(NS - 1) : "memory");
         __syncthreads();
         const int J = (N - 2 - s + B) / B;
-        for (int j = threadIdx.x / G; j < J; j += AT / G) {
-            const float *v = R + j * RS;
-            const float tau = v[0];
-            if (tau == 0.f) continue;
-            const int c0 = s + 1 + j * B, L = min(B, N - c0);
-            float4 *x0 = reinterpret_cast<float4 *>(Xs + ri(c0) * CW + 4 * g);
-            float4 seg[KEEP ? B : 1];
-            float4 w = *x0;
-            if (KEEP) seg[0] = w;
+        // thread: part q (rows 8q .. 8q+7 of the reflector), column group g,
+        // reflector slot js; the P parts of a reflector are neighbouring lanes
+        for (int jb = 0; jb < J; jb += JSTEP) {
+            const int jj = jb + js;
+            const float *v = R + jj * RS;
+            const float tau = (jj < J) ? v[0] : 0.f;
+            const int c0 = s + 1 + jj * B, L = min(B, N - c0);
+            float4 seg[8];
+            float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (tau != 0.f) {
 #pragma unroll
-            for (int l = 1; l < B; l++) {
-                if (l < L) {
-                    const float4 xv = *reinterpret_cast<const float4 *>(Xs + ri(c0 + l) * CW + 4 * g);
-                    if (KEEP) seg[l] = xv;
-                    const float vl = v[l];
-                    w.x += vl * xv.x; w.y += vl * xv.y; w.z += vl * xv.z; w.w += vl * xv.w;
+                for (int l = 0; l < 8; l++) {
+                    const int lr = 8 * q + l;
+                    if (lr < L) {
+                        seg[l] = *reinterpret_cast<const float4 *>(Xs + ri(c0 + lr) * CW + 4 * g);
+                        const float vl = lr ? v[lr] : 1.f;
+                        w.x += vl * seg[l].x; w.y += vl * seg[l].y; w.z += vl * seg[l].z; w.w += vl * seg[l].w;
+                    }
                 }
             }
-            w.x *= tau; w.y *= tau; w.z *= tau; w.w *= tau;
-            {
-                const float4 xv = KEEP ? seg[0] : *x0;
-                *x0 = make_float4(xv.x - w.x, xv.y - w.y, xv.z - w.z, xv.w - w.w);
-            }
 #pragma unroll
-            for (int l = 1; l < B; l++) {
-                if (l < L) {
-                    float4 *xp = reinterpret_cast<float4 *>(Xs + ri(c0 + l) * CW + 4 * g);
-                    const float4 xv = KEEP ? seg[l] : *xp;
-                    const float vl = v[l];
-                    *xp = make_float4(xv.x - vl * w.x, xv.y - vl * w.y, xv.z - vl * w.z, xv.w - vl * w.w);
+            for (int o = 1; o < P; o <<= 1) {
+                w.x += __shfl_xor_sync(0xffffffffu, w.x, o);
+                w.y += __shfl_xor_sync(0xffffffffu, w.y, o);
+                w.z += __shfl_xor_sync(0xffffffffu, w.z, o);
+                w.w += __shfl_xor_sync(0xffffffffu, w.w, o);
+            }
+            if (tau != 0.f) {
+                w.x *= tau; w.y *= tau; w.z *= tau; w.w *= tau;
+#pragma unroll
+                for (int l = 0; l < 8; l++) {
+                    const int lr = 8 * q + l;
+                    if (lr < L) {
+                        const float vl = lr ? v[lr] : 1.f;
+                        *reinterpret_cast<float4 *>(Xs + ri(c0 + lr) * CW + 4 * g) =
+                            make_float4(seg[l].x - vl * w.x, seg[l].y - vl * w.y, seg[l].z - vl * w.z,
+                                        seg[l].w - vl * w.w);
+                    }
                 }
             }
         }
