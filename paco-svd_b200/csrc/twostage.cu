@@ -299,7 +299,7 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src)
 // columns of X held in shared memory (row r at r + r/32, so the rows that
 // the reflectors of one warp start at fall into different banks).  A
 // reflector's work on 4 columns (a float4 column group, G = CW / 4 of them)
-// is split over P = B / 8 neighbouring lanes, 8 rows each kept in registers
+// is split over P = B / 8 neighbouring lanes, 8 interleaved rows each kept in registers
 // between the dot product (summed over the P lanes by shuffles) and the
 // update; the reflectors of the sweeps ahead are staged by cp.async (row
 // stride B + 4 floats) while sweep s is applied.
@@ -354,7 +354,8 @@ __global__ void __launch_bounds__(AT, 1) ts_apply_k(float *X, long ld, int N, in
         asm volatile("cp.async.wait_group %0;" ::"n"(NS - 1) : "memory");
         __syncthreads();
         const int J = (N - 2 - s + B) / B;
-        // thread: part q (rows 8q .. 8q+7 of the reflector), column group g,
+        // thread: part q (rows q, q + P, q + 2P, ... of the reflector: the 8
+        // lanes of a quarter-warp reach 8 different banks), column group g,
         // reflector slot js; the P parts of a reflector are neighbouring lanes
         for (int jb = 0; jb < J; jb += JSTEP) {
             const int jj = jb + js;
@@ -366,7 +367,7 @@ __global__ void __launch_bounds__(AT, 1) ts_apply_k(float *X, long ld, int N, in
             if (tau != 0.f) {
 #pragma unroll
                 for (int l = 0; l < 8; l++) {
-                    const int lr = 8 * q + l;
+                    const int lr = q + P * l;
                     if (lr < L) {
                         seg[l] = *reinterpret_cast<const float4 *>(Xs + ri(c0 + lr) * CW + 4 * g);
                         const float vl = lr ? v[lr] : 1.f;
@@ -385,7 +386,7 @@ __global__ void __launch_bounds__(AT, 1) ts_apply_k(float *X, long ld, int N, in
                 w.x *= tau; w.y *= tau; w.z *= tau; w.w *= tau;
 #pragma unroll
                 for (int l = 0; l < 8; l++) {
-                    const int lr = 8 * q + l;
+                    const int lr = q + P * l;
                     if (lr < L) {
                         const float vl = lr ? v[lr] : 1.f;
                         *reinterpret_cast<float4 *>(Xs + ri(c0 + lr) * CW + 4 * g) =
