@@ -23,8 +23,8 @@
 // once: the concurrent tasks are 3b - 1 rows apart and never share a row.
 // The band lives in the shared memory of one 16-CTA cluster (contiguous
 // row ranges, row r stored at columns r - b .. r + 2b - 1), each task runs
-// on one warp of the CTA owning its row c0 through distributed shared
-// memory, and the super-steps are separated by cluster barriers.
+// on a team of four warps of the CTA owning its row c0 through distributed
+// shared memory, and the super-steps are separated by cluster barriers.
 //
 // Back-transformation: U = Q1 blockdiag(Q2 U_B, I), V = P1 P2 V_B with Q1, P1
 // from stage 1 (formed explicitly by the compact-WY products of qr.cu) and
@@ -32,7 +32,7 @@
 // chasing reflectors of every sweep, in sweep order, to U[:, :N] from the
 // right and to Vt from the left; it splits the matrix into chunks of 8 (or
 // 4) independent columns (rows of U) held in shared memory, and stages the
-// reflectors of each sweep by cp.async while the previous sweep is applied.
+// reflectors of the sweeps ahead by cp.async while a sweep is applied.
 #include <cooperative_groups.h>
 
 #include "qr.cuh"
@@ -478,7 +478,6 @@ TsCfg ts_cfg()
     return g_ts_cfg[dev];
 }
 
-int apply_cw(int N) { return N <= 4608 ? 8 : 4; }
 
 size_t apply_smem(int N, int b, int cw, int ns)
 {
@@ -493,8 +492,23 @@ int optin_smem()
     return optin;
 }
 
-// reflector stages of the back-transformation: 4 when they fit, else 2
-int apply_stages(int N, int b) { return apply_smem(N, b, apply_cw(N), 4) <= (size_t)optin_smem() ? 4 : 2; }
+// Columns per CTA and reflector stages of the back-transformation: the first
+// of (8, 4), (8, 2), (4, 4), (4, 2) that lets two CTAs share an SM (16 warps
+// to hide the shared-memory latency), else the first that fits one CTA.
+struct ApplyCfg {
+    int cw, ns;
+};
+
+ApplyCfg apply_cfg(int N, int b)
+{
+    const ApplyCfg c[4] = {{8, 4}, {8, 2}, {4, 4}, {4, 2}};
+    const size_t optin = (size_t)optin_smem(), two = 113 * 1024;
+    for (const ApplyCfg &x : c)
+        if (apply_smem(N, b, x.cw, x.ns) <= two) return x;
+    for (const ApplyCfg &x : c)
+        if (apply_smem(N, b, x.cw, x.ns) <= optin) return x;
+    return {0, 0};
+}
 
 }  // namespace
 
@@ -504,11 +518,7 @@ bool ts_fits(int N, int b)
 {
     const TsCfg c = ts_cfg();
     if (c.cs <= 0 || (b != 32 && b != 64) || N <= b || c.cs > 16) return false;
-    int dev = 0, optin = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    return chase_smem(N, b, c.cs) <= (size_t)c.max_smem && apply_smem(N, b, apply_cw(N), 2) <= (size_t)optin &&
-           qr_fits(N, b);
+    return chase_smem(N, b, c.cs) <= (size_t)c.max_smem && apply_cfg(N, b).cw > 0 && qr_fits(N, b);
 }
 
 int ts_band_reduce(const BdWs &w, int M, int N, int b, float *tauq, float *taup, cudaStream_t s)
@@ -600,12 +610,13 @@ int ts_apply(float *X, long ld, int N, int ncols, int trans, int b, const float 
 {
     (void)st;
     if (N < 2 || ncols <= 0) return PACO_OK;
-    const int cw = apply_cw(N);
+    const ApplyCfg ac = apply_cfg(N, b);
+    const int cw = ac.cw, ns = ac.ns;
+    if (cw == 0) return PACO_ERR_UNSUPPORTED;
     const int jm = ts::jmax(N, b);
     const int grid = ceil_div(ncols, cw);
     paco_count_launch();
     using K = void (*)(float *, long, int, int, int, int, const float *);
-    const int ns = apply_stages(N, b);
     K k = ns == 4 ? (cw == 8 ? (b == 32 ? ts_apply_k<8, 32, 4> : ts_apply_k<8, 64, 4>)
                              : (b == 32 ? ts_apply_k<4, 32, 4> : ts_apply_k<4, 64, 4>))
                   : (cw == 8 ? (b == 32 ? ts_apply_k<8, 32, 2> : ts_apply_k<8, 64, 2>)
