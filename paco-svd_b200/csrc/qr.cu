@@ -14,8 +14,9 @@
 //              columns.  The CTAs' partial sums (the column norm, then
 //              v^T A for the remaining columns) are pushed into every CTA's
 //              shared memory through distributed shared memory and added in
-//              rank order, so each CTA forms the same reflector; two cluster
-//              barriers per column.
+//              rank order, so each CTA forms the same reflector; one cluster
+//              barrier per column (the next column's sums are formed right
+//              after a column's update, v^T A from unscaled x: see the kernel).
 // trailing     A[q0:, q1:N] <- (I - V T^T V^T) A[q0:, q1:N] through the
 //              block-reflector products of stage 1 (Gram on the SIMT engine,
 //              T, then V^T A, T^T G1, A -= V G2 on the tensor cores).
@@ -83,13 +84,19 @@ __device__ __forceinline__ void q_st(uint32_t addr, float v)
 
 // Every CTA pushes its partial sums into a slot of its own in every CTA of
 // the cluster (remote stores), so after the cluster barrier each CTA adds the
-// slots from its own shared memory, in rank order.
+// slots from its own shared memory, in rank order.  One cluster barrier per
+// column: right after a column's update each CTA publishes, for the next
+// column x (pivot row p), |x below p|^2 and S_k = sum_{r > p} x_r A[r, k]
+// for the columns k right of it, and the owner of row p publishes that row;
+// with v = x / v0 below the pivot (v_p = 1) the reflector's v^T A is then
+// A[p, k] + S_k / v0, formed by every CTA after the barrier.  The slots
+// alternate between two sets (column parity).
 __global__ void __launch_bounds__(QT, 1) qr_block_k(QrArgs a)
 {
     extern __shared__ float qrows[];          // rpc x (QB + 1): this CTA's rows of the block
-    __shared__ float s_sig_all[QCS_MAX];      // partial |x[1:]|^2 of the current column, by CTA
-    __shared__ float s_x0_all;                // its pivot, from the owner
-    __shared__ float s_w_all[QCS_MAX][QB];    // partial v^T A[:, k], by CTA
+    __shared__ float s_sig[2][QCS_MAX];       // partial |x below the pivot|^2, by parity and CTA
+    __shared__ float s_S[2][QCS_MAX][QB];     // partial S_k, by parity and CTA
+    __shared__ float s_prow[2][QB];           // the pivot row, from its owner
     __shared__ float wpart[QW][QB];           // per-warp partials
     __shared__ float red[QW];
     __shared__ float s_wsum[QB];              // tau v^T A[:, k] of the current column
@@ -102,81 +109,76 @@ __global__ void __launch_bounds__(QT, 1) qr_block_k(QrArgs a)
         const int i = t / nb, k = t % nb;
         qrows[i * LD + k] = a.W[(long)(r0 + i) * a.ldw + a.q0 + k];
     }
-    q_cluster_sync();  // every CTA of the cluster runs before the first remote store
-    // publishes this CTA's sum for the column whose pivot row is pr (and the
-    // pivot itself from its owner)
-    auto push_sig = [&](float t, int pr, int col) {
-        if (tid < CS) {
-            q_st(q_dsmem(&s_sig_all[rank], tid), t);
-            if (pr >= r0 && pr < r0 + nr) q_st(q_dsmem(&s_x0_all, tid), qrows[(pr - r0) * LD + col]);
+    // slots read for columns past the last row (no owner, no rows below) hold 0
+    for (int t = tid; t < 2 * QB; t += QT) (&s_prow[0][0])[t] = 0.f;
+    for (int t = tid; t < 2 * QCS_MAX * QB; t += QT) (&s_S[0][0][0])[t] = 0.f;
+    if (tid < 2 * QCS_MAX) (&s_sig[0][0])[tid] = 0.f;
+    q_cluster_sync();  // every CTA of the cluster runs (and has cleared its slots) before the first remote store
+    // this CTA's partials of column col into slot set par of every CTA
+    auto publish = [&](int col, int par) {
+        const int pr = a.q0 + col;
+        float accs = 0.f, acc0 = 0.f, acc1 = 0.f;
+        for (int i = warp; i < nr; i += QW) {
+            const int r = r0 + i;
+            if (r <= pr) continue;
+            const float x = qrows[i * LD + col];
+            if (lane == 0) accs += x * x;
+            const int k0 = col + 1 + lane, k1 = col + 33 + lane;
+            if (k0 < nb) acc0 += x * qrows[i * LD + k0];
+            if (k1 < nb) acc1 += x * qrows[i * LD + k1];
+        }
+        wpart[warp][lane] = acc0;
+        wpart[warp][lane + 32] = acc1;
+        const float sig = q_block_sum(accs, red);  // its barriers also publish wpart
+        const int kn = nb - col - 1;
+        if (tid < kn) {
+            float t = 0.f;
+#pragma unroll
+            for (int w = 0; w < QW; w++) t += wpart[w][tid];
+            for (int c = 0; c < CS; c++) q_st(q_dsmem(&s_S[par][rank][col + 1 + tid], c), t);
+        }
+        if (tid < CS) q_st(q_dsmem(&s_sig[par][rank], tid), sig);
+        if (pr >= r0 && pr < r0 + nr) {
+            const int i = pr - r0, w = nb - col;
+            for (int t = tid; t < w * CS; t += QT) {
+                const int k = col + t % w, c = t / w;
+                q_st(q_dsmem(&s_prow[par][k], c), qrows[i * LD + k]);
+            }
         }
     };
-    {
-        float acc = 0.f;
-        for (int i = tid; i < nr; i += QT)
-            if (r0 + i > a.q0) acc += qrows[i * LD] * qrows[i * LD];
-        push_sig(q_block_sum(acc, red), a.q0, 0);
-    }
+    publish(0, 0);
     for (int j = 0; j < nb; j++) {
-        const int pr = a.q0 + j;  // pivot row
-        q_cluster_sync();         // every CTA's sums of column j are in place
+        const int par = j & 1, pr = a.q0 + j;  // pivot row
+        q_cluster_sync();                      // every CTA's partials of column j are in place
         float sig = 0.f;
 #pragma unroll
-        for (int c = 0; c < QCS_MAX; c++) sig += (c < CS) ? s_sig_all[c] : 0.f;
+        for (int c = 0; c < QCS_MAX; c++) sig += (c < CS) ? s_sig[par][c] : 0.f;
         float beta, tau, v0;
-        make_reflector(s_x0_all, sig, a.M - pr, &beta, &tau, &v0);
+        make_reflector(s_prow[par][j], sig, a.M - pr, &beta, &tau, &v0);
         const float inv = 1.f / v0;
-        // partial w_k = sum_r v_r A[r, k] over the remaining columns, with
-        // v_r = x_r / v0 below the pivot (stored in place by lane 0 of the
-        // row's warp) and v_pr = 1
         const int kn = nb - j - 1;
-        float acc0 = 0.f, acc1 = 0.f;
+        if (tid < kn) {
+            const int k = j + 1 + tid;
+            float S = 0.f;
+#pragma unroll
+            for (int c = 0; c < QCS_MAX; c++) S += (c < CS) ? s_S[par][c][k] : 0.f;
+            s_wsum[k] = tau * (s_prow[par][k] + S * inv);
+        }
+        if (tid == 0 && rank == 0) a.tau[j] = tau;  // tau of the block's column j
+        __syncthreads();
+        // A[r, k] -= tau v_r w_k for the remaining columns, v stored in column j
         for (int i = warp; i < nr; i += QW) {
             const int r = r0 + i;
             if (r < pr) continue;
             const float v = (r == pr) ? 1.f : qrows[i * LD + j] * inv;
             const int k0 = j + 1 + lane, k1 = j + 33 + lane;
-            if (k0 < nb) acc0 += v * qrows[i * LD + k0];
-            if (k1 < nb) acc1 += v * qrows[i * LD + k1];
+            if (k0 < nb) qrows[i * LD + k0] -= v * s_wsum[k0];
+            if (k1 < nb) qrows[i * LD + k1] -= v * s_wsum[k1];
             __syncwarp();
             if (lane == 0) qrows[i * LD + j] = (r == pr) ? beta : v;
         }
-        wpart[warp][lane] = acc0;
-        wpart[warp][lane + 32] = acc1;
         __syncthreads();
-        if (tid < kn) {
-            float t = 0.f;
-#pragma unroll
-            for (int w = 0; w < QW; w++) t += wpart[w][tid];
-            for (int c = 0; c < CS; c++) q_st(q_dsmem(&s_w_all[rank][tid], c), t);
-        }
-        if (tid == 0 && rank == 0) a.tau[j] = tau;  // tau of the block's column j
-        q_cluster_sync();  // every CTA's partial v^T A is in place
-        if (kn > 0) {
-            if (tid < kn) {
-                float t = 0.f;
-#pragma unroll
-                for (int c = 0; c < QCS_MAX; c++) t += (c < CS) ? s_w_all[c][tid] : 0.f;
-                s_wsum[tid] = t * tau;
-            }
-            __syncthreads();
-            // A[r, k] -= tau v_r w_k for the remaining columns; the sums of
-            // column j + 1 (rows below its pivot) on the way
-            float acc = 0.f;
-            for (int i = warp; i < nr; i += QW) {
-                const int r = r0 + i;
-                if (r < pr) continue;
-                const float v = (r == pr) ? 1.f : qrows[i * LD + j];
-                const int k0 = j + 1 + lane, k1 = j + 33 + lane;
-                if (k0 < nb) {
-                    const float x = qrows[i * LD + k0] - v * s_wsum[lane];
-                    qrows[i * LD + k0] = x;
-                    if (lane == 0 && r > pr + 1) acc += x * x;
-                }
-                if (k1 < nb) qrows[i * LD + k1] -= v * s_wsum[lane + 32];
-            }
-            push_sig(q_block_sum(acc, red), pr + 1, j + 1);
-        }
+        if (j + 1 < nb) publish(j + 1, par ^ 1);
     }
     __syncthreads();
     for (int t = tid; t < nr * nb; t += QT) {
