@@ -12,7 +12,10 @@
 //          thread 0 runs a 2-stage pipeline of bulk copies (mbarrier
 //          complete_tx) and issues the MMAs (tcgen05.mma.cta_group::1
 //          .kind::tf32, M=128, N=128, K=8) into a TMEM accumulator; a
-//          tcgen05.commit per stage releases the stage.  The C tile is
+//          tcgen05.commit per stage releases the stage.  The split's k range
+//          runs in chains of KCHAIN images: the 4 warps add each finished
+//          chain into FP32 sums in TMEM (round-to-nearest; the tensor cores
+//          round their own accumulation toward zero).  The C tile is
 //          bulk-copied into shared memory while the products run (beta != 0);
 //          the 4 warps then read the accumulator with tcgen05.ld, combine it
 //          with C in shared memory and the tile leaves by bulk stores, one
@@ -118,20 +121,18 @@ TcGeom tc_geom(int M, int N, int K)
     g.NT = ceil_div(N, TN);
     g.KT = ceil_div(K, TK);
     // enough CTAs to cover the SMs, at least 4 images of k per split
-    const int tiles = g.MT * g.NT;
-    g.splits = std::max(1, std::min({MAX_SPLITS, ceil_div(148, tiles), g.KT / 4}));
+    const int tiles = g.MT * g.NT, fill = ceil_div(148, tiles);
+    g.splits = std::max(1, std::min({MAX_SPLITS, fill, g.KT / 4}));
     // The tensor cores round each accumulation into TMEM toward zero, so a
-    // long k chain loses about one ulp of the running sum per MMA.  Skinny
-    // products (one or two row tiles, e.g. V^T Q with k = the matrix height)
-    // are split into k chains of at most KCHAIN images whose FP32 partial sums
-    // are added with round-to-nearest, as long as the partials stay small.
-    // (Unsplit products on the persistent kernel chain their k range the same
-    // way inside the kernel, KCP images per chain.)
+    // long k chain would lose about one ulp of the running sum per MMA: both
+    // kernels run a split's k range in chains of KCHAIN (KCP) images whose
+    // sums are added in FP32 with round-to-nearest.  Skinny products (one or
+    // two row tiles, e.g. V^T Q with k = the matrix height) take more splits,
+    // to fill the SMs, as long as the partial sums stay small.
     if (g.MT <= 2) {
-        const int want = ceil_div(g.KT, KCHAIN);
         const long budget = 32L << 20;  // floats of partial sums
-        const int cap = (int)std::max(1L, std::min((long)MAX_CHAIN_SPLITS, budget / std::max(1L, (long)M * N)));
-        g.splits = std::max(g.splits, std::min(want, cap));
+        const long cap = std::max(1L, std::min((long)MAX_CHAIN_SPLITS, budget / std::max(1L, (long)M * N)));
+        g.splits = (int)std::max(1L, std::min({cap, (long)fill, (long)std::max(1, g.KT / KCHAIN)}));
     }
     return g;
 }
@@ -211,7 +212,7 @@ __global__ void __launch_bounds__(128, 1)
 {
     if (lim) M = min(M, *lim);  // rows at or beyond the limit are left as they are
     extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
-    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done, cbar;
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done, cbar, chbar;
     __shared__ uint32_t s_tmem;
     __shared__ int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -238,7 +239,7 @@ __global__ void __launch_bounds__(128, 1)
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
-                     "r"(TN)
+                     "r"(2 * TN)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -249,6 +250,7 @@ __global__ void __launch_bounds__(128, 1)
         }
         mbar_init(&done, 1);
         mbar_init(&cbar, 1);
+        mbar_init(&chbar, 1);
         mbar_init_fence();
         s_fail = 0;
     }
@@ -256,6 +258,33 @@ __global__ void __launch_bounds__(128, 1)
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
+    // The split's k range runs in chains of KCHAIN images: each finished
+    // chain's accumulator (TMEM columns 0..TN-1) is added by the four warps
+    // into FP32 sums (columns TN..2TN-1, round-to-nearest) before the next
+    // chain overwrites it.  Returns false (in every thread) when a wait gave up.
+    const int nch = (nk + KCHAIN - 1) / KCHAIN;
+    const bool chained = nch > 1;
+    const uint32_t tq = tmem + ((uint32_t)(warp * 32) << 16);
+    auto fold = [&](int c, bool fail) -> bool {
+        if (__syncthreads_or(fail)) return false;
+        const bool okw = mbar_wait_bounded(&chbar, c & 1, st, 508);
+        if (__syncthreads_or(!okw)) return false;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll 1
+        for (int cb = 0; cb < TN; cb += 32) {
+            uint32_t v[32], w[32];
+            tmem_ld32(tq + (uint32_t)cb, v);
+            if (c > 0) {
+                tmem_ld32(tq + (uint32_t)(TN + cb), w);
+#pragma unroll
+                for (int q = 0; q < 32; q++) v[q] = __float_as_uint(__uint_as_float(v[q]) + __uint_as_float(w[q]));
+            }
+            tmem_st32(tq + (uint32_t)(TN + cb), v);
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        return true;
+    };
 
     if (tid == 0 && cload) {
         // the C tile streams in while the products run
@@ -329,11 +358,18 @@ __global__ void __launch_bounds__(128, 1)
 #pragma unroll
                     for (int j = 0; j < TK / 8; j++) {
                         const uint64_t dk = (uint64_t)(j * 32 >> 4);
-                        mma_tf32(tmem, alo + dk, bhi + dk, (kb | j) ? 1u : 0u);
+                        mma_tf32(tmem, alo + dk, bhi + dk, ((kb % KCHAIN) | j) ? 1u : 0u);
                         mma_tf32(tmem, ahi + dk, blo + dk, 1u);
                         mma_tf32(tmem, ahi + dk, bhi + dk, 1u);
                     }
                     mma_commit(&empty[s]);
+                }
+            }
+            if (chained && (kb % KCHAIN == KCHAIN - 1 || kb + 1 == nk)) {
+                if (tid == 0 && ok) mma_commit(&chbar);
+                if (!fold(kb / KCHAIN, tid == 0 && !ok)) {
+                    if (tid == 0) ok = false;
+                    break;
                 }
             }
         }
@@ -345,7 +381,9 @@ __global__ void __launch_bounds__(128, 1)
             }
             mma_commit(&done);
         }
-    } else if (tid == 0) {
+    } else {
+        // packed B: thread 0 issues the copies and the MMAs; every thread
+        // joins the chain folds
         const long abase = (long)mt * KT * IMG, bbase = (long)nt * KT * IMG;
         auto produce = [&](int j) {  // k-block j of this split into stage j % STAGES
             float *dst = stage + (long)(j % STAGES) * 4 * IMG;
@@ -358,45 +396,57 @@ __global__ void __launch_bounds__(128, 1)
             tma_load_1d(dst + 3 * IMG, Blo + bbase + ko, IMG * 4u, bar);
         };
         int issued = 0, consumed = 0;
-        for (; issued < nk && issued < STAGES; issued++) produce(issued);
+        if (tid == 0)
+            for (; issued < nk && issued < STAGES; issued++) produce(issued);
         bool ok = true;
-        for (int kb = 0; kb < nk && ok; kb++) {
-            const int s = kb % STAGES;
-            if (!mbar_wait_bounded(&full[s], (kb / STAGES) & 1, st, 500)) {
-                ok = false;
-                break;
-            }
-            consumed = kb + 1;
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t base = smem_u32(stage + (long)s * 4 * IMG);
-            const uint64_t ahi = smem_desc(base), alo = smem_desc(base + IMG * 4);
-            const uint64_t bhi = smem_desc(base + 2 * IMG * 4), blo = smem_desc(base + 3 * IMG * 4);
-#pragma unroll
-            for (int j = 0; j < TK / 8; j++) {
-                const uint64_t dk = (uint64_t)(j * 32 >> 4);  // 8 TF32 = 32 bytes along k
-                mma_tf32(tmem, alo + dk, bhi + dk, (kb | j) ? 1u : 0u);
-                mma_tf32(tmem, ahi + dk, blo + dk, 1u);
-                mma_tf32(tmem, ahi + dk, bhi + dk, 1u);
-            }
-            mma_commit(&empty[s]);
-            // refill the stage the previous k-block used once its MMAs are done
-            if (kb >= 1 && issued < nk) {
-                const int pk = kb - 1;
-                if (!mbar_wait_bounded(&empty[pk % STAGES], (pk / STAGES) & 1, st, 501)) {
+        for (int kb = 0; kb < nk; kb++) {
+            if (tid == 0 && ok) {
+                const int s = kb % STAGES;
+                if (!mbar_wait_bounded(&full[s], (kb / STAGES) & 1, st, 500)) {
                     ok = false;
+                } else {
+                    consumed = kb + 1;
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t base = smem_u32(stage + (long)s * 4 * IMG);
+                    const uint64_t ahi = smem_desc(base), alo = smem_desc(base + IMG * 4);
+                    const uint64_t bhi = smem_desc(base + 2 * IMG * 4), blo = smem_desc(base + 3 * IMG * 4);
+#pragma unroll
+                    for (int j = 0; j < TK / 8; j++) {
+                        const uint64_t dk = (uint64_t)(j * 32 >> 4);  // 8 TF32 = 32 bytes along k
+                        mma_tf32(tmem, alo + dk, bhi + dk, ((kb % KCHAIN) | j) ? 1u : 0u);
+                        mma_tf32(tmem, ahi + dk, blo + dk, 1u);
+                        mma_tf32(tmem, ahi + dk, bhi + dk, 1u);
+                    }
+                    mma_commit(&empty[s]);
+                    // refill the stage the previous k-block used once its MMAs are done
+                    if (kb >= 1 && issued < nk) {
+                        const int pk = kb - 1;
+                        if (!mbar_wait_bounded(&empty[pk % STAGES], (pk / STAGES) & 1, st, 501))
+                            ok = false;
+                        else
+                            produce(issued++);
+                    }
+                }
+            }
+            if (chained && (kb % KCHAIN == KCHAIN - 1 || kb + 1 == nk)) {
+                if (tid == 0 && ok) mma_commit(&chbar);
+                if (!fold(kb / KCHAIN, tid == 0 && !ok)) {
+                    if (tid == 0) ok = false;
                     break;
                 }
-                produce(issued);
-                issued++;
+            } else if (!chained && tid == 0 && !ok) {
+                break;
             }
         }
-        if (!ok) {
-            s_fail = 1;
-            // copies still in flight land before the CTA may exit
-            for (int j = consumed; j < issued; j++)
-                mbar_wait_bounded(&full[j % STAGES], (j / STAGES) & 1, st, 503, 1000000000LL);
+        if (tid == 0) {
+            if (!ok) {
+                s_fail = 1;
+                // copies still in flight land before the CTA may exit
+                for (int j = consumed; j < issued; j++)
+                    mbar_wait_bounded(&full[j % STAGES], (j / STAGES) & 1, st, 503, 1000000000LL);
+            }
+            mma_commit(&done);  // arrives when every MMA issued above has completed
         }
-        mma_commit(&done);  // arrives when every MMA issued above has completed
     }
     __syncthreads();
     bool ok = mbar_wait_bounded(&done, 0, st, 502);
@@ -411,7 +461,7 @@ __global__ void __launch_bounds__(128, 1)
         // block is transposed through shared memory so that the lanes then
         // walk the columns of one row
         float(*sb)[33] = reinterpret_cast<float(*)[33]>(stage + warp * 32 * 33);
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+        const uint32_t taddr = tq + (chained ? (uint32_t)TN : 0u);  // the sums, or the one chain's accumulator
 #pragma unroll 1
         for (int c0 = 0; c0 < TN; c0 += 32) {
             uint32_t v[32];
@@ -458,7 +508,7 @@ __global__ void __launch_bounds__(128, 1)
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TN) : "memory");
 }
 
 // ------------------------------------------------------------------ persistent GEMM

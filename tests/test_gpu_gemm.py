@@ -107,13 +107,13 @@ def test_persistent_and_per_tile_kernels_agree_bitwise(M, N, K):
     assert torch.equal(outs[0], outs[1])
 
 
-def test_persistent_kernel_sums_long_k_in_chains():
-    # 2048 x 2048 (256 tiles: no split-K, the persistent kernel), k = 4096.
-    # The tensor cores round every accumulation into TMEM toward zero; one
-    # chain over the whole k range (the one-tile kernel) carries that bias
-    # through 1536 MMAs, the persistent kernel folds chains of 4 images into
-    # FP32 sums with round-to-nearest.  Its error stays within 1e-6 of the
-    # |A||B| scale and well below the single chain's.
+def test_long_k_products_sum_their_chains():
+    # 2048 x 2048 (256 tiles: no split-K, the persistent kernel) and the
+    # one-tile kernel (mode 2, one CTA per tile and split of k), k = 4096.
+    # The tensor cores round every accumulation into TMEM toward zero; both
+    # kernels fold chains of 4 images into FP32 sums with round-to-nearest, so
+    # neither carries that bias through 1536 MMAs: both stay within 1e-6 of
+    # the |A||B| scale, with RMS errors of the same size.
     import torch
     M = N = 2048
     K = 4096
@@ -128,5 +128,20 @@ def test_persistent_kernel_sums_long_k_in_chains():
         run_gemm(A64.float().cuda(), B64.float().cuda(), C, 1.0, 0.0, mode)
         d = C.double().cpu() - ref
         err[mode] = (d.abs().max().item(), d.pow(2).mean().sqrt().item())
-    assert err[1][0] <= 1e-6 * scale, (err, scale)
-    assert err[1][1] <= 0.25 * err[2][1], err
+    for mode in (1, 2):
+        assert err[mode][0] <= 1e-6 * scale, (err, scale)
+    assert 0.5 <= err[1][1] / err[2][1] <= 2.0, err
+
+
+def test_skinny_product_with_few_splits_is_accurate():
+    # one row tile (128 x 2048), k = 16384: a few splits of 128 images, each
+    # folding 32 chains in the kernel
+    import torch
+    g = torch.Generator().manual_seed(78)
+    A64 = torch.randn(128, 16384, generator=g, dtype=torch.float64).float().double()
+    B64 = torch.randn(16384, 2048, generator=g, dtype=torch.float64).float().double()
+    ref = A64 @ B64
+    scale = (A64.abs() @ B64.abs()).max().item()
+    C = torch.zeros(128, 2048, device="cuda")
+    run_gemm(A64.float().cuda(), B64.float().cuda(), C, 1.0, 0.0, 2)
+    assert (C.double().cpu() - ref).abs().max().item() <= 1e-6 * scale
