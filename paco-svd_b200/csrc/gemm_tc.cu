@@ -294,10 +294,12 @@ __global__ void __launch_bounds__(128, 1)
     }
     if (Bd.p) {
         // thread (warp w, lane l): k chunks c = w, w + 4 (4 k each) of image
-        // rows n = l + 32 j, j < 4
+        // rows n = l + 32 j, j < 4; two images of B in flight in registers
+        // (even images in rb0, odd ones in rb1) while one is converted
         const long abase = (long)mt * KT * IMG;
-        float rb[2][4][4];
-        auto load_b = [&](int j) {
+        using Reg = float[2][4][4];
+        Reg rb0, rb1;
+        auto load_b = [&](Reg &rb, int j) {
             const int kbase = (kb0 + j) * TK;
 #pragma unroll
             for (int cc = 0; cc < 2; cc++)
@@ -311,15 +313,18 @@ __global__ void __launch_bounds__(128, 1)
                     }
                 }
         };
-        if (nk > 0) load_b(0);
+        if (nk > 0) load_b(rb0, 0);
+        if (nk > 1) load_b(rb1, 1);
         bool ok = true;
         int issued = 0, consumed = 0;
-        for (int kb = 0; kb < nk; kb++) {
+        // one k-block: its B image from rb into the stage, rb refilled with
+        // image kb + 2, the MMAs; false when the loop has to stop
+        auto step = [&](int kb, Reg &rb) -> bool {
             const int s = kb % STAGES;
             // the stage's previous MMAs are done before it is refilled
             if (tid == 0 && kb >= STAGES && ok && !mbar_wait_bounded(&empty[s], ((kb / STAGES) - 1) & 1, st, 505))
                 ok = false;
-            if (__syncthreads_or(tid == 0 && !ok)) break;
+            if (__syncthreads_or(tid == 0 && !ok)) return false;
             float *dst = stage + (long)s * 4 * IMG;
             if (tid == 0) {
                 mbar_expect_tx(&full[s], 2u * IMG * 4u);
@@ -343,7 +348,7 @@ __global__ void __launch_bounds__(128, 1)
                     *reinterpret_cast<float4 *>(dst + 3 * IMG + off) = l;
                 }
             }
-            if (kb + 1 < nk) load_b(kb + 1);
+            if (kb + 2 < nk) load_b(rb, kb + 2);
             proxy_async_fence();  // the images written here, visible to the tensor cores
             __syncthreads();
             if (tid == 0 && ok) {
@@ -369,9 +374,14 @@ __global__ void __launch_bounds__(128, 1)
                 if (tid == 0 && ok) mma_commit(&chbar);
                 if (!fold(kb / KCHAIN, tid == 0 && !ok)) {
                     if (tid == 0) ok = false;
-                    break;
+                    return false;
                 }
             }
+            return true;
+        };
+        for (int kb = 0; kb < nk; kb += 2) {
+            if (!step(kb, rb0)) break;
+            if (kb + 1 < nk && !step(kb + 1, rb1)) break;
         }
         if (tid == 0) {
             if (!ok) {
