@@ -103,14 +103,16 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def traffic_ratio():
+def traffic_ratio(resident=False):
     """DRAM bytes per streamed byte of the persistent panel kernel, from the
-    committed ncu summary (profiles/bd_panel_pk_8192x4096.txt, line
-    'dram_per_alg_byte: X')."""
-    path = os.path.join(ROOT, "profiles", "bd_panel_pk_8192x4096.txt")
+    committed ncu summaries: profiles/bd_panel_pk_8192x4096.txt (a trailing
+    matrix larger than L2, line 'dram_per_alg_byte: X') or, when the matrix
+    fits L2, profiles/bd_panel_pk_4096_l2resident.txt ('dram_per_streamed_byte: X')."""
+    name, key = (("bd_panel_pk_4096_l2resident.txt", "dram_per_streamed_byte:") if resident
+                 else ("bd_panel_pk_8192x4096.txt", "dram_per_alg_byte:"))
     try:
-        for ln in open(path):
-            if ln.startswith("dram_per_alg_byte:"):
+        for ln in open(os.path.join(ROOT, "profiles", name)):
+            if ln.startswith(key):
                 return float(ln.split(":")[1])
     except Exception:
         pass
@@ -471,7 +473,8 @@ def main():
     alg_per_launch = classic * args.steps / n_launch
     avg_s = rp_ms / 1e3 / n_launch
     achieved = (alg_per_launch / 1e9) / avg_s if rp_ms > 0 else None
-    ratio = traffic_ratio()
+    # the trailing matrix of the column steps fits L2 (126 MB) or streams from DRAM
+    ratio = traffic_ratio(resident=4.0 * Mg * N <= 96 * 2**20)
     roof = {"kernel": kname, "bound": "hbm",
             "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": (achieved / peaks["hbm_gbs"]) if achieved else None,
