@@ -299,10 +299,10 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src)
 // columns of X held in shared memory (row r at r + r/32, so the rows that
 // the reflectors of one warp start at fall into different banks).  A
 // reflector's work on 4 columns (a float4 column group, G = CW / 4 of them)
-// is split over P = B / 8 neighbouring lanes, 8 interleaved rows each kept in registers
-// between the dot product (summed over the P lanes by shuffles) and the
-// update; the reflectors of the sweeps ahead are staged by cp.async (row
-// stride B + 4 floats) while sweep s is applied.
+// is split over P = B / 8 neighbouring lanes, 8 interleaved rows each, kept
+// in registers between the dot product (summed over the P lanes by
+// shuffles) and the update; the reflectors of the sweeps ahead are staged
+// by cp.async (row stride B + 4 floats) while sweep s is applied.
 template <int CW, int B, int NS>
 __global__ void __launch_bounds__(AT, 1) ts_apply_k(float *X, long ld, int N, int ncols, int trans, int jmax,
                                                    const float *__restrict__ refl)
