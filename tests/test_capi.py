@@ -108,6 +108,22 @@ def test_noalloc_scratch_covers_its_largest_shape():
     assert P.lib().paco_svd_workspace_size(1024, 512) <= 16 << 20
 
 
+def test_workspace_covers_the_two_stage_buffers():
+    # from N = 1024 on, paco_svd_workspace_size also reserves the two-stage
+    # path's band (N x 3b) and its two chasing-reflector stores
+    # (N x ceil((N-1)/b) x b floats each), sized for the widest band b = 64
+    L = P.lib()
+    for M, N in ((1023, 1023), (1024, 1024), (4096, 4096), (8192, 4096)):
+        ws = L.paco_svd_workspace_size(M, N)
+        if N < 1024:
+            continue
+        jmax = (N - 2 + 64) // 64
+        extra = 4 * (N * 3 * 64 + 2 * N * jmax * 64)
+        assert ws >= extra
+    a, b = L.paco_svd_workspace_size(1023, 1023), L.paco_svd_workspace_size(1024, 1024)
+    assert b - a >= 4 * 2 * 1024 * 16 * 64  # the step at N = 1024
+
+
 def test_batched_workspace_rejects_bad_shapes():
     assert P.batched_workspace_size([(4, 8)]) == 0               # M < N
     assert P.batched_workspace_size([(10, 0)]) == 0              # N = 0
