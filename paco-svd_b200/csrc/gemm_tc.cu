@@ -120,8 +120,9 @@ TcGeom tc_geom(int M, int N, int K)
     g.MT = ceil_div(M, TM);
     g.NT = ceil_div(N, TN);
     g.KT = ceil_div(K, TK);
-    // enough CTAs to cover the SMs, at least 4 images of k per split
-    const int tiles = g.MT * g.NT, fill = ceil_div(148, tiles);
+    // as many CTAs as fit one wave on the SMs (a second, partial wave would
+    // double the time), at least 4 images of k per split
+    const int tiles = g.MT * g.NT, fill = std::max(1, 148 / tiles);
     g.splits = std::max(1, std::min({MAX_SPLITS, fill, g.KT / 4}));
     // The tensor cores round each accumulation into TMEM toward zero, so a
     // long k chain would lose about one ulp of the running sum per MMA: both
