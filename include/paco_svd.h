@@ -162,12 +162,12 @@ void paco_ctx_destroy(paco_ctx *ctx);
  * PACO_ERR_UNSUPPORTED).  All scratch lives in a 16 MiB device array inside
  * the library, which every GPU that loads the library holds until the process
  * exits; no device memory is allocated per call.  The first call on a device
- * looks up that array's address (make it before any stream capture) and keeps
- * it for the life of the process, so a device reset with cudaDeviceReset
- * must not be followed by further calls on that device.  Calls
- * share the array: calls that overlap on the GPU, from any stream or thread,
- * race and must be serialized by the caller.  The call synchronizes `stream`
- * and returns the device status of the run. */
+ * looks up that array's address and keeps it for the life of the process, so
+ * a device reset with cudaDeviceReset must not be followed by further calls
+ * on that device.  Calls share the array: calls that overlap on the GPU, from
+ * any stream or thread, race and must be serialized by the caller.  The call
+ * synchronizes `stream` and returns the device status of the run
+ * (PACO_ERR_INVALID_ARG when `stream` is being captured). */
 int paco_svd_noalloc(int M, int N, float *A, float *U, float *Vt, float *sigma, void *stream);
 
 /* Largest M (and so N) of a matrix of the batched form's one-CTA-per-matrix

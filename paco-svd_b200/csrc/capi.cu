@@ -1223,6 +1223,13 @@ int paco_svd_noalloc(int M, int N, float *A, float *U, float *Vt, float *sigma, 
     if (N < 1 || M < N) return PACO_ERR_INVALID_ARG;
     if (M > PACO_NOALLOC_MAX_M || N > PACO_NOALLOC_MAX_N) return PACO_ERR_UNSUPPORTED;
     if (!A || !U || !Vt || !sigma) return PACO_ERR_INVALID_ARG;
+    // the call ends by synchronizing the stream, which a stream capture forbids
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing((cudaStream_t)stream, &cs) != cudaSuccess) {
+        cudaGetLastError();
+        return PACO_ERR_INVALID_ARG;
+    }
+    if (cs != cudaStreamCaptureStatusNone) return PACO_ERR_INVALID_ARG;
     SvdLayout L = svd_layout(M, N);
     if (L.total > PACO_NOALLOC_BYTES) return PACO_ERR_UNSUPPORTED;
     void *scratch = nullptr;

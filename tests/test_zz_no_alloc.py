@@ -4,7 +4,8 @@ not grow its memory after start-up).  Its scratch is a device array inside
 the library, so the test checks that two calls in a row, sharing that array,
 each give the same SVD as the allocating entry point paco_svd, and singular
 values within 1e-5 * sigma_1 of FP64 LAPACK dgesdd, within the tolerances of
-the other GPU tests.  The file name sorts last so that a run
+the other GPU tests, and that a stream under capture is rejected (the call
+ends by synchronizing its stream).  The file name sorts last so that a run
 that stops at the first failure has already run every other test."""
 import ctypes
 
@@ -65,3 +66,21 @@ def test_noalloc_rejects_shapes_beyond_its_scratch():
     assert f(2048, 64, None, None, None, None, None) == P.PACO_ERR_UNSUPPORTED
     assert f(1024, 600, None, None, None, None, None) == P.PACO_ERR_UNSUPPORTED
     assert f(8, 16, None, None, None, None, None) == P.PACO_ERR_INVALID_ARG
+
+
+def test_noalloc_rejects_a_capturing_stream():
+    f = noalloc_fn()
+    A = torch.randn(64, 32, device="cuda")
+    U = torch.empty(64, 64, device="cuda")
+    Vt = torch.empty(32, 32, device="cuda")
+    s = torch.empty(32, device="cuda")
+    x = torch.zeros(4, device="cuda")
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        rc = f(64, 32, A.data_ptr(), U.data_ptr(), Vt.data_ptr(), s.data_ptr(),
+               torch.cuda.current_stream().cuda_stream)
+        x += 1
+    assert rc == P.PACO_ERR_INVALID_ARG
+    g.replay()  # the capture was left intact
+    torch.cuda.synchronize()
+    assert x[0].item() == 1.0
